@@ -1,0 +1,238 @@
+// rtm_capi.cpp — extern "C" entry points: the drop-in rtm_model() and the host-side
+// pieces of the path.  rtm_model keeps the reference's symbol, argument list and file side
+// effects (gubingluo RTM_GPU_velstr.cpp:23-28, rtm_model.cu:12-17, :286-303, :490-538,
+// :571-585) on top of the batched session engine.
+#include <sys/stat.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rtm_b200.h"
+#include "rtm_internal.h"
+
+namespace rtm {
+int session_batch_size(rtm_session *ss);
+int session_run_range(rtm_session *ss, int k0, int n);
+}  // namespace rtm
+
+using namespace rtm;
+
+static int env_int(const char *name, int def)
+{
+    const char *v = std::getenv(name);
+    return v && *v ? std::atoi(v) : def;
+}
+static int env_prec(const char *name)
+{
+    const char *v = std::getenv(name);
+    if (!v) return RTM_PREC_FP32;
+    if (!std::strcmp(v, "fp16")) return RTM_PREC_FP16;
+    if (!std::strcmp(v, "bf16")) return RTM_PREC_BF16;
+    return RTM_PREC_FP32;
+}
+
+extern "C" {
+
+void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int medium_flag, int flag_layout,
+               int sgyflag, int endianflag, int ismth, int nx, int nz, int nt, float dx, float dz, float dt, int npml,
+               float direct, float direct0, float tsnap, float fdom, float spx0, float spz0, float dspx, float offset,
+               float offsetmax, float amp, float alp, float *vp0, float *rho0, float *diffcoef, float *wavelet,
+               float *image1, float *image2s, float *image3s, float *image4s, float *image5s, float *image2m,
+               float *image3m, float *image4m, float *image5m, float *illum)
+{
+    (void)tsnap;
+    (void)wavelet;   // the reference regenerates the wavelet on the device (rtm_model.cu:86-88)
+    clear_error();
+    rtm_survey s;
+    std::memset(&s, 0, sizeof(s));
+    s.nx = nx; s.nz = nz; s.nt = nt; s.dx = dx; s.dz = dz; s.dt = dt; s.npml = npml;
+    s.fdom = fdom; s.amp = amp; s.alp = alp; s.layout = flag_layout;
+    s.spx0 = spx0; s.spz0 = spz0; s.dspx = dspx; s.offset = offset; s.offsetmax = offsetmax;
+    s.mode = mode; s.medium_flag = medium_flag; s.ismth = ismth;
+    s.direct = direct; s.direct0 = direct0; s.mute = 1;
+    s.receiver_depth = env_int("RTM_B200_RECEIVER_DEPTH", 0);
+    rtm_options o;
+    std::memset(&o, 0, sizeof(o));
+    o.device = idevice;
+    o.strip_precision = env_prec("RTM_B200_STRIPS");
+    o.gather_precision = env_prec("RTM_B200_GATHERS");
+    o.accum_fp64 = env_int("RTM_B200_ACCUM_FP64", 0);
+    o.batch = env_int("RTM_B200_BATCH", 0);
+    o.verbose = 1;
+    const size_t nimg = (size_t)nx * nz;
+    float *zero_imgs[6] = {image3s, image4s, image5s, image3m, image4m, image5m};
+    for (float *p : zero_imgs)
+        if (p) std::memset(p, 0, nimg * sizeof(float));
+
+    std::vector<int> shots;
+    for (int ishot = startshot; ishot <= nshot; ishot += (dshot > 0 ? dshot : 1)) shots.push_back(ishot);
+    if (shots.empty()) {
+        std::printf("rtm_model: no shots between %d and %d\n", startshot, nshot);
+        return;
+    }
+    rtm_session *ss = nullptr;
+    int rc = rtm_session_open(&ss, &s, &o, shots.data(), (int)shots.size(), vp0, rho0, nullptr, nullptr, diffcoef);
+    if (rc) {
+        std::printf("rtm_model: %s\n", rtm_last_error());
+        return;
+    }
+    char path[512];
+    if (mode == 1) {
+        for (size_t k = 0; k < shots.size(); k++) {
+            std::snprintf(path, sizeof(path), "./seisReal/%dseisreal.su", shots[k]);
+            int nt_f = 0, ntr_f = 0;
+            rc = read_gather_su(path, sgyflag, nullptr, &nt_f, &ntr_f, nullptr);
+            if (!rc && (nt_f != nt || ntr_f != rtm_session_nrec(ss, (int)k)))
+                rc = fail(RTM_ERR_IO, std::string(path) + " does not match nt/receiver count of the shot");
+            std::vector<float> g;
+            if (!rc) {
+                g.resize((size_t)nt_f * ntr_f);
+                rc = read_gather_su(path, sgyflag, g.data(), nullptr, nullptr, nullptr);
+            }
+            if (!rc) rc = rtm_session_set_gather(ss, (int)k, g.data());
+            if (rc) {
+                std::printf("rtm_model: %s\n", rtm_last_error());
+                rtm_session_close(ss);
+                return;
+            }
+        }
+    }
+    const int B = session_batch_size(ss);
+    std::vector<float> tmp(nimg), zeros(nimg, 0.0f);
+    for (size_t k0 = 0; k0 < shots.size(); k0 += B) {
+        int n = (int)std::min<size_t>(B, shots.size() - k0);
+        auto t0 = std::chrono::steady_clock::now();
+        rc = session_run_range(ss, (int)k0, n);
+        if (rc) {
+            std::printf("rtm_model: %s\n", rtm_last_error());
+            rtm_session_close(ss);
+            return;
+        }
+        double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        bool temp_dump = false;
+        for (int j = 0; j < n; j++) {
+            const int ishot = shots[k0 + j];
+            if (mode == 0) {   // rtm_model.cu:286-288
+                rtm_geometry g;
+                shot_geometry(s, ishot, g);
+                std::vector<float> gat((size_t)nt * g.nrec);
+                rtm_session_get_gather(ss, (int)(k0 + j), gat.data());
+                std::snprintf(path, sizeof(path), "./seisReal/%dseisreal.su", ishot);
+                if (write_gather_su(path, gat.data(), g, nt, sgyflag, endianflag))
+                    std::printf("The file %s open failed !\n", path);
+            }
+            if ((ishot - 1) % 50 == 0) temp_dump = true;
+            std::printf("%d shot finished: %g (s)\n", ishot, sec / n);
+        }
+        if (temp_dump) {   // rtm_model.cu:490-538 (images are written with dx, as there)
+            float *outs[4] = {image1, image2s, image2m, illum};
+            rtm_session_get_images(ss, outs[0] ? outs[0] : tmp.data(), image2s ? image2s : tmp.data(),
+                                   image2m ? image2m : tmp.data(), illum ? illum : tmp.data());
+            struct {
+                const char *name;
+                const float *img;
+            } temps[] = {{"Image2stemp", image2s}, {"Image3stemp", zeros.data()}, {"Image4stemp", zeros.data()},
+                         {"Image5stemp", zeros.data()}, {"Image1temp", image1}, {"Illumtemp", illum},
+                         {"Image2mtemp", image2m}, {"Image3mtemp", zeros.data()}, {"Image4mtemp", zeros.data()},
+                         {"Image5mtemp", zeros.data()}, {"Imagetruetemp", zeros.data()}};
+            for (auto &t : temps) {
+                if (!t.img) continue;
+                std::snprintf(path, sizeof(path), "./output/%s.su", t.name);
+                if (write_image_su(path, t.img, nz, nx, dx)) std::printf("The file %s open failed !\n", path);
+            }
+        }
+    }
+    rtm_session_get_images(ss, image1, image2s, image2m, illum);   // rtm_model.cu:575-585
+    std::snprintf(path, sizeof(path), "./output/%dImagetrue.su", idevice);
+    if (write_image_su(path, zeros.data(), nz, nx, dx)) std::printf("The file %s open failed !\n", path);
+    rtm_session_close(ss);
+}
+
+int rtm_shot_geometry(const rtm_survey *s, int ishot, rtm_geometry *g)
+{
+    if (!s || !g) return fail(RTM_ERR_ARG, "null argument");
+    return shot_geometry(*s, ishot, *g);
+}
+
+void rtm_coef_table(float *c100) { coef_table(c100); }
+
+int rtm_prepare_model(const float *vp, const float *rho, int nx, int nz, int nx1, int nx2, int npml, int medium_flag,
+                      float *vp2_pad, float *rho_pad)
+{
+    if (!vp || nx1 < 0 || nx2 >= nx || nx2 < nx1 || npml < 0) return fail(RTM_ERR_ARG, "bad model window");
+    const int X = nx2 - nx1 + 1 + 2 * npml, Z = nz + 2 * npml;
+    if (vp2_pad) {
+        extract_extend(vp, nx, nz, nx1, nx2, npml, true, vp2_pad);
+        if (medium_flag) pml_smooth(vp2_pad, X, Z, npml);
+    }
+    if (rho && rho_pad) {
+        extract_extend(rho, nx, nz, nx1, nx2, npml, false, rho_pad);
+        if (medium_flag) pml_smooth(rho_pad, X, Z, npml);
+    }
+    return RTM_OK;
+}
+
+int rtm_velsmooth(float *a, int n1, int n2, int nsp)
+{
+    if (!a || n1 < 1 || n2 < 1 || nsp < 0) return fail(RTM_ERR_ARG, "bad smoothing argument");
+    gauss_smooth(a, n1, n2, nsp);
+    return RTM_OK;
+}
+
+int rtm_pmlsmooth(float *a, int nxpad, int nzpad, int npml)
+{
+    if (!a || nxpad < 3 || nzpad < 3 || npml < 1) return fail(RTM_ERR_ARG, "bad smoothing argument");
+    pml_smooth(a, nxpad, nzpad, npml);
+    return RTM_OK;
+}
+
+int rtm_interp_model(const float *vp0, float *vp, int nx0, int nz0, int nx, int nz, int lx, int lz)
+{
+    if (!vp0 || !vp || lx < 1 || lz < 1 || nx != (nx0 - 1) * lx + 1 || nz != (nz0 - 1) * lz + 1)
+        return fail(RTM_ERR_ARG, "bad interpolation sizes");
+    interp_model(vp0, vp, nx0, nz0, nx, lx, lz);
+    return RTM_OK;
+}
+
+void rtm_get_constant(const float *vp, float fdom, float dx0, float dz0, int nx0, int nz0, int nt0, float dt0,
+                      float *dx, float *dz, int *nx, int *nz, int *nt, float *dt, int *lx, int *lz, float *vpmin,
+                      float *vpmax)
+{
+    get_constant(vp, fdom, dx0, dz0, nx0, nz0, nt0, dt0, dx, dz, nx, nz, nt, dt, lx, lz, vpmin, vpmax);
+}
+
+void rtm_laplace_image(float *image, int nx, int nz, int dx, int dz) { laplace_image(image, nx, nz, dx, dz); }
+void rtm_scale_image(const float *illum, float *image, int n) { scale_image(illum, image, n); }
+
+int rtm_read_params(const char *input_dir, rtm_params *p)
+{
+    if (!p) return fail(RTM_ERR_ARG, "null argument");
+    return read_params(input_dir, *p);
+}
+int rtm_read_velocity(const char *path, int nx, int nz, float *vp)
+{
+    if (!path || !vp || nx < 1 || nz < 1) return fail(RTM_ERR_ARG, "bad argument");
+    return read_velocity(path, nx, nz, vp);
+}
+int rtm_write_image_su(const char *path, const float *image, int nz, int nx, float d)
+{
+    if (!path || !image) return fail(RTM_ERR_ARG, "bad argument");
+    return write_image_su(path, image, nz, nx, d);
+}
+int rtm_write_gather_su(const char *path, const float *gather, const rtm_geometry *g, int nt, int sgyflag,
+                        int endianflag)
+{
+    if (!path || !gather || !g) return fail(RTM_ERR_ARG, "bad argument");
+    return write_gather_su(path, gather, *g, nt, sgyflag, endianflag);
+}
+int rtm_read_gather_su(const char *path, int sgyflag, float *gather, int *nt, int *ntr, rtm_geometry *keys)
+{
+    if (!path) return fail(RTM_ERR_ARG, "bad argument");
+    return read_gather_su(path, sgyflag, gather, nt, ntr, keys);
+}
+
+}  // extern "C"

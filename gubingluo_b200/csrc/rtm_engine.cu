@@ -1,0 +1,843 @@
+// rtm_engine.cu — host engine: sessions, device memory, batching of shots and the
+// per-pass time loops (reference shot driver rtm_model.cu:117-569, re-designed so that a
+// batch of shots shares every launch and all boundary strips stay in HBM).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "rtm_b200.h"
+#include "rtm_internal.h"
+#include "rtm_launch.h"
+#include "rtm_types.h"
+
+namespace rtm {
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(RTM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+    } while (0)
+
+static constexpr int kRing = 32;   // fp32 staging ring (steps) for reduced-precision strips
+
+static size_t elem_size(int prec) { return prec == RTM_PREC_FP32 ? 4 : 2; }
+static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Device allocation arena: one cudaMalloc per session, 256-byte aligned sub-allocations.
+struct Arena {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    void *take(size_t n)
+    {
+        size_t off = (used + 255) & ~(size_t)255;
+        if (off + n > size) return nullptr;
+        used = off + n;
+        return base + off;
+    }
+};
+
+struct ModelDev {       // one padded model pair on the device
+    float *inv_rho = nullptr, *kappa = nullptr;
+};
+
+struct ShotState {
+    int ishot = 0;
+    rtm_geometry g{};
+    int X = 0, Z = 0, pitch = 0, nxi = 0, nzi = 0, strip_len = 0;
+    float vpmax = 0;
+    int sbx0 = 0, sbz0 = 0, sbnx = 0, sbnz = 0;
+    ModelDev mf, mb;
+    float *pml = nullptr, *src = nullptr, *mute_row = nullptr;   // mute_row: v^2 row rz (+ v^2 at source)
+    float *gather_raw = nullptr;      // mode 0: [nt][nrec] modelled gather, unmuted
+    float *gather32 = nullptr;        // [nt][nrec] fp32 gather that is migrated (muted)
+    void *gather_packed = nullptr;    // fp16/bf16 copy
+    float *gather_scale = nullptr;
+    bool gather_ready = false;
+    std::vector<float> mute_row_host;
+};
+
+struct Slot {
+    WaveDev a{}, b{};
+    void *strips = nullptr;
+    float *strip_scale = nullptr, *strip_stage = nullptr;
+    void *g1 = nullptr, *illum = nullptr;
+};
+
+struct KernelTiming {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    int used = 0;
+};
+
+}  // namespace rtm
+
+struct rtm_session {
+    rtm_survey s{};
+    rtm_options o{};
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    rtm::Arena arena;
+    std::vector<rtm::ShotState> shots;
+    std::vector<rtm::Slot> slots;
+    int B = 0;                       // batch size (slots)
+    int maxX = 0, maxPitch = 0, Z = 0;
+    float *wavelet = nullptr, *coef = nullptr;
+    void *img1 = nullptr, *img2s = nullptr, *img2m = nullptr, *illum = nullptr;
+    ShotDev *d_shots = nullptr;
+    TileRef *d_tiles = nullptr;
+    void *d_fin = nullptr;
+    int max_tiles = 0;
+    std::map<std::string, rtm::KernelTiming> timing;
+    int launches = 0;
+    int last_batch_n = 0;
+    std::vector<int> last_batch_shots;
+};
+
+namespace rtm {
+
+static int check_survey(const rtm_survey &s)
+{
+    if (s.nx < 2 || s.nz < 2 || s.nt < 2) return fail(RTM_ERR_ARG, "nx, nz and nt must be >= 2");
+    if (!(s.dx > 0) || !(s.dz > 0) || !(s.dt > 0)) return fail(RTM_ERR_ARG, "dx, dz and dt must be > 0");
+    if (s.npml < RTM_RADIUS) return fail(RTM_ERR_ARG, "npml must be >= 10 (the stencil radius)");
+    if (s.mode != 0 && s.mode != 1) return fail(RTM_ERR_ARG, "mode must be 0 or 1");
+    if (s.receiver_depth < 0 || s.receiver_depth >= s.nz) return fail(RTM_ERR_ARG, "receiver_depth out of range");
+    return RTM_OK;
+}
+
+// Padded model pair of one shot window: v^2 (squared in float, extractvel1) and rho,
+// optionally PML-smoothed (medium_flag) and Gaussian-smoothed (ismth).
+static void prep_model(const rtm_survey &s, const float *vp, const float *rho, int nx1, int nx2, bool smooth,
+                       std::vector<float> &vp2, std::vector<float> &rp)
+{
+    const int nxl = nx2 - nx1 + 1, X = nxl + 2 * s.npml, Z = s.nz + 2 * s.npml;
+    vp2.assign((size_t)X * Z, 0.0f);
+    rp.assign((size_t)X * Z, 0.0f);
+    extract_extend(vp, s.nx, s.nz, nx1, nx2, s.npml, true, vp2.data());
+    extract_extend(rho, s.nx, s.nz, nx1, nx2, s.npml, false, rp.data());
+    if (s.medium_flag) {
+        pml_smooth(vp2.data(), X, Z, s.npml);
+        pml_smooth(rp.data(), X, Z, s.npml);
+    }
+    if (smooth && s.ismth > 0) {
+        gauss_smooth(vp2.data(), Z, X, s.ismth);
+        gauss_smooth(rp.data(), Z, X, s.ismth);
+    }
+}
+
+static int upload_model(rtm_session *ss, const std::vector<float> &vp2, const std::vector<float> &rho, int X, int Z,
+                        int pitch, ModelDev &m)
+{
+    std::vector<float> ir((size_t)pitch * Z, 0.0f), ka((size_t)pitch * Z, 0.0f);
+    for (int z = 0; z < Z; z++)
+        for (int x = 0; x < X; x++) {
+            float r = rho[(size_t)z * X + x];
+            ir[(size_t)z * pitch + x] = 1.0f / r;
+            ka[(size_t)z * pitch + x] = r * vp2[(size_t)z * X + x];
+        }
+    m.inv_rho = (float *)ss->arena.take(sizeof(float) * ir.size());
+    m.kappa = (float *)ss->arena.take(sizeof(float) * ka.size());
+    if (!m.inv_rho || !m.kappa) return fail(RTM_ERR_NOMEM, "device arena exhausted (models)");
+    CK(cudaMemcpyAsync(m.inv_rho, ir.data(), sizeof(float) * ir.size(), cudaMemcpyHostToDevice, ss->stream));
+    CK(cudaMemcpyAsync(m.kappa, ka.data(), sizeof(float) * ka.size(), cudaMemcpyHostToDevice, ss->stream));
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
+static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, int Z, int strip_len, int nxi, int nzi)
+{
+    size_t field = (size_t)pitch * Z * sizeof(float) + 256;
+    size_t b = 10 * field;
+    b += (size_t)s.nt * strip_len * elem_size(o.strip_precision) + 256;
+    if (o.strip_precision != RTM_PREC_FP32) {
+        b += (size_t)s.nt * 4 * sizeof(float) + 256;
+        b += (size_t)kRing * strip_len * sizeof(float) + 256;
+    }
+    b += 2 * ((size_t)nxi * nzi * (o.accum_fp64 ? 8 : 4) + 256);
+    return b;
+}
+
+static int open_session(rtm_session *ss, const float *vp, const float *rho, const float *vp_mig,
+                        const float *rho_mig, const float *diffcoef, const int *shot_ids, int nshots)
+{
+    const rtm_survey &s = ss->s;
+    const rtm_options &o = ss->o;
+    int rc = check_survey(s);
+    if (rc) return rc;
+    if (nshots < 1) return fail(RTM_ERR_ARG, "no shots");
+    CK(cudaSetDevice(o.device));
+    ss->dev = o.device;
+    CK(cudaStreamCreateWithFlags(&ss->stream, cudaStreamNonBlocking));
+
+    // geometry and sizes of every shot
+    ss->shots.resize(nshots);
+    size_t shot_bytes_total = 0;
+    ss->Z = s.nz + 2 * s.npml;
+    for (int k = 0; k < nshots; k++) {
+        ShotState &sh = ss->shots[k];
+        sh.ishot = shot_ids[k];
+        rc = shot_geometry(s, sh.ishot, sh.g);
+        if (rc) return rc;
+        sh.X = sh.g.nxpad;
+        sh.Z = sh.g.nzpad;
+        sh.pitch = round_up(sh.X, 32);
+        sh.nxi = sh.g.nxlength;
+        sh.nzi = s.nz;
+        sh.strip_len = 2 * RTM_RADIUS * (sh.nzi + sh.nxi) * 2;
+        ss->maxX = std::max(ss->maxX, sh.X);
+        ss->maxPitch = std::max(ss->maxPitch, sh.pitch);
+        size_t gb = (size_t)s.nt * sh.g.nrec;
+        shot_bytes_total += (s.mode == 0 ? 2 : 1) * (gb * 4 + 256);
+        if (o.gather_precision != RTM_PREC_FP32) shot_bytes_total += gb * 2 + (size_t)s.nt * 4 + 512;
+        shot_bytes_total += (size_t)pml_offsets(sh.X, sh.Z).total * 4 + 256 + (size_t)(sh.X + 1) * 4 + 256;
+    }
+    // source stamp boxes: cells where amp*expf(-alp^2*dist) can be non-zero
+    for (ShotState &sh : ss->shots) {
+        int hx = sh.X, hz = sh.Z;
+        if (s.alp != 0.0f) {
+            double r = std::sqrt(104.0 / ((double)s.alp * s.alp));
+            hx = (int)(r / s.dx) + 2;
+            hz = (int)(r / s.dz) + 2;
+        }
+        sh.sbx0 = std::max(0, sh.g.nsx - hx);
+        sh.sbz0 = std::max(0, sh.g.nsz - hz);
+        int x1 = std::min(sh.X - 1, sh.g.nsx + hx), z1 = std::min(sh.Z - 1, sh.g.nsz + hz);
+        sh.sbnx = x1 - sh.sbx0 + 1;
+        sh.sbnz = z1 - sh.sbz0 + 1;
+        shot_bytes_total += (size_t)sh.sbnx * sh.sbnz * 4 + 256;
+    }
+    // models: one padded pair per distinct window (layout 2 shares one for every shot)
+    std::map<std::pair<int, int>, int> windows;
+    for (ShotState &sh : ss->shots) windows[{sh.g.nx1, sh.g.nx2}] = 0;
+    const bool sep_b = (vp_mig != nullptr) || (s.ismth > 0);
+    size_t model_bytes = 0;
+    for (auto &w : windows) {
+        int X = w.first.second - w.first.first + 1 + 2 * s.npml;
+        model_bytes += (sep_b ? 4 : 2) * ((size_t)round_up(X, 32) * ss->Z * 4 + 256);
+    }
+    // device memory plan
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    const ShotState &big = *std::max_element(ss->shots.begin(), ss->shots.end(),
+                                             [](const ShotState &a, const ShotState &b) { return a.X < b.X; });
+    size_t per_slot = slot_bytes(s, o, big.pitch, big.Z, big.strip_len, big.nxi, big.nzi);
+    size_t fixed = model_bytes + shot_bytes_total + 4 * ((size_t)s.nx * s.nz * 8 + 256) + (size_t)s.nt * 4 + 4096 +
+                   (size_t)(64 << 20);
+    size_t budget = (size_t)(free_b * 0.92);
+    if (fixed + per_slot > budget) return fail(RTM_ERR_NOMEM, "survey does not fit in device memory");
+    int B = (int)std::min<size_t>((size_t)nshots, (budget - fixed) / per_slot);
+    if (o.batch > 0) B = std::min(B, o.batch);
+    B = std::max(B, 1);
+    ss->B = B;
+    size_t arena_bytes = fixed + (size_t)B * per_slot;
+    char *base = nullptr;
+    CK(cudaMalloc((void **)&base, arena_bytes));
+    ss->arena.base = base;
+    ss->arena.size = arena_bytes;
+
+    // wavelet and coefficient table
+    ss->wavelet = (float *)ss->arena.take((size_t)s.nt * 4);
+    ss->coef = (float *)ss->arena.take(100 * 4);
+    launch_ricker(ss->wavelet, s.fdom, s.dt, s.nt, ss->stream);
+    ss->launches++;
+    float ctab[100];
+    if (diffcoef) std::memcpy(ctab, diffcoef, sizeof(ctab));
+    else coef_table(ctab);
+    CK(cudaMemcpyAsync(ss->coef, ctab, sizeof(ctab), cudaMemcpyHostToDevice, ss->stream));
+    CK(cudaStreamSynchronize(ss->stream));
+    // stacked images
+    const size_t isz = (size_t)s.nx * s.nz * (o.accum_fp64 ? 8 : 4);
+    ss->img1 = ss->arena.take(isz);
+    ss->img2s = ss->arena.take(isz);
+    ss->img2m = ss->arena.take(isz);
+    ss->illum = ss->arena.take(isz);
+    CK(cudaMemsetAsync(ss->img1, 0, isz, ss->stream));
+    CK(cudaMemsetAsync(ss->img2s, 0, isz, ss->stream));
+    CK(cudaMemsetAsync(ss->img2m, 0, isz, ss->stream));
+    CK(cudaMemsetAsync(ss->illum, 0, isz, ss->stream));
+
+    // models
+    std::map<std::pair<int, int>, std::pair<ModelDev, ModelDev>> mcache;
+    std::map<std::pair<int, int>, std::pair<float, std::vector<float>>> vp2cache;
+    for (auto &w : windows) {
+        std::vector<float> vp2, rp;
+        const int nx1 = w.first.first, nx2 = w.first.second;
+        const int X = nx2 - nx1 + 1 + 2 * s.npml, pitch = round_up(X, 32);
+        prep_model(s, vp, rho, nx1, nx2, false, vp2, rp);
+        float m = vp2[0];
+        for (float v : vp2) m = v > m ? v : m;
+        ModelDev mf, mb;
+        rc = upload_model(ss, vp2, rp, X, ss->Z, pitch, mf);
+        if (rc) return rc;
+        mb = mf;
+        if (sep_b) {
+            std::vector<float> vb2, rb;
+            prep_model(s, vp_mig ? vp_mig : vp, rho_mig ? rho_mig : (vp_mig ? rho : rho), nx1, nx2, true, vb2, rb);
+            rc = upload_model(ss, vb2, rb, X, ss->Z, pitch, mb);
+            if (rc) return rc;
+        }
+        mcache[w.first] = {mf, mb};
+        vp2cache[w.first] = {sqrtf(m), std::move(vp2)};
+    }
+    // per-shot device state
+    for (ShotState &sh : ss->shots) {
+        auto key = std::make_pair(sh.g.nx1, sh.g.nx2);
+        sh.mf = mcache[key].first;
+        sh.mb = mcache[key].second;
+        sh.vpmax = vp2cache[key].first;
+        const std::vector<float> &v2 = vp2cache[key].second;
+        PmlOffsets po = pml_offsets(sh.X, sh.Z);
+        sh.pml = (float *)ss->arena.take((size_t)po.total * 4);
+        sh.src = (float *)ss->arena.take((size_t)sh.sbnx * sh.sbnz * 4);
+        sh.mute_row = (float *)ss->arena.take((size_t)(sh.X + 1) * 4);
+        size_t gb = (size_t)s.nt * sh.g.nrec;
+        sh.gather32 = (float *)ss->arena.take(gb * 4);
+        if (s.mode == 0) {
+            sh.gather_raw = (float *)ss->arena.take(gb * 4);
+            if (!sh.gather_raw) return fail(RTM_ERR_NOMEM, "device arena exhausted (gathers)");
+            CK(cudaMemsetAsync(sh.gather_raw, 0, gb * 4, ss->stream));
+        }
+        if (o.gather_precision != RTM_PREC_FP32) {
+            sh.gather_packed = ss->arena.take(gb * 2);
+            sh.gather_scale = (float *)ss->arena.take((size_t)s.nt * 4);
+        }
+        if (!sh.pml || !sh.src || !sh.mute_row || !sh.gather32 ||
+            (o.gather_precision != RTM_PREC_FP32 && (!sh.gather_packed || !sh.gather_scale)))
+            return fail(RTM_ERR_NOMEM, "device arena exhausted (shots)");
+        launch_setup_pml(sh.pml, sh.X, sh.Z, s.npml, s.dx, s.dz, s.dt, sh.vpmax, ss->stream);
+        launch_setup_source(sh.src, sh.sbx0, sh.sbz0, sh.sbnx, sh.sbnz, sh.g.nsx, sh.g.nsz, s.amp, s.alp,
+                            s.dx * s.dx, s.dz * s.dz, s.dt, ss->stream);
+        ss->launches += 2;
+        sh.mute_row_host.assign(sh.X + 1, 0.0f);
+        for (int x = 0; x < sh.X; x++) sh.mute_row_host[x] = v2[(size_t)sh.g.rz * sh.X + x];
+        sh.mute_row_host[sh.X] = v2[(size_t)sh.g.nsz * sh.X + sh.g.nsx];
+        CK(cudaMemcpyAsync(sh.mute_row, sh.mute_row_host.data(), sizeof(float) * (sh.X + 1), cudaMemcpyHostToDevice,
+                           ss->stream));
+        CK(cudaMemsetAsync(sh.gather32, 0, gb * 4, ss->stream));
+        CK(cudaStreamSynchronize(ss->stream));
+    }
+    // batch slots
+    ss->slots.resize(B);
+    for (Slot &sl : ss->slots) {
+        const size_t fb = (size_t)big.pitch * big.Z * 4;
+        float **f[10] = {&sl.a.p, &sl.a.vx, &sl.a.vz, &sl.a.sx, &sl.a.sz, &sl.b.p, &sl.b.vx, &sl.b.vz, &sl.b.sx, &sl.b.sz};
+        for (float **pp : f) {
+            *pp = (float *)ss->arena.take(fb);
+            if (!*pp) return fail(RTM_ERR_NOMEM, "device arena exhausted (fields)");
+        }
+        sl.strips = ss->arena.take((size_t)s.nt * big.strip_len * elem_size(o.strip_precision));
+        if (o.strip_precision != RTM_PREC_FP32) {
+            sl.strip_scale = (float *)ss->arena.take((size_t)s.nt * 4 * 4);
+            sl.strip_stage = (float *)ss->arena.take((size_t)kRing * big.strip_len * 4);
+        }
+        size_t ib = (size_t)big.nxi * big.nzi * (o.accum_fp64 ? 8 : 4);
+        sl.g1 = ss->arena.take(ib);
+        sl.illum = ss->arena.take(ib);
+        if (!sl.strips || !sl.g1 || !sl.illum) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
+    }
+    // descriptor and tile tables
+    ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
+    int tiles_per_shot = ((big.X + RTM_TX - 1) / RTM_TX) * ((big.Z + RTM_TZ - 1) / RTM_TZ);
+    ss->max_tiles = tiles_per_shot * B;
+    ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
+    ss->d_fin = ss->arena.take(finalize_shot_size() * B);
+    if (!ss->d_shots || !ss->d_tiles || !ss->d_fin) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
+// Mute the fp32 gather of shot k in place (reference kernel.cu:96-173) and pack it to the
+// storage precision.
+static int finish_gather(rtm_session *ss, ShotState &sh)
+{
+    const rtm_survey &s = ss->s;
+    if (s.mode == 0)
+        CK(cudaMemcpyAsync(sh.gather32, sh.gather_raw, sizeof(float) * (size_t)s.nt * sh.g.nrec,
+                           cudaMemcpyDeviceToDevice, ss->stream));
+    if (s.mute) {
+        int nw = (int)(s.direct / (s.fdom * s.dt));   // rtm_model.cu:22-23
+        int tlength = (int)(s.direct0 / s.dt);
+        float rdt = (float)(1.0 / s.dt);
+        launch_mute(sh.gather32, sh.mute_row, sh.X, sh.g.nsx, sh.g.nsz, s.nt, sh.g.rz, sh.g.rx0, sh.g.nrec, nw,
+                    tlength, s.dx * s.dx, s.dz * s.dz, rdt, ss->stream);
+        ss->launches++;
+    }
+    if (ss->o.gather_precision != RTM_PREC_FP32) {
+        launch_gather_pack(sh.gather32, sh.gather_packed, sh.gather_scale, s.nt, sh.g.nrec, ss->o.gather_precision,
+                           ss->stream);
+        ss->launches++;
+    }
+    sh.gather_ready = true;
+    CK(cudaGetLastError());
+    return RTM_OK;
+}
+
+static void timing_begin(rtm_session *ss, const char *name, int it, cudaEvent_t *ev_end)
+{
+    *ev_end = nullptr;
+    if (it % 64 != 7) return;
+    KernelTiming &t = ss->timing[name];
+    if (t.used == (int)t.ev.size()) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        t.ev.push_back({a, b});
+    }
+    cudaEventRecord(t.ev[t.used].first, ss->stream);
+    *ev_end = t.ev[t.used].second;
+    t.used++;
+}
+static void timing_end(rtm_session *ss, cudaEvent_t ev)
+{
+    if (ev) cudaEventRecord(ev, ss->stream);
+}
+
+// Batch state shared by the phases of one batch.
+struct BatchRun {
+    int k0 = 0, n = 0, ntiles = 0, maxrec = 0;
+    std::vector<ShotDev> hd;
+    StepArgs a{};
+};
+
+// Bind shots [k0, k0+n) to slots 0..n-1, zero their wavefields and accumulators, upload
+// the descriptor and (shot, tile) tables.
+static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
+{
+    const rtm_survey &s = ss->s;
+    const rtm_options &o = ss->o;
+    cudaStream_t st = ss->stream;
+    br.k0 = k0;
+    br.n = n;
+    br.hd.assign(n, ShotDev{});
+    std::vector<TileRef> tiles;
+    br.maxrec = 0;
+    for (int j = 0; j < n; j++) {
+        ShotState &sh = ss->shots[k0 + j];
+        Slot &sl = ss->slots[j];
+        ShotDev &d = br.hd[j];
+        std::memset(&d, 0, sizeof(d));
+        d.X = sh.X; d.Z = sh.Z; d.npml = s.npml; d.pitch = sh.pitch;
+        d.nxi = sh.nxi; d.nzi = sh.nzi;
+        d.nsx = sh.g.nsx; d.nsz = sh.g.nsz;
+        d.sbx0 = sh.sbx0; d.sbz0 = sh.sbz0; d.sbnx = sh.sbnx; d.sbnz = sh.sbnz;
+        d.rz = sh.g.rz; d.rx0 = sh.g.rx0; d.nrec = sh.g.nrec;
+        d.ntx = (sh.X + RTM_TX - 1) / RTM_TX;
+        d.strip_len = sh.strip_len;
+        d.inv_rho_f = sh.mf.inv_rho; d.kappa_f = sh.mf.kappa;
+        d.inv_rho_b = sh.mb.inv_rho; d.kappa_b = sh.mb.kappa;
+        d.pml = sh.pml; d.src = sh.src;
+        d.a = sl.a; d.b = sl.b;
+        d.strips = sl.strips; d.strip_scale = sl.strip_scale; d.strip_stage = sl.strip_stage;
+        d.gather = s.mode == 0 ? sh.gather_raw : sh.gather32;
+        d.gather_scale = nullptr;
+        d.g1 = sl.g1; d.illum = sl.illum;
+        int ntz = (sh.Z + RTM_TZ - 1) / RTM_TZ;
+        for (int t = 0; t < d.ntx * ntz; t++) tiles.push_back({j, t});
+        br.maxrec = std::max(br.maxrec, sh.g.nrec);
+        size_t fb = (size_t)sh.pitch * sh.Z * 4;
+        float *f[10] = {sl.a.p, sl.a.vx, sl.a.vz, sl.a.sx, sl.a.sz, sl.b.p, sl.b.vx, sl.b.vz, sl.b.sx, sl.b.sz};
+        for (float *p : f) CK(cudaMemsetAsync(p, 0, fb, st));
+        size_t ib = (size_t)sh.nxi * sh.nzi * (o.accum_fp64 ? 8 : 4);
+        CK(cudaMemsetAsync(sl.g1, 0, ib, st));
+        CK(cudaMemsetAsync(sl.illum, 0, ib, st));
+    }
+    br.ntiles = (int)tiles.size();
+    CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ss->d_tiles, tiles.data(), sizeof(TileRef) * br.ntiles, cudaMemcpyHostToDevice, st));
+    StepArgs &a = br.a;
+    std::memset(&a, 0, sizeof(a));
+    a.shots = ss->d_shots;
+    a.tiles = ss->d_tiles;
+    a.wavelet = ss->wavelet;
+    a.coef = ss->coef;
+    a.dt = s.dt;
+    a.dtx = s.dt / s.dx;   // rtm_model.cu:73-74
+    a.dtz = s.dt / s.dz;
+    a.strip_prec = o.strip_precision;
+    a.gather_prec = RTM_PREC_FP32;
+    a.accum_fp64 = o.accum_fp64;
+    ss->last_batch_n = n;
+    ss->last_batch_shots.clear();
+    for (int j = 0; j < n; j++) ss->last_batch_shots.push_back(k0 + j);
+    return RTM_OK;
+}
+
+// Source pass (rtm_model.cu:322-346): nsteps forward steps with the source added; strips
+// saved every step when `save`; the gather recorded when `record` (mode 0 fuses the
+// reference's separate modelling pass, rtm_model.cu:266-290, which is the same
+// computation in the same model, into this pass).
+static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, bool record)
+{
+    const rtm_options &o = ss->o;
+    cudaStream_t st = ss->stream;
+    StepArgs &a = br.a;
+    for (int it = 0; it < nsteps; it++) {
+        a.it = it;
+        a.ring = it % kRing;
+        cudaEvent_t e;
+        timing_begin(ss, "vel_fwd", it, &e);
+        launch_vel_fwd(a, br.ntiles, save ? 1 : 0, st);
+        timing_end(ss, e);
+        timing_begin(ss, "pres_fwd", it, &e);
+        launch_pres_fwd(a, br.ntiles, save ? 1 : 0, record ? 1 : 0, st);
+        timing_end(ss, e);
+        ss->launches += 2;
+        if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
+            launch_strip_pack(ss->d_shots, br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
+            ss->launches++;
+        }
+    }
+    CK(cudaGetLastError());
+    return RTM_OK;
+}
+
+// Backward pass (rtm_model.cu:348-456) and stacking (:458-488).
+static int batch_backward(rtm_session *ss, BatchRun &br)
+{
+    const rtm_survey &s = ss->s;
+    const rtm_options &o = ss->o;
+    cudaStream_t st = ss->stream;
+    const int n = br.n;
+    StepArgs &a = br.a;
+    for (int j = 0; j < n; j++) {
+        ShotState &sh = ss->shots[br.k0 + j];
+        if (s.mode == 0) {
+            int rc = finish_gather(ss, sh);
+            if (rc) return rc;
+        } else if (!sh.gather_ready) {
+            return fail(RTM_ERR_ARG, "shot " + std::to_string(sh.ishot) + " has no gather (rtm_session_set_gather)");
+        }
+        if (o.gather_precision != RTM_PREC_FP32) {
+            br.hd[j].gather = sh.gather_packed;
+            br.hd[j].gather_scale = sh.gather_scale;
+        } else {
+            br.hd[j].gather = sh.gather32;
+        }
+    }
+    CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
+    a.gather_prec = o.gather_precision;
+    // ps = final forward p; vxs = vzs = 0 (rtm_model.cu:367-372); the receiver wavefield
+    // starts from rest with the last gather sample injected (:410)
+    for (int j = 0; j < n; j++) {
+        ShotState &sh = ss->shots[br.k0 + j];
+        Slot &sl = ss->slots[j];
+        size_t fb = (size_t)sh.pitch * sh.Z * 4;
+        CK(cudaMemsetAsync(sl.a.vx, 0, fb, st));
+        CK(cudaMemsetAsync(sl.a.vz, 0, fb, st));
+    }
+    launch_inject(ss->d_shots, n, br.maxrec, s.nt - 1, s.dt, o.gather_precision, st);
+    ss->launches++;
+    for (int it = s.nt - 2; it >= 0; it--) {
+        a.it = it;
+        cudaEvent_t e;
+        timing_begin(ss, "vel_bwd", it, &e);
+        launch_vel_bwd(a, br.ntiles, st);
+        timing_end(ss, e);
+        timing_begin(ss, "pres_bwd", it, &e);
+        launch_pres_bwd(a, br.ntiles, st);
+        timing_end(ss, e);
+        ss->launches += 2;
+    }
+    CK(cudaGetLastError());
+    std::vector<char> fin(finalize_shot_size() * n);
+    for (int j = 0; j < n; j++) {
+        ShotState &sh = ss->shots[br.k0 + j];
+        int nwin = 50;   // rtm_model.cu:70, :464-465
+        while (2 * nwin >= sh.nxi) nwin -= 3;
+        fill_finalize_shot(fin.data() + j * finalize_shot_size(), ss->slots[j].g1, ss->slots[j].illum, sh.g.nx1,
+                           sh.nxi, nwin);
+    }
+    CK(cudaMemcpyAsync(ss->d_fin, fin.data(), fin.size(), cudaMemcpyHostToDevice, st));
+    launch_finalize(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->img1, ss->img2s, ss->img2m, ss->illum, st);
+    ss->launches++;
+    CK(cudaGetLastError());
+    return RTM_OK;
+}
+
+static int run_batch(rtm_session *ss, int k0, int n)
+{
+    BatchRun br;
+    int rc = batch_setup(ss, k0, n, br);
+    if (rc) return rc;
+    if ((rc = batch_forward(ss, br, ss->s.nt, true, ss->s.mode == 0))) return rc;
+    if ((rc = batch_backward(ss, br))) return rc;
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
+int session_batch_size(rtm_session *ss) { return ss ? ss->B : 0; }
+
+// Run shots [k0, k0+n) (n <= batch size) as one batch.
+int session_run_range(rtm_session *ss, int k0, int n)
+{
+    if (!ss || k0 < 0 || n < 1 || n > ss->B || k0 + n > (int)ss->shots.size())
+        return fail(RTM_ERR_ARG, "bad shot range");
+    CK(cudaSetDevice(ss->dev));
+    return run_batch(ss, k0, n);
+}
+
+}  // namespace rtm
+
+using namespace rtm;
+
+extern "C" {
+
+const char *rtm_last_error(void) { return rtm::last_error(); }
+const char *rtm_version(void) { return "rtm_b200 0.1 (sm_100a)"; }
+
+int rtm_session_open(rtm_session **out, const rtm_survey *s, const rtm_options *o, const int *shots, int nshots,
+                     const float *vp, const float *rho, const float *vp_mig, const float *rho_mig,
+                     const float *diffcoef)
+{
+    clear_error();
+    if (!out || !s || !o || !shots || !vp || !rho) return fail(RTM_ERR_ARG, "null argument");
+    *out = nullptr;
+    rtm_session *ss = new rtm_session();
+    ss->s = *s;
+    ss->o = *o;
+    int rc = open_session(ss, vp, rho, vp_mig, rho_mig, diffcoef, shots, nshots);
+    if (rc) {
+        rtm_session_close(ss);
+        return rc;
+    }
+    *out = ss;
+    return RTM_OK;
+}
+
+int rtm_session_set_gather(rtm_session *ss, int k, const float *gather)
+{
+    if (!ss || k < 0 || k >= (int)ss->shots.size() || !gather) return fail(RTM_ERR_ARG, "bad gather argument");
+    ShotState &sh = ss->shots[k];
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaMemcpyAsync(sh.gather32, gather, sizeof(float) * (size_t)ss->s.nt * sh.g.nrec, cudaMemcpyHostToDevice,
+                       ss->stream));
+    int rc = finish_gather(ss, sh);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
+int rtm_session_run(rtm_session *ss, rtm_stats *stats)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    CK(cudaSetDevice(ss->dev));
+    for (auto &kv : ss->timing) kv.second.used = 0;
+    int l0 = ss->launches;
+    auto t0 = std::chrono::steady_clock::now();
+    int nb = 0;
+    double cells = 0;
+    for (int k0 = 0; k0 < (int)ss->shots.size(); k0 += ss->B) {
+        int n = std::min(ss->B, (int)ss->shots.size() - k0);
+        int rc = run_batch(ss, k0, n);
+        if (rc) return rc;
+        nb++;
+        for (int j = 0; j < n; j++) {
+            const ShotState &sh = ss->shots[k0 + j];
+            cells += (double)ss->s.nt * (2.0 * sh.X * sh.Z + (double)sh.nxi * sh.nzi);
+        }
+        if (ss->o.verbose)
+            std::printf("rtm_b200: batch of %d shots done (%d/%zu)\n", n, k0 + n, ss->shots.size());
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (stats) {
+        stats->seconds_total = std::chrono::duration<double>(t1 - t0).count();
+        stats->gcell_updates = cells * 1e-9;
+        stats->shots = (int)ss->shots.size();
+        stats->batches = nb;
+        stats->kernel_launches = ss->launches - l0;
+    }
+    return RTM_OK;
+}
+
+int rtm_session_get_gather(rtm_session *ss, int k, float *gather)
+{
+    if (!ss || k < 0 || k >= (int)ss->shots.size() || !gather) return fail(RTM_ERR_ARG, "bad gather argument");
+    const ShotState &sh = ss->shots[k];
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    const float *src = ss->s.mode == 0 ? sh.gather_raw : sh.gather32;
+    CK(cudaMemcpy(gather, src, sizeof(float) * (size_t)ss->s.nt * sh.g.nrec, cudaMemcpyDeviceToHost));
+    return RTM_OK;
+}
+
+int rtm_session_nrec(rtm_session *ss, int k)
+{
+    if (!ss || k < 0 || k >= (int)ss->shots.size()) return -1;
+    return ss->shots[k].g.nrec;
+}
+
+static int copy_image(rtm_session *ss, void *dev, float *out)
+{
+    if (!out) return RTM_OK;
+    size_t n = (size_t)ss->s.nx * ss->s.nz;
+    if (ss->o.accum_fp64) {
+        std::vector<double> t(n);
+        CK(cudaMemcpy(t.data(), dev, n * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; i++) out[i] = (float)t[i];
+    } else {
+        CK(cudaMemcpy(out, dev, n * 4, cudaMemcpyDeviceToHost));
+    }
+    return RTM_OK;
+}
+
+int rtm_session_get_images(rtm_session *ss, float *image1, float *image2s, float *image2m, float *illum)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    int rc;
+    if ((rc = copy_image(ss, ss->img1, image1))) return rc;
+    if ((rc = copy_image(ss, ss->img2s, image2s))) return rc;
+    if ((rc = copy_image(ss, ss->img2m, image2m))) return rc;
+    if ((rc = copy_image(ss, ss->illum, illum))) return rc;
+    return RTM_OK;
+}
+
+int rtm_session_get_images_f64(rtm_session *ss, double *image1, double *image2s, double *illum)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    if (!ss->o.accum_fp64) return fail(RTM_ERR_ARG, "session accumulates in fp32");
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    size_t n = (size_t)ss->s.nx * ss->s.nz * 8;
+    if (image1) CK(cudaMemcpy(image1, ss->img1, n, cudaMemcpyDeviceToHost));
+    if (image2s) CK(cudaMemcpy(image2s, ss->img2s, n, cudaMemcpyDeviceToHost));
+    if (illum) CK(cudaMemcpy(illum, ss->illum, n, cudaMemcpyDeviceToHost));
+    return RTM_OK;
+}
+
+int rtm_session_reset_images(rtm_session *ss)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    size_t isz = (size_t)ss->s.nx * ss->s.nz * (ss->o.accum_fp64 ? 8 : 4);
+    CK(cudaMemsetAsync(ss->img1, 0, isz, ss->stream));
+    CK(cudaMemsetAsync(ss->img2s, 0, isz, ss->stream));
+    CK(cudaMemsetAsync(ss->img2m, 0, isz, ss->stream));
+    CK(cudaMemsetAsync(ss->illum, 0, isz, ss->stream));
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
+void *rtm_session_stream(rtm_session *ss) { return ss ? (void *)ss->stream : nullptr; }
+
+double rtm_session_kernel_ms(rtm_session *ss, const char *kernel, int *launches)
+{
+    if (launches) *launches = 0;
+    if (!ss || !kernel) return -1;
+    auto it = ss->timing.find(kernel);
+    if (it == ss->timing.end() || it->second.used == 0) return -1;
+    cudaStreamSynchronize(ss->stream);
+    double tot = 0;
+    for (int i = 0; i < it->second.used; i++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, it->second.ev[i].first, it->second.ev[i].second);
+        tot += ms;
+    }
+    if (launches) *launches = it->second.used;
+    return tot / it->second.used;
+}
+
+int rtm_session_get_wavefields(rtm_session *ss, int slot, float *ps, float *pr)
+{
+    if (!ss || slot < 0 || slot >= ss->last_batch_n) return fail(RTM_ERR_ARG, "bad slot");
+    const ShotState &sh = ss->shots[ss->last_batch_shots[slot]];
+    const Slot &sl = ss->slots[slot];
+    CK(cudaSetDevice(ss->dev));
+    if (ps) CK(cudaMemcpy2D(ps, sh.X * 4, sl.a.p, sh.pitch * 4, sh.X * 4, sh.Z, cudaMemcpyDeviceToHost));
+    if (pr) CK(cudaMemcpy2D(pr, sh.X * 4, sl.b.p, sh.pitch * 4, sh.X * 4, sh.Z, cudaMemcpyDeviceToHost));
+    return RTM_OK;
+}
+
+void rtm_session_close(rtm_session *ss)
+{
+    if (!ss) return;
+    cudaSetDevice(ss->dev);
+    if (ss->stream) cudaStreamSynchronize(ss->stream);
+    for (auto &kv : ss->timing)
+        for (auto &e : kv.second.ev) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    if (ss->arena.base) cudaFree(ss->arena.base);
+    if (ss->stream) cudaStreamDestroy(ss->stream);
+    delete ss;
+}
+
+int rtm_forward(const rtm_survey *s, const rtm_options *o, int ishot, const float *vp, const float *rho, int nsteps,
+                float *p, float *vx, float *vz, float *gather)
+{
+    clear_error();
+    if (!s || !o || !vp || !rho) return fail(RTM_ERR_ARG, "null argument");
+    if (nsteps < 1 || nsteps > s->nt) return fail(RTM_ERR_ARG, "nsteps must be in [1, nt]");
+    rtm_options oo = *o;
+    oo.batch = 1;
+    rtm_session *ss = nullptr;
+    int rc = rtm_session_open(&ss, s, &oo, &ishot, 1, vp, rho, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    BatchRun br;
+    const ShotState &sh = ss->shots[0];
+    const Slot &sl = ss->slots[0];
+    if (!(rc = batch_setup(ss, 0, 1, br)) && !(rc = batch_forward(ss, br, nsteps, false, true))) {
+        cudaError_t e = cudaStreamSynchronize(ss->stream);
+        if (e != cudaSuccess) rc = fail(RTM_ERR_CUDA, cudaGetErrorString(e));
+        const size_t w = sizeof(float);
+        if (!rc && p && cudaMemcpy2D(p, sh.X * w, sl.a.p, sh.pitch * w, sh.X * w, sh.Z, cudaMemcpyDeviceToHost))
+            rc = fail(RTM_ERR_CUDA, "copy p");
+        if (!rc && vx &&
+            cudaMemcpy2D(vx, (sh.X - 1) * w, sl.a.vx, sh.pitch * w, (sh.X - 1) * w, sh.Z, cudaMemcpyDeviceToHost))
+            rc = fail(RTM_ERR_CUDA, "copy vx");
+        if (!rc && vz && cudaMemcpy2D(vz, sh.X * w, sl.a.vz, sh.pitch * w, sh.X * w, sh.Z - 1, cudaMemcpyDeviceToHost))
+            rc = fail(RTM_ERR_CUDA, "copy vz");
+        if (!rc && gather &&
+            cudaMemcpy(gather, s->mode == 0 ? sh.gather_raw : sh.gather32, w * (size_t)nsteps * sh.g.nrec,
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = fail(RTM_ERR_CUDA, "copy gather");
+    }
+    rtm_session_close(ss);
+    return rc;
+}
+
+int rtm_migrate(const rtm_survey *s, const rtm_options *o, const int *shots, int nshots, const float *vp,
+                const float *rho, const float *vp_mig, const float *rho_mig, const float *const *gathers_in,
+                float *const *gathers_out, float *image1, float *image2s, float *image2m, float *illum,
+                rtm_stats *stats)
+{
+    rtm_session *ss = nullptr;
+    int rc = rtm_session_open(&ss, s, o, shots, nshots, vp, rho, vp_mig, rho_mig, nullptr);
+    if (rc) return rc;
+    if (s->mode == 1) {
+        for (int k = 0; k < nshots; k++) {
+            if (!gathers_in || !gathers_in[k]) {
+                rtm_session_close(ss);
+                return fail(RTM_ERR_ARG, "mode 1 needs a gather for every shot");
+            }
+            if ((rc = rtm_session_set_gather(ss, k, gathers_in[k]))) {
+                rtm_session_close(ss);
+                return rc;
+            }
+        }
+    }
+    if ((rc = rtm_session_run(ss, stats))) {
+        rtm_session_close(ss);
+        return rc;
+    }
+    if (s->mode == 0 && gathers_out)
+        for (int k = 0; k < nshots; k++)
+            if (gathers_out[k] && (rc = rtm_session_get_gather(ss, k, gathers_out[k]))) {
+                rtm_session_close(ss);
+                return rc;
+            }
+    rc = rtm_session_get_images(ss, image1, image2s, image2m, illum);
+    rtm_session_close(ss);
+    return rc;
+}
+
+}  // extern "C"

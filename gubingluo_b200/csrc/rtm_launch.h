@@ -1,0 +1,24 @@
+// rtm_launch.h — host launchers of the kernels in rtm_kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "rtm_types.h"
+
+void launch_vel_fwd(const StepArgs &a, int ntiles, int save, cudaStream_t s);
+void launch_pres_fwd(const StepArgs &a, int ntiles, int save, int record, cudaStream_t s);
+void launch_vel_bwd(const StepArgs &a, int ntiles, cudaStream_t s);
+void launch_pres_bwd(const StepArgs &a, int ntiles, cudaStream_t s);
+void launch_setup_pml(float *pml, int X, int Z, int npml, float dx, float dz, float dt, float vpmax, cudaStream_t s);
+void launch_setup_source(float *src, int sbx0, int sbz0, int sbnx, int sbnz, int nsx, int nsz, float amp, float alp,
+                         float dx2, float dz2, float dt, cudaStream_t s);
+void launch_ricker(float *w, float fdom, float dt, int nt, cudaStream_t s);
+void launch_mute(float *g, const float *vrow, int X, int nsx, int nsz, int nt, int rz, int rx0, int nrec, int nw,
+                 int tlength, float dx2, float dz2, float rdt, cudaStream_t s);
+void launch_strip_pack(const ShotDev *shots, int nshots, int it0, int ring0, int nsteps, int prec, cudaStream_t s);
+void launch_gather_pack(const float *g, void *out, float *scale, int nt, int nrec, int prec, cudaStream_t s);
+void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void *image1, void *image2s, void *image2m,
+                     void *illum, cudaStream_t s);
+void launch_laplace(const float *in, float *out, int nx, int nz, int dx, int dz, cudaStream_t s);
+void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float dt, int gather_prec, cudaStream_t s);
+size_t finalize_shot_size();
+void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin);

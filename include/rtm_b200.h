@@ -1,0 +1,207 @@
+/*
+ * rtm_b200.h — C-ABI of librtm_b200.so, the B200 (sm_100a) implementation of the
+ * gubingluo 2D acoustic prestack reverse-time-migration hot path.
+ *
+ * Plain C types only (ints, floats, pointers, sizes).  All arrays are host memory unless a
+ * comment says otherwise; models and images are row-major [iz][ix] (x fastest), gathers
+ * are [it][itrace] (trace fastest), exactly as in the reference.
+ *
+ * Reference interfaces replaced (gubingluo/gubingluo):
+ *   rtm_model          <- extern "C" rtm_model   RTM_GPU_velstr.cpp:23-28, rtm_model.cu:12-17
+ *   rtm_migrate / rtm_session_*  new: status-returning, file-free form of the same path
+ *   rtm_read_params    <- parameter-file reader  RTM_GPU_velstr.cpp:60-120
+ *   rtm_get_constant   <- get_constant           RTM_GPU_velstr.cpp:319-362
+ *   rtm_shot_geometry  <- per-layout shot window rtm_model.cu:122-154, 626-650, 1122-1158, 1629-1665
+ *   rtm_prepare_model  <- extractvel1/extractrho1/extendvel1/pmlvelsmooth1d/velsmooth1d
+ *                         Velocity_function.cpp:2011-2073, :9-103, :199-313
+ *   rtm_interp_model   <- interpvel1             Velocity_function.cpp:1946-1975
+ *   rtm_laplace_image  <- laplacefd1d            image_function.cpp:44-79
+ *   rtm_scale_image    <- scaleimage1d           image_function.cpp:11-20
+ *   rtm_coef_table     <- Diff_coeffVelStrLiuyang FD_function.cpp:73-165 (+ table RTM_GPU_velstr.cpp:184-196)
+ *   rtm_read_velocity  <- ReadVelMod             IO_function.cpp:9-35
+ *   rtm_write_image_su <- Output1d               IO_function.cpp:366-422
+ *   rtm_write_gather_su<- Outseisfile1d          IO_function.cpp:131-183 (+ sgyhead_function.cpp:351-383)
+ *   rtm_read_gather_su <- Inseisfile1d/get_parameter IO_function.cpp:284-324, :226-283
+ */
+#ifndef RTM_B200_H
+#define RTM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define RTM_OK 0
+#define RTM_ERR_ARG -1      /* invalid argument or size */
+#define RTM_ERR_CUDA -2     /* CUDA runtime error (device, launch, memory) */
+#define RTM_ERR_IO -3       /* file missing, unreadable or malformed */
+#define RTM_ERR_NOMEM -4    /* host or device allocation failed */
+
+/* ---- storage precisions ---- */
+#define RTM_PREC_FP32 0
+#define RTM_PREC_FP16 1
+#define RTM_PREC_BF16 2
+
+/* One survey: model grid, time axis, source, acquisition layout and migration mode.
+ * Field meanings follow the reference parameter file (RTM_GPU_velstr.cpp:76-120). */
+typedef struct rtm_survey {
+    int nx, nz, nt;          /* model size (after regridding) and time samples */
+    float dx, dz, dt;
+    int npml;                /* PML width in cells (any value >= 10) */
+    float fdom, amp, alp;    /* Ricker peak frequency, source amplitude, Gaussian width */
+    int layout;              /* 1 bilateral, 2 full array, 3 unilateral right, 4 unilateral left */
+    float spx0, spz0, dspx;  /* first source position, source depth, source interval (m) */
+    float offset, offsetmax; /* minimum offset (layouts 3/4) and aperture (layouts 1/3/4) */
+    int mode;                /* 0: model each shot's gather first, 1: migrate given gathers */
+    int medium_flag;         /* smooth the PML zone of the models (pmlvelsmooth1d) */
+    int ismth;               /* >0: smooth v^2 and rho by a Gaussian of half-width ismth after the
+                                source pass, as the reference does (rtm_model.cu:402-408) */
+    float direct, direct0;   /* direct-wave mute: nw = direct/(fdom*dt), tlength = direct0/dt */
+    int mute;                /* apply the direct-wave mute (the reference always does) */
+    int receiver_depth;      /* receiver row below z = 0 in cells (reference: 0) */
+} rtm_survey;
+
+typedef struct rtm_options {
+    int device;              /* CUDA device ordinal */
+    int strip_precision;     /* RTM_PREC_*: storage of the saved boundary strips */
+    int gather_precision;    /* RTM_PREC_*: storage of the receiver gathers */
+    int accum_fp64;          /* 1: image/illumination accumulation and division in fp64 */
+    int batch;               /* shots per launch; 0 = as many as fit in device memory */
+    int use_graph;           /* capture each pass's time loop in a CUDA graph */
+    int verbose;             /* print per-batch progress like the reference */
+} rtm_options;
+
+/* Geometry of one shot for the survey's layout (padded coordinates include the PML). */
+typedef struct rtm_geometry {
+    int nx1, nx2, nxlength, noffset;   /* model window [nx1, nx2] */
+    int nsx, nsz, nxpad, nzpad;        /* source node, padded grid */
+    int rz, rx0, nrec;                 /* receiver row, first receiver column, traces */
+    int iTraceAll, iTrace, Offset, sx, gx, Nt, Dt, Ntrace;  /* SU header keys of trace 1 */
+    float Dx;
+} rtm_geometry;
+
+typedef struct rtm_stats {
+    double seconds_total;    /* wall time of rtm_session_run / rtm_migrate's migration */
+    double gcell_updates;    /* cell-updates performed: nt*(2*X*Z + nxlen*nz) per shot */
+    int shots;
+    int batches;
+    int kernel_launches;     /* launches of this library's kernels */
+} rtm_stats;
+
+/* ---- drop-in entry point (same symbol, signature and file side effects as the reference) ----
+ * Writes ./seisReal/{ishot}seisreal.su in mode 0, reads it in mode 1, writes
+ * the ./output/ temp images after shots with (ishot-1)%50 == 0 and ./output/{idevice}Imagetrue.su,
+ * and overwrites the ten image arrays (nx*nz each).  The image3, image4 and image5 arrays and the Poynting image
+ * are the reference's extra imaging conditions, outside this library's scope: they are
+ * returned as zeros.  Errors are printed and recorded in rtm_last_error(). */
+void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int medium_flag,
+               int flag_layout, int sgyflag, int endianflag, int ismth, int nx, int nz, int nt,
+               float dx, float dz, float dt, int npml, float direct, float direct0, float tsnap,
+               float fdom, float spx0, float spz0, float dspx, float offset, float offsetmax,
+               float amp, float alp, float *vp0, float *rho0, float *diffcoef, float *wavelet,
+               float *image1, float *image2s, float *image3s, float *image4s, float *image5s,
+               float *image2m, float *image3m, float *image4m, float *image5m, float *illum);
+
+/* Last error message of this thread ("" when none). */
+const char *rtm_last_error(void);
+
+/* Library version string. */
+const char *rtm_version(void);
+
+/* ---- sessions: device-resident migration of a shot list ----
+ * shots: shot numbers (1-based ishot of the reference).  vp/rho: nz*nx velocity (m/s) and
+ * density (kg/m^3); vp_mig/rho_mig: model of the backward pass, NULL for the same model.
+ * diffcoef: 10x10 coefficient table (rtm_coef_table), NULL for the built-in one. */
+typedef struct rtm_session rtm_session;
+
+int rtm_session_open(rtm_session **out, const rtm_survey *s, const rtm_options *o, const int *shots,
+                     int nshots, const float *vp, const float *rho, const float *vp_mig,
+                     const float *rho_mig, const float *diffcoef);
+/* Mode 1: upload shot k's gather gathers[k] ([nt][nrec_k]), mute and pack it on the device. */
+int rtm_session_set_gather(rtm_session *ss, int k, const float *gather);
+/* Migrate every shot of the session; images accumulate on the device.  Inputs must be
+ * resident (rtm_session_set_gather for mode 1). */
+int rtm_session_run(rtm_session *ss, rtm_stats *stats);
+/* Mode 0: copy shot k's modelled (unmuted) gather to the host, [nt][nrec_k]. */
+int rtm_session_get_gather(rtm_session *ss, int k, float *gather);
+/* Copy the stacked images (nz*nx each; any pointer may be NULL). */
+int rtm_session_get_images(rtm_session *ss, float *image1, float *image2s, float *image2m,
+                           float *illum);
+int rtm_session_get_images_f64(rtm_session *ss, double *image1, double *image2s, double *illum);
+/* Zero the stacked images. */
+int rtm_session_reset_images(rtm_session *ss);
+/* Number of traces of shot k. */
+int rtm_session_nrec(rtm_session *ss, int k);
+/* cudaStream_t of the session (as void*), for event timing by the caller. */
+void *rtm_session_stream(rtm_session *ss);
+/* Per-launch device time of the named kernel family over the last run, measured with
+ * events on the session stream for a sample of the steps: "vel_bwd", "pres_bwd",
+ * "vel_fwd", "pres_fwd".  Returns the mean milliseconds per launch (-1 if not sampled). */
+double rtm_session_kernel_ms(rtm_session *ss, const char *kernel, int *launches);
+/* Final reconstructed source pressure and receiver pressure of the last shot run in slot k
+ * of the last batch ([nzpad][nxpad]); for parity tests. */
+int rtm_session_get_wavefields(rtm_session *ss, int slot, float *ps, float *pr);
+void rtm_session_close(rtm_session *ss);
+
+/* One call: open, upload (mode 1), run, fetch images, close. gathers_in (mode 1) and
+ * gathers_out (mode 0) are arrays of nshots host pointers (NULL entries skipped). */
+int rtm_migrate(const rtm_survey *s, const rtm_options *o, const int *shots, int nshots,
+                const float *vp, const float *rho, const float *vp_mig, const float *rho_mig,
+                const float *const *gathers_in, float *const *gathers_out, float *image1,
+                float *image2s, float *image2m, float *illum, rtm_stats *stats);
+
+/* Forward modelling only: nsteps source-pass steps of shot `ishot` from rest, in the model
+ * vp/rho (nz*nx, as for sessions).  Outputs (any may be NULL): p [nzpad][nxpad],
+ * vx [nzpad][nxpad-1], vz [nzpad-1][nxpad], gather [nsteps][nrec]. */
+int rtm_forward(const rtm_survey *s, const rtm_options *o, int ishot, const float *vp, const float *rho,
+                int nsteps, float *p, float *vx, float *vz, float *gather);
+
+/* ---- host-side pieces of the path ---- */
+int rtm_shot_geometry(const rtm_survey *s, int ishot, rtm_geometry *g);
+void rtm_coef_table(float *c100);
+/* Window [nx1, nx2] of the nz*nx models, square the velocity, pad by npml (edge
+ * replication), optionally smooth the PML zone: out [nz+2npml][nxlen+2npml]. */
+int rtm_prepare_model(const float *vp, const float *rho, int nx, int nz, int nx1, int nx2,
+                      int npml, int medium_flag, float *vp2_pad, float *rho_pad);
+int rtm_velsmooth(float *a, int n1, int n2, int nsp);
+int rtm_pmlsmooth(float *a, int nxpad, int nzpad, int npml);
+int rtm_interp_model(const float *vp0, float *vp, int nx0, int nz0, int nx, int nz, int lx, int lz);
+void rtm_get_constant(const float *vp, float fdom, float dx0, float dz0, int nx0, int nz0, int nt0,
+                      float dt0, float *dx, float *dz, int *nx, int *nz, int *nt, float *dt,
+                      int *lx, int *lz, float *vpmin, float *vpmax);
+void rtm_laplace_image(float *image, int nx, int nz, int dx, int dz);
+void rtm_scale_image(const float *illum, float *image, int n);
+
+/* ---- files ---- */
+typedef struct rtm_params {
+    float dt0; int nt0; float tsnap;
+    float xmax, zmax, dx0, dz0;
+    float fdom, amp, alp;
+    float spx0, spz0, dspx;
+    float offset, offsetmax;
+    int startshot, nshot, dshot, nshotall;
+    int npml;
+    int medium_flag, ismth;
+    float direct, direct0;
+    int idevice, flag_layout, mode, dataflag, sgyflag, endianflag, rhoflag;
+    char vp_file[256], shotgather_file[256], rho_file[256];
+} rtm_params;
+
+/* Read "<dir>/cmd.in" (its 2nd line names the parameter file, read from <dir>). */
+int rtm_read_params(const char *input_dir, rtm_params *p);
+/* nx traces of 240-byte header + nz native floats -> vp [nz][nx]. */
+int rtm_read_velocity(const char *path, int nx, int nz, float *vp);
+int rtm_write_image_su(const char *path, const float *image, int nz, int nx, float d);
+int rtm_write_gather_su(const char *path, const float *gather, const rtm_geometry *g, int nt,
+                        int sgyflag, int endianflag);
+/* Reads ntr traces of nt samples into gather [nt][ntr]; returns RTM_OK and the counts.
+ * gather may be NULL to query the sizes only. */
+int rtm_read_gather_su(const char *path, int sgyflag, float *gather, int *nt, int *ntr,
+                       rtm_geometry *keys);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,283 @@
+"""Python driver of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/_build/liboracle.so`` (the C restatement in rtm_oracle.c) and restates the
+reference's shot loop (gubingluo rtm_model.cu:117-488) on top of it: per-shot geometry,
+model window + square + padding (+ optional PML smoothing), one ``orc_shot`` per shot and
+the per-shot stacking.  Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU
+baseline use this module; the product never imports it.
+
+``load_reference_host()`` loads ``oracle/_ref/libref_host.so``: the reference's own host
+C++ compiled from its sources (oracle/ref/Makefile), used to pin the restatement.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_HOST = os.path.join(HERE, "_ref", "libref_host.so")
+REFERENCE_DIR = os.environ.get("RTM_REFERENCE_DIR", "/root/reference")
+
+_vp = C.c_void_p
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class OrcShot(C.Structure):
+    _fields_ = [("X", C.c_int), ("Z", C.c_int), ("npml", C.c_int), ("nt", C.c_int),
+                ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float),
+                ("nsx", C.c_int), ("nsz", C.c_int), ("amp", C.c_float), ("alp", C.c_float),
+                ("fdom", C.c_float), ("rz", C.c_int), ("rx0", C.c_int), ("nrec", C.c_int),
+                ("vpmax", C.c_float)]
+
+
+class OrcGeom(C.Structure):
+    _fields_ = ([(n, C.c_int) for n in ("nx1", "nx2", "nxlength", "noffset", "nsx", "nsz", "nxpad",
+                                        "nzpad", "rx0", "nrec", "iTraceAll", "iTrace", "Offset", "sx",
+                                        "gx")]
+                + [("Nt", C.c_ushort), ("Dt", C.c_ushort), ("Dx", C.c_float), ("Ntrace", C.c_int)])
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        for name in ("orc_shot_f32", "orc_shot_f64"):
+            getattr(L, name).argtypes = [C.POINTER(OrcShot)] + [_vp] * 6 + [C.c_int, _vp, C.c_int, C.c_int,
+                                                                             C.c_int] + [_vp] * 4
+        for name in ("orc_forward_f32", "orc_forward_f64"):
+            getattr(L, name).argtypes = [C.POINTER(OrcShot), _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp]
+        L.orc_finalize_f32.argtypes = [_vp, _vp] + [C.c_int] * 4 + [_vp] * 3
+        L.orc_finalize_f64.argtypes = [_vp, _vp] + [C.c_int] * 4 + [_vp] * 3
+        L.orc_geometry.argtypes = [C.POINTER(OrcGeom)] + [C.c_int] * 5 + [C.c_float] * 3 + [C.c_int] + [C.c_float] * 5
+        L.orc_coef_table.argtypes = [_vp]
+        L.orc_ricker_device.argtypes = [_vp, C.c_float, C.c_float, C.c_int]
+        L.orc_ricker_host.argtypes = [_vp, C.c_float, C.c_int, C.c_float]
+        L.orc_pml_profiles.argtypes = [_vp] * 4 + [C.c_float] * 3 + [C.c_int] * 3
+        L.orc_norder.argtypes = [_vp] * 3 + [C.c_int] * 2
+        L.orc_source.argtypes = [_vp] + [C.c_int] * 4 + [C.c_float] * 4
+        L.orc_mute.argtypes = [_vp, _vp] + [C.c_int] * 9 + [C.c_float] * 3
+        L.orc_taper.argtypes = [_vp, C.c_int, C.c_int, C.c_float]
+        L.orc_taper_nwin.argtypes = [C.c_int]
+        L.orc_extractvel1.argtypes = [_vp, _vp] + [C.c_int] * 5
+        L.orc_extendvel1.argtypes = [_vp, _vp] + [C.c_int] * 3
+        L.orc_pmlvelsmooth1d.argtypes = [_vp] + [C.c_int] * 3
+        L.orc_velsmooth1d.argtypes = [_vp] + [C.c_int] * 3
+        L.orc_interpvel1.argtypes = [_vp, _vp] + [C.c_int] * 6
+        L.orc_laplacefd1d.argtypes = [C.c_int] * 4 + [_vp]
+        L.orc_scaleimage1d.argtypes = [_vp, _vp, C.c_int]
+        L.orc_get_constant.argtypes = [_vp, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
+                                       C.c_float] + [_vp] * 10
+        _lib = L
+    return _lib
+
+
+def num_threads():
+    return lib().orc_num_threads()
+
+
+def coef_table():
+    c = np.zeros(100, np.float32)
+    lib().orc_coef_table(_p(c))
+    return c
+
+
+def geometry(layout, ishot, nx, nz, nt, dx, dz, dt, npml, spx0, spz0, dspx, offset=0.0, offsetmax=0.0):
+    g = OrcGeom()
+    rc = lib().orc_geometry(C.byref(g), layout, ishot, nx, nz, nt, dx, dz, dt, npml, spx0, spz0, dspx,
+                            offset, offsetmax)
+    if rc:
+        raise ValueError("bad layout")
+    return g
+
+
+def pad_model(v, nx1, nx2, npml, square, medium_flag=0):
+    """extractvel1/extractrho1 + extendvel1 (+ pmlvelsmooth1d)."""
+    v = f32(v)
+    nz, nx = v.shape
+    nxl = nx2 - nx1 + 1
+    tmp = np.zeros((nz, nxl), np.float32)
+    lib().orc_extractvel1(_p(tmp), _p(v), nx, nz, nx1, nx2, int(square))
+    pad = np.zeros((nz + 2 * npml, nxl + 2 * npml), np.float32)
+    lib().orc_extendvel1(_p(pad), _p(tmp), nxl, nz, npml)
+    if medium_flag:
+        lib().orc_pmlvelsmooth1d(_p(pad), pad.shape[1], pad.shape[0], npml)
+    return pad
+
+
+def velsmooth(a, nsp):
+    a = f32(a).copy()
+    lib().orc_velsmooth1d(_p(a), a.shape[0], a.shape[1], nsp)
+    return a
+
+
+def pml_profiles(vpmax, dx, dz, npml, X, Z):
+    out = [np.zeros(n, np.float32) for n in (X, Z, X - 1, Z - 1)]
+    lib().orc_pml_profiles(*[_p(a) for a in out], vpmax, dx, dz, npml, X, Z)
+    return out
+
+
+def norder(X, Z):
+    n = np.zeros((Z, X), np.int32)
+    nx_ = np.zeros(X - 1, np.int32)
+    nz_ = np.zeros(Z - 1, np.int32)
+    lib().orc_norder(_p(n), _p(nx_), _p(nz_), X, Z)
+    return n, nx_, nz_
+
+
+def shot_struct(X, Z, npml, nt, dx, dz, dt, nsx, nsz, amp, alp, fdom, rz, rx0, nrec, vpmax):
+    s = OrcShot()
+    for k, v in dict(X=X, Z=Z, npml=npml, nt=nt, dx=dx, dz=dz, dt=dt, nsx=nsx, nsz=nsz, amp=amp,
+                     alp=alp, fdom=fdom, rz=rz, rx0=rx0, nrec=nrec, vpmax=vpmax).items():
+        setattr(s, k, v)
+    return s
+
+
+def forward(shot: OrcShot, vp2, rho, nsteps, precision="f32", coef=None, wavelet=None):
+    """nsteps forward steps from rest -> (p, vx, vz, gather)."""
+    dt = np.float32 if precision == "f32" else np.float64
+    X, Z = shot.X, shot.Z
+    p = np.zeros((Z, X), dt)
+    vx = np.zeros((Z, X - 1), dt)
+    vz = np.zeros((Z - 1, X), dt)
+    g = np.zeros((nsteps, shot.nrec), dt)
+    coef = coef_table() if coef is None else f32(coef)
+    fn = lib().orc_forward_f32 if precision == "f32" else lib().orc_forward_f64
+    fn(C.byref(shot), _p(f32(vp2)), _p(f32(rho)), _p(coef), _p(None if wavelet is None else f32(wavelet)),
+       nsteps, _p(p), _p(vx), _p(vz), _p(g))
+    return p, vx, vz, g
+
+
+def shot(shot: OrcShot, vp2f, rhof, vp2b=None, rhob=None, mode=1, gather=None, mute=1, nw=0,
+         tlength=0, precision="f32", coef=None, wavelet=None, want_fields=False):
+    """One shot of RTM (source pass, backward loop, imaging); returns dict with g1, illum,
+    gather (modelled in mode 0) and optionally the final ps/p wavefields."""
+    dt = np.float32 if precision == "f32" else np.float64
+    nzi, nxi = shot.Z - 2 * shot.npml, shot.X - 2 * shot.npml
+    g1 = np.zeros((nzi, nxi), dt)
+    il = np.zeros((nzi, nxi), dt)
+    ps = np.zeros((shot.Z, shot.X), dt) if want_fields else None
+    pr = np.zeros((shot.Z, shot.X), dt) if want_fields else None
+    if gather is None:
+        gather = np.zeros((shot.nt, shot.nrec), np.float32)
+    else:
+        gather = f32(gather).copy()
+    coef = coef_table() if coef is None else f32(coef)
+    vp2f, rhof = f32(vp2f), f32(rhof)
+    vp2b = vp2f if vp2b is None else f32(vp2b)
+    rhob = rhof if rhob is None else f32(rhob)
+    fn = lib().orc_shot_f32 if precision == "f32" else lib().orc_shot_f64
+    rc = fn(C.byref(shot), _p(vp2f), _p(rhof), _p(vp2b), _p(rhob), _p(coef),
+            _p(None if wavelet is None else f32(wavelet)), mode, _p(gather), mute, nw, tlength,
+            _p(g1), _p(il), _p(ps), _p(pr))
+    if rc:
+        raise MemoryError("oracle allocation failed")
+    return dict(g1=g1, illum=il, gather=gather, ps=ps, p=pr)
+
+
+def rtm_model(survey: dict, shots, vp, rho, vp_mig=None, rho_mig=None, gathers=None,
+              precision="f32", keep_fields=False):
+    """Restatement of the reference's rtm_model shot loop for one layout (mode 0 models each
+    gather in (vp, rho) first; mode 1 migrates ``gathers``).  ``survey`` keys: nx nz nt dx dz
+    dt npml fdom amp alp layout spx0 spz0 dspx offset offsetmax mode medium_flag ismth direct
+    direct0 mute receiver_depth.  Returns stacked images (+ gathers)."""
+    s = survey
+    nx, nz = s["nx"], s["nz"]
+    acc = np.float32 if precision == "f32" else np.float64
+    image1 = np.zeros((nz, nx), acc)
+    image2s = np.zeros((nz, nx), acc)
+    illum = np.zeros((nz, nx), acc)
+    out_gathers, fields = [], []
+    nw = int(np.float32(s["direct"]) / (np.float32(s["fdom"]) * np.float32(s["dt"])))
+    tlength = int(np.float32(s["direct0"]) / np.float32(s["dt"]))
+    for k, ishot in enumerate(shots):
+        g = geometry(s["layout"], ishot, nx, nz, s["nt"], s["dx"], s["dz"], s["dt"], s["npml"],
+                     s["spx0"], s["spz0"], s["dspx"], s.get("offset", 0.0), s.get("offsetmax", 0.0))
+        vp2f = pad_model(vp, g.nx1, g.nx2, s["npml"], True, s.get("medium_flag", 0))
+        rhof = pad_model(rho, g.nx1, g.nx2, s["npml"], False, s.get("medium_flag", 0))
+        if vp_mig is not None or s.get("ismth", 0) > 0:
+            vb = vp_mig if vp_mig is not None else vp
+            rb = rho_mig if rho_mig is not None else rho
+            vp2b = pad_model(vb, g.nx1, g.nx2, s["npml"], True, s.get("medium_flag", 0))
+            rhob = pad_model(rb, g.nx1, g.nx2, s["npml"], False, s.get("medium_flag", 0))
+            if s.get("ismth", 0) > 0:
+                vp2b = velsmooth(vp2b, s["ismth"])
+                rhob = velsmooth(rhob, s["ismth"])
+        else:
+            vp2b, rhob = vp2f, rhof
+        vpmax = float(np.sqrt(np.float32(vp2f.max()), dtype=np.float32))
+        rz = s["npml"] + s.get("receiver_depth", 0)
+        sh = shot_struct(g.nxpad, g.nzpad, s["npml"], s["nt"], s["dx"], s["dz"], s["dt"], g.nsx, g.nsz,
+                         s["amp"], s["alp"], s["fdom"], rz, g.rx0, g.nrec, vpmax)
+        r = globals()["shot"](sh, vp2f, rhof, vp2b, rhob, mode=s["mode"],
+                              gather=None if s["mode"] == 0 else gathers[k], mute=s.get("mute", 1),
+                              nw=nw, tlength=tlength, precision=precision, want_fields=keep_fields)
+        out_gathers.append(r["gather"])
+        if keep_fields:
+            fields.append((r["ps"], r["p"]))
+        fin = lib().orc_finalize_f32 if precision == "f32" else lib().orc_finalize_f64
+        img2m = np.zeros_like(image1)
+        fin(_p(r["g1"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1, _p(image1), _p(image2s), _p(illum))
+    return dict(image1=image1, image2s=image2s, image2m=image1.copy(), illum=illum,
+                gathers=out_gathers, fields=fields)
+
+
+# ---- the reference's own host code (compiled from its sources) ----
+_ref = None
+
+
+def build_reference_host():
+    if not os.path.isdir(REFERENCE_DIR):
+        return False
+    subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "host", f"REF={REFERENCE_DIR}"], check=True)
+    return os.path.exists(REF_HOST)
+
+
+def load_reference_host():
+    """The reference's host C++ (libref_host.so) or None when it cannot be built here."""
+    global _ref
+    if _ref is not None:
+        return _ref
+    if not os.path.exists(REF_HOST) and not build_reference_host():
+        return None
+    L = C.CDLL(REF_HOST)
+    L.ref_Diff_coeffVelStrLiuyang.argtypes = [_vp, C.c_int]
+    L.ref_Ricker.argtypes = [_vp, C.c_float, C.c_int, C.c_float, C.c_int]
+    L.ref_pmlvelsmooth1d.argtypes = [_vp] + [C.c_int] * 3
+    L.ref_velsmooth1d.argtypes = [_vp] + [C.c_int] * 3
+    L.ref_interpvel1.argtypes = [_vp, _vp] + [C.c_int] * 6
+    L.ref_extendvel1.argtypes = [_vp, _vp] + [C.c_int] * 3
+    L.ref_extractvel1.argtypes = [_vp, _vp] + [C.c_int] * 4
+    L.ref_extractrho1.argtypes = [_vp, _vp] + [C.c_int] * 4
+    L.ref_laplacefd1d.argtypes = [C.c_int] * 4 + [_vp]
+    L.ref_scaleimage1d.argtypes = [_vp, _vp, C.c_int]
+    L.ref_Maxval1.argtypes = [_vp, C.c_int]
+    L.ref_Maxval1.restype = C.c_float
+    L.ref_get_constant.argtypes = [_vp, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
+                                   C.c_float] + [_vp] * 10
+    L.ref_Output1d.argtypes = [_vp, C.c_int, C.c_int, C.c_float, C.c_char_p, C.c_int]
+    L.ref_ReadVelMod.argtypes = [C.c_char_p, C.c_int, C.c_int, _vp]
+    L.ref_Outseisfile1d.argtypes = ([_vp] + [C.c_int] * 7 + [C.c_float] + [C.c_int] * 4 + [C.c_char_p])
+    L.ref_Inseisfile1d.argtypes = [_vp, C.c_int, C.c_int, C.c_char_p, _vp, _vp]
+    L.ref_get_parameter.argtypes = [C.c_char_p, C.c_int, _vp, _vp, _vp, _vp]
+    _ref = L
+    return L

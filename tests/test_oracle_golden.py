@@ -1,0 +1,146 @@
+"""Pins the CPU oracle to the reference itself.
+
+Golden vectors: the reference's own CUDA kernels and shot driver, rebuilt from its sources
+for sm_100a and run on a B200 (tests/golden/make_golden.py documents how).  The reference
+has no tests or fixtures of its own, so these runs are the only golden data.
+
+Tolerances: integer maps, PML profiles and the mute mask are bit-exact; quantities that go
+through expf (Ricker, source, taper) differ by at most 1 ulp between CUDA's and the host's
+expf; wavefields, gathers and images agree to FP32 rounding (rel-L2 <= 1e-5).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_case, rel_l2, survey_from_case
+
+
+@pytest.fixture(scope="module")
+def units():
+    path = os.path.join(GOLDEN, "ref_units.npz")
+    if not os.path.exists(path):
+        pytest.skip("ref_units.npz missing")
+    z = np.load(path)
+    m = z["units_meta"]
+    nxl, nzl, npml, dx, dz, dt, fdom, nt, nsx, nsz, amp, alp = m
+    d = dict(nxl=int(nxl), nzl=int(nzl), npml=int(npml), dx=dx, dz=dz, dt=dt, fdom=fdom, nt=int(nt),
+             nsx=int(nsx), nsz=int(nsz), amp=amp, alp=alp)
+    d["X"], d["Z"] = d["nxl"] + 2 * d["npml"], d["nzl"] + 2 * d["npml"]
+    vpmax, vpmax_prof, nsteps, nback = z["units_meta2"]
+    d.update(vpmax=vpmax, vpmax_prof=vpmax_prof, nsteps=int(nsteps), nback=int(nback))
+    return z, d
+
+
+def ulp_close(a, b, ulps=2):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    return np.all(np.abs(a - b) <= ulps * np.spacing(np.maximum(np.abs(a), np.abs(b))))
+
+
+def test_pml_profiles_bit_exact(oracle, units):
+    z, d = units
+    got = oracle.pml_profiles(np.float32(d["vpmax_prof"]), d["dx"], d["dz"], d["npml"], d["X"], d["Z"])
+    for name, g in zip(("pml_ddx", "pml_ddz", "pml_ddxvx", "pml_ddzvz"), got):
+        assert np.array_equal(g.view(np.int32), z[name].view(np.int32)), name
+
+
+def test_norder_maps_bit_exact(oracle, units):
+    z, d = units
+    n, nx_, nz_ = oracle.norder(d["X"], d["Z"])
+    assert np.array_equal(n.ravel(), z["norder"])
+    assert np.array_equal(nx_, z["norderx"])
+    assert np.array_equal(nz_, z["norderz"])
+
+
+def test_ricker_source_taper_ulp(oracle, units):
+    z, d = units
+    w = np.zeros(d["nt"], np.float32)
+    oracle.lib().orc_ricker_device(oracle._p(w), np.float32(d["fdom"]), np.float32(d["dt"]), d["nt"])
+    assert ulp_close(w, z["ricker"], 2)
+    X, Z = d["X"], d["Z"]
+    src = np.zeros((Z, X), np.float32)
+    oracle.lib().orc_source(oracle._p(src), X, Z, d["nsx"], d["nsz"], np.float32(d["amp"]), np.float32(d["alp"]),
+                            np.float32(d["dx"] * d["dx"]), np.float32(d["dz"] * d["dz"]))
+    ref = z["source"].reshape(Z, X)
+    assert np.array_equal(src != 0, ref != 0), "source support differs"
+    assert ulp_close(src, ref, 2)
+    nwin = oracle.lib().orc_taper_nwin(d["nxl"])
+    t = np.zeros(d["nxl"], np.float32)
+    oracle.lib().orc_taper(oracle._p(t), d["nxl"], nwin, np.float32(0.06))
+    tr = z["taper"].reshape(d["nzl"], d["nxl"])
+    assert (tr == tr[0]).all()
+    assert ulp_close(t, tr[0], 2)
+
+
+def _padded_model(oracle, z, d):
+    v = z["model_v"].reshape(d["nzl"], d["nxl"])
+    r = z["model_rho"].reshape(d["nzl"], d["nxl"])
+    vp2 = oracle.pad_model(v, 0, d["nxl"] - 1, d["npml"], True)
+    rho = oracle.pad_model(r, 0, d["nxl"] - 1, d["npml"], False)
+    return vp2, rho
+
+
+def test_mute_mask_bit_exact(oracle, units):
+    z, d = units
+    vp2, _ = _padded_model(oracle, z, d)
+    nw, tl = z["mute_meta"]
+    g = np.ones((d["nt"], d["nxl"]), np.float32)
+    rdt = np.float32(1.0 / np.float64(np.float32(d["dt"])))
+    oracle.lib().orc_mute(oracle._p(g), oracle._p(vp2), d["X"], d["nsx"], d["nsz"], d["nt"], d["npml"],
+                          d["npml"], d["nxl"], int(nw), int(tl), np.float32(d["dx"] ** 2),
+                          np.float32(d["dz"] ** 2), rdt)
+    assert np.array_equal(g, z["mute_mask"].reshape(d["nt"], d["nxl"]))
+
+
+def _shot(oracle, d, vpmax):
+    return oracle.shot_struct(d["X"], d["Z"], d["npml"], d["nt"], d["dx"], d["dz"], d["dt"], d["nsx"], d["nsz"],
+                              d["amp"], d["alp"], d["fdom"], d["npml"], d["npml"], d["nxl"], vpmax)
+
+
+def test_forward_steps_match_reference(oracle, units):
+    """300 steps of the reference's 9-launch forward step (interior + split PML + source)."""
+    z, d = units
+    vp2, rho = _padded_model(oracle, z, d)
+    vpmax = np.float32(np.sqrt(np.float32(vp2.max()), dtype=np.float32))
+    assert vpmax == np.float32(d["vpmax"])
+    p, vx, vz, g = oracle.forward(_shot(oracle, d, vpmax), vp2, rho, d["nsteps"])
+    X, Z = d["X"], d["Z"]
+    assert rel_l2(p, z["fwd_p"].reshape(Z, X)) < 1e-5
+    assert rel_l2(vx, z["fwd_vx"].reshape(Z, X - 1)) < 1e-5
+    assert rel_l2(vz, z["fwd_vz"].reshape(Z - 1, X)) < 1e-5
+    assert rel_l2(g, z["fwd_gather"].reshape(d["nsteps"], d["nxl"])) < 1e-5
+    # the PML band of p equals the reference's split-field sum there
+    npml = d["npml"]
+    band = np.ones((Z, X), bool)
+    band[npml:Z - npml, npml:X - npml] = False
+    assert rel_l2(p[band], z["fwd_p"].reshape(Z, X)[band]) < 1e-5
+
+
+def test_fp64_oracle_agrees(oracle, units):
+    z, d = units
+    vp2, rho = _padded_model(oracle, z, d)
+    vpmax = np.float32(d["vpmax"])
+    p32 = oracle.forward(_shot(oracle, d, vpmax), vp2, rho, d["nsteps"])[0]
+    p64 = oracle.forward(_shot(oracle, d, vpmax), vp2, rho, d["nsteps"], precision="f64")[0]
+    assert rel_l2(p32, p64) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["caseB", "caseC", "caseD"])
+def test_rtm_images_match_reference(oracle, name):
+    """Full rtm_model() runs of the reference (modelling, source pass with strips,
+    reconstruction, receiver back-propagation, imaging, taper and stacking)."""
+    z, prm = load_case(name)
+    s = survey_from_case(prm)
+    shots = list(range(1, prm["nshot"] + 1))
+    vp, rho = z["vp0"], z["rho0"]
+    gathers = None
+    if prm["mode"] == 1:
+        src, _ = load_case(prm["data_from"])
+        gathers = [src[f"gather{i}"] for i in shots]
+    r = oracle.rtm_model(s, shots, vp, rho, gathers=gathers)
+    for k in ("image1", "image2s", "image2m", "illum"):
+        assert rel_l2(r[k], z[k]) < 1e-5, k
+    if prm["mode"] == 0:
+        for i in shots:
+            assert rel_l2(r["gathers"][i - 1], z[f"gather{i}"]) < 1e-5
