@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 RTM path: shots/s (and Gcell-updates/s) of 2-D acoustic prestack
+reverse-time migration on the 64-shot full-spread survey of benchmark configuration 2
+(1701 x 351 grid, dx = dz = 12.5 m, 50-cell PML, nt = 4000, 15 Hz Ricker,
+source-illumination-normalised imaging), synthetic seeded model.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step migrates --shots-per-step shots per GPU (mode 1: recorded gathers in, stacked images
+out).  `value` times K steps with the gathers already resident in device memory; `e2e` times
+K steps through the same public C-ABI with each step's gathers copied from pinned host memory
+and the stacked image read back.  Under torchrun each rank migrates its own shots (weak
+scaling); the partial images are summed across ranks with an NCCL all-reduce every step.
+
+--impl reference times the reference's CPU path on the host cores.  The reference has no CPU
+implementation of the stencil or imaging (its host code is serial model preparation and file
+I/O), so this arm runs the CPU restatement of its algorithm (oracle/, FP32, OpenMP on all host
+threads) on a bounded sample: one shot of the same grid for --cpu-sample-steps time steps,
+scaled to shots/s of the full nt.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("config 2: 1701x351 grid (X x Z = 1801 x 451 padded), dx=dz=12.5 m, 50-cell PML, nt=4000, "
+            "dt=1 ms, 15 Hz Ricker, 64 full-spread shots every 25 grid points, source-illumination-"
+            "normalised imaging, FP32 stencil/strips/gathers/accumulators")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--shots-per-step", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=0, help="shots per launch (0: all shots of a step)")
+    ap.add_argument("--nt", type=int, default=0, help="override nt (quick runs only)")
+    ap.add_argument("--strips", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--gathers", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--accum-fp64", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="run --steps steps and exit (for ncu launch lists)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd[1:1] = ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], swp=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        load = [r for r in rows if r["power"] > 250.0] or rows
+        reasons = set()
+        for r in load:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("swp", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in load), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(load)}
+
+
+def measured_hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_unit(kernel: str):
+    """DRAM bytes per cell of one launch of `kernel` from the committed ncu summary
+    (profiles/ncu_<kernel>.txt, line 'dram_bytes_per_cell=<float>'), or None."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel}.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_cell="):
+            return float(line.split("=", 1)[1])
+    return None
+
+
+# ------------------------------------------------------------------------------------------
+def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int) -> float:
+    """Algorithmic DRAM bytes of one launch of `kind` for one shot: every array the kernel
+    must read or write, once (4-byte fields; PML split fields excluded as thin bands).
+      vel_*:  read p, 1/rho; read+write vx, vz                  -> 24 B per padded cell
+      pres_*: read vx, vz, kappa; read+write p                  -> 20 B per padded cell
+      backward kernels add the interior reconstruction (vel: read ps, rw vxs, vzs = 20 B;
+      pres: read vxs, vzs, rw ps = 16 B) and pres_bwd the imaging (rw g1, illum)."""
+    cells, inner = X * Z, nxi * nzi
+    strips = 80 * (nxi + nzi)   # one kernel writes or reads half of the 40*(nxi+nzi) fp32 strips
+    if kind == "vel_fwd":
+        return 24 * cells + strips
+    if kind == "pres_fwd":
+        return 20 * cells + strips
+    if kind == "vel_bwd":
+        return 24 * cells + 20 * inner + strips
+    if kind == "pres_bwd":
+        return 20 * cells + 16 * inner + 4 * accum_bytes * inner + strips + 4 * nrec
+    raise ValueError(kind)
+
+
+class _CudaArray:
+    """__cuda_array_interface__ view of a device pointer (for torch.distributed)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import gubingluo_b200 as G
+    from gubingluo_b200 import synthetic
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    s, all_shots, v_true, v_mig, rho, meta = synthetic.config(args.config, nt=args.nt or None)
+    B = args.shots_per_step
+    K, W = args.steps, args.warmup
+    # this rank's shots: every world-th shot of the survey, repeated as needed
+    mine = all_shots[rank::world] or all_shots[:1]
+    need = B * (K + W)
+    uniq = mine[: min(len(mine), need)]
+    step_shots = [uniq[(i * B + j) % len(uniq)] for i in range(K + W) for j in range(B)]
+    opts = G.RunOptions(device=local_rank, strip_precision=args.strips, gather_precision=args.gathers,
+                        accum_fp64=args.accum_fp64, batch=args.batch or B)
+    # ---- synthetic data: model this rank's gathers in the true model (untimed setup)
+    t0 = time.time()
+    s_model = G.SurveyConfig(**{**s.__dict__, "mode": 0})
+    with G.Session(s_model, G.RunOptions(device=local_rank, batch=min(len(uniq), 32)), uniq, v_true, rho) as ms:
+        ms.model()
+        gathers = {sh: ms.gather(k) for k, sh in enumerate(uniq)}
+    t_data = time.time() - t0
+    # ---- migration session: the session holds every shot the steps use (inputs resident)
+    s_mig = G.SurveyConfig(**{**s.__dict__, "mode": 1})
+    ss = G.Session(s_mig, opts, step_shots, v_mig, rho)
+    for k, sh in enumerate(step_shots):
+        ss.set_gather(k, gathers[sh])
+    geo = G.geometry(s_mig, step_shots[0])
+    X, Z, nxi, nzi, nrec = geo.nxpad, geo.nzpad, geo.nxlength, s.nz, geo.nrec
+    w_shot = s.nt * (2.0 * X * Z + nxi * nzi)           # cell-updates per shot
+    stream = torch.cuda.ExternalStream(ss.stream())
+    ptrs = ss.image_ptrs()
+    npix = s.nx * s.nz
+    typestr = "<f8" if args.accum_fp64 else "<f4"
+    img_views = [torch.as_tensor(_CudaArray(ptrs[k], npix, typestr), device=f"cuda:{local_rank}")
+                 for k in ("image1", "image2s", "illum")] if dist else []
+
+    def reduce_images():
+        if dist:
+            with torch.cuda.stream(stream):
+                for t in img_views:
+                    dist.all_reduce(t)
+
+    def step(i):
+        st = ss.run_range(i * B, B)
+        reduce_images()
+        return st
+
+    for i in range(W):
+        step(i)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    for i in range(W, W + K):
+        launches += step(i).kernel_launches
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    if dist:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    kern = {k: ss.kernel_ms(k) for k in ("vel_fwd", "pres_fwd", "vel_bwd", "pres_bwd")}
+    if args.profile_only:
+        ss.close()
+        return None
+    t_max = torch.tensor([ms_total], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_total = float(t_max.item())
+    shots_done = K * B * world
+    value = shots_done / (ms_total * 1e-3)
+    gcell = shots_done * w_shot / (ms_total * 1e-3) * 1e-9
+
+    # ---- e2e: the same steps through the public API with host-resident inputs
+    e2e = None
+    if not args.no_e2e:
+        host = {}
+        for sh in set(step_shots):
+            t = torch.empty((s.nt, nrec), dtype=torch.float32, pin_memory=True)
+            t.numpy()[:] = gathers[sh]
+            host[sh] = t
+        img_host = torch.empty((s.nz, s.nx), dtype=torch.float32, pin_memory=True)
+        h2d = B * s.nt * nrec * 4
+        d2h = s.nz * s.nx * 4
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(W, W + K):
+            for j in range(B):
+                k = i * B + j
+                G._check(G.lib().rtm_session_set_gather(ss.h, k, host[step_shots[k]].data_ptr()))
+            step(i)
+            G._check(G.lib().rtm_session_get_images(ss.h, None, img_host.data_ptr(), None, None))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1)
+        t_max = torch.tensor([ms_e2e], dtype=torch.float64, device=f"cuda:{local_rank}")
+        if dist:
+            dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t_max.item())
+        e2e = {"value": shots_done / (ms_e2e * 1e-3), "unit": "shots/s", "h2d_bytes_per_step": h2d * world,
+               "d2h_bytes_per_step": d2h * world, "ms_per_step": ms_e2e / K}
+    ss.close()
+
+    # ---- roofline of the dominant kernel
+    accum_bytes = 8 if args.accum_fp64 else 4
+    sampled = {k: v for k, v in kern.items() if v[0] > 0}
+    dom = max(sampled, key=lambda k: sampled[k][0])
+    launch_ms = sampled[dom][0]
+    nshots_launch = min(B, args.batch or B)
+    bytes_launch = nshots_launch * kernel_bytes(dom, X, Z, nxi, nzi, nrec, accum_bytes)
+    achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    per_cell = ncu_traffic_per_unit(dom)
+    roofline = {"kernel": f"k_{dom}", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": None if per_cell is None else round(per_cell * nshots_launch * X * Z),
+                "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 4),
+                "launches_sampled": sampled[dom][1],
+                "kernel_ms": {k: round(v[0], 4) for k, v in sampled.items()}}
+    return dict(value=value, gcell=gcell, ms_total=ms_total, launches=launches, e2e=e2e, roofline=roofline,
+                clocks=clock_info, shots_done=shots_done, t_data=t_data, X=X, Z=Z, nxi=nxi, nzi=nzi, nrec=nrec,
+                w_shot=w_shot, s=s)
+
+
+# ------------------------------------------------------------------------------------------
+def cpu_sample(args, s, v_mig, rho, nrec, w_shot):
+    """The CPU restatement of the reference's path (oracle, FP32, OpenMP) on one shot of the
+    same grid for --cpu-sample-steps steps; returns shots/s of the full nt and the sample."""
+    from oracle import oracle as O
+
+    nt_s = args.cpu_sample_steps
+    g = O.geometry(s.layout, 1, s.nx, s.nz, nt_s, s.dx, s.dz, s.dt, s.npml, s.spx0, s.spz0, s.dspx)
+    vp2 = O.pad_model(v_mig, g.nx1, g.nx2, s.npml, True)
+    rp = O.pad_model(rho, g.nx1, g.nx2, s.npml, False)
+    vpmax = float(np.sqrt(np.float32(vp2.max()), dtype=np.float32))
+    sh = O.shot_struct(g.nxpad, g.nzpad, s.npml, nt_s, s.dx, s.dz, s.dt, g.nsx, g.nsz, s.amp, s.alp, s.fdom,
+                       s.npml + s.receiver_depth, g.rx0, g.nrec, vpmax)
+    data = np.random.default_rng(1).standard_normal((nt_s, g.nrec)).astype(np.float32) * 1e-6
+    t0 = time.time()
+    O.shot(sh, vp2, rp, mode=1, gather=data, mute=1, nw=int(np.float32(1.5) / (s.fdom * s.dt)), tlength=0)
+    sec = time.time() - t0
+    cells = nt_s * (2.0 * g.nxpad * g.nzpad + g.nxlength * s.nz)
+    gcell = cells / sec * 1e-9
+    return {"value": gcell * 1e9 / w_shot, "unit": "shots/s", "cores": O.num_threads(), "kind": "port",
+            "gcell_updates_per_s": round(gcell, 4), "seconds": round(sec, 2),
+            "sample": f"1 shot of the same {g.nxpad}x{g.nzpad} grid for {nt_s} of {s.nt} time steps (source pass, "
+                      f"reconstruction, receiver pass, imaging), scaled to the full nt"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from gubingluo_b200 import synthetic
+
+    s, shots, v_true, v_mig, rho, meta = synthetic.config(args.config, nt=args.nt or None)
+    X, Z = s.nx + 2 * s.npml, s.nz + 2 * s.npml
+    w_shot = s.nt * (2.0 * X * Z + s.nx * s.nz)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(args, s, v_mig, rho, s.nx, w_shot)
+        if i >= args.warmup:
+            vals.append(r)
+    value = statistics.mean(r["value"] for r in vals)
+    sec = statistics.mean(r["seconds"] for r in vals)
+    line = {"metric": "shots/s", "value": value, "unit": "shots/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "impl": "reference",
+            "data": "synthetic (seeded model of benchmark configuration 2)",
+            "config": {"workload": WORKLOAD, "shots_per_step": "bounded CPU sample"},
+            "gcell_updates_per_s": statistics.mean(r["gcell_updates_per_s"] for r in vals),
+            "cpu_baseline": {**vals[-1], "value": value},
+            "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    r = run_ours(args, rank, world, local_rank)
+    if r is None or rank != 0:
+        return
+    s = r["s"]
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from gubingluo_b200 import synthetic
+
+        _, _, _, v_mig, rho, _ = synthetic.config(args.config, nt=args.nt or None)
+        cpu = cpu_sample(args, s, v_mig, rho, r["nrec"], r["w_shot"])
+    dtype = "f32" if args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64 else \
+        f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {'f64' if args.accum_fp64 else 'f32'} images"
+    ws_gb = (args.batch or args.shots_per_step) * 12 * r["X"] * r["Z"] * 4 / 1e9
+    line = {"metric": "shots/s", "value": r["value"], "unit": "shots/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_total"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded gradient + random-field + thrust-fault model of configuration 2; gathers "
+                    "modelled in the true model by this library before timing; migration in the 250 m-smoothed model)",
+            "config": {"workload": WORKLOAD, "shots_per_step_per_gpu": args.shots_per_step,
+                       "shots_per_launch": args.batch or args.shots_per_step, "nt": s.nt,
+                       "parallelism": f"shots sharded over {world} GPU(s)",
+                       "l2": f"inputs larger than L2: per-launch wavefield+model working set {ws_gb:.1f} GB vs 126 MB L2"},
+            "gcell_updates_per_s": r["gcell"],
+            "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
+            "clocks": r["clocks"], "setup_seconds_data_modelling": round(r["t_data"], 2)}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -87,6 +87,9 @@ def lib() -> C.CDLL:
     L.rtm_session_set_gather.argtypes = [vp, C.c_int, vp]
     L.rtm_session_run.argtypes = [vp, C.POINTER(Stats)]
     L.rtm_session_get_gather.argtypes = [vp, C.c_int, vp]
+    L.rtm_session_run_range.argtypes = [vp, C.c_int, C.c_int, C.POINTER(Stats)]
+    L.rtm_session_model.argtypes = [vp]
+    L.rtm_session_image_ptrs.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
     L.rtm_session_get_images.argtypes = [vp, vp, vp, vp, vp]
     L.rtm_session_get_images_f64.argtypes = [vp, vp, vp, vp]
     L.rtm_session_reset_images.argtypes = [vp]
@@ -235,6 +238,20 @@ class Session:
         st = Stats()
         _check(lib().rtm_session_run(self.h, C.byref(st)))
         return st
+
+    def run_range(self, k0: int, n: int) -> Stats:
+        st = Stats()
+        _check(lib().rtm_session_run_range(self.h, k0, n, C.byref(st)))
+        return st
+
+    def model(self):
+        """Mode-0 sessions: model every shot's gather (no migration)."""
+        _check(lib().rtm_session_model(self.h))
+
+    def image_ptrs(self):
+        ptrs = [C.c_void_p() for _ in range(4)]
+        _check(lib().rtm_session_image_ptrs(self.h, *[C.byref(p) for p in ptrs]))
+        return dict(zip(("image1", "image2s", "image2m", "illum"), [p.value for p in ptrs]))
 
     def gather(self, k: int) -> np.ndarray:
         g = np.zeros((self.survey.nt, self.nrec(k)), np.float32)

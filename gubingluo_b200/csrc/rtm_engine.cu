@@ -575,6 +575,18 @@ static int run_batch(rtm_session *ss, int k0, int n)
 
 int session_batch_size(rtm_session *ss) { return ss ? ss->B : 0; }
 
+// Modelling only (the reference's mode-0 modelling pass, rtm_model.cu:266-290): record
+// the gathers of shots [k0, k0+n) without saving strips or migrating.
+static int model_range(rtm_session *ss, int k0, int n)
+{
+    BatchRun br;
+    int rc = batch_setup(ss, k0, n, br);
+    if (rc) return rc;
+    if ((rc = batch_forward(ss, br, ss->s.nt, false, true))) return rc;
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
 // Run shots [k0, k0+n) (n <= batch size) as one batch.
 int session_run_range(rtm_session *ss, int k0, int n)
 {
@@ -654,6 +666,59 @@ int rtm_session_run(rtm_session *ss, rtm_stats *stats)
         stats->batches = nb;
         stats->kernel_launches = ss->launches - l0;
     }
+    return RTM_OK;
+}
+
+int rtm_session_run_range(rtm_session *ss, int k0, int n, rtm_stats *stats)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    if (k0 < 0 || n < 1 || k0 + n > (int)ss->shots.size()) return fail(RTM_ERR_ARG, "bad shot range");
+    CK(cudaSetDevice(ss->dev));
+    for (auto &kv : ss->timing) kv.second.used = 0;
+    int l0 = ss->launches;
+    auto t0 = std::chrono::steady_clock::now();
+    int nb = 0;
+    double cells = 0;
+    for (int b0 = k0; b0 < k0 + n; b0 += ss->B) {
+        int m = std::min(ss->B, k0 + n - b0);
+        int rc = run_batch(ss, b0, m);
+        if (rc) return rc;
+        nb++;
+        for (int j = 0; j < m; j++) {
+            const ShotState &sh = ss->shots[b0 + j];
+            cells += (double)ss->s.nt * (2.0 * sh.X * sh.Z + (double)sh.nxi * sh.nzi);
+        }
+    }
+    if (stats) {
+        stats->seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        stats->gcell_updates = cells * 1e-9;
+        stats->shots = n;
+        stats->batches = nb;
+        stats->kernel_launches = ss->launches - l0;
+    }
+    return RTM_OK;
+}
+
+int rtm_session_model(rtm_session *ss)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    if (ss->s.mode != 0) return fail(RTM_ERR_ARG, "modelling needs a mode-0 session");
+    CK(cudaSetDevice(ss->dev));
+    for (int k0 = 0; k0 < (int)ss->shots.size(); k0 += ss->B) {
+        int n = std::min(ss->B, (int)ss->shots.size() - k0);
+        int rc = model_range(ss, k0, n);
+        if (rc) return rc;
+    }
+    return RTM_OK;
+}
+
+int rtm_session_image_ptrs(rtm_session *ss, void **image1, void **image2s, void **image2m, void **illum)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    if (image1) *image1 = ss->img1;
+    if (image2s) *image2s = ss->img2s;
+    if (image2m) *image2m = ss->img2m;
+    if (illum) *illum = ss->illum;
     return RTM_OK;
 }
 

@@ -124,6 +124,14 @@ int rtm_session_set_gather(rtm_session *ss, int k, const float *gather);
 /* Migrate every shot of the session; images accumulate on the device.  Inputs must be
  * resident (rtm_session_set_gather for mode 1). */
 int rtm_session_run(rtm_session *ss, rtm_stats *stats);
+/* Migrate shots [k0, k0+n) only (batches of the session's batch size); images accumulate. */
+int rtm_session_run_range(rtm_session *ss, int k0, int n, rtm_stats *stats);
+/* Mode 0 only: model every shot's gather (forward pass with receiver sampling; no
+ * migration), the reference's modelling pass (rtm_model.cu:266-290). */
+int rtm_session_model(rtm_session *ss);
+/* Device pointers of the stacked images (nz*nx, float or double per accum_fp64), for
+ * reductions across GPUs; valid until rtm_session_close. */
+int rtm_session_image_ptrs(rtm_session *ss, void **image1, void **image2s, void **image2m, void **illum);
 /* Mode 0: copy shot k's modelled (unmuted) gather to the host, [nt][nrec_k]. */
 int rtm_session_get_gather(rtm_session *ss, int k, float *gather);
 /* Copy the stacked images (nz*nx each; any pointer may be NULL). */

@@ -1,0 +1,254 @@
+"""CUDA path (librtm_b200.so, through its C-ABI) against the reference's own output (golden
+fixtures) and against the CPU oracle.
+
+Tolerances (FP32 stencil): gathers and images within 1e-4 rel-L2 of the
+reference / oracle; the reduced-precision forms (fp16/bf16 strips and gathers, fp64
+accumulation) within 1e-3 rel-L2 of the FP64 oracle.  PML profiles and source/receiver
+indices are checked bit-exact.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_case, rel_l2, survey_from_case
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-4
+TOL_MIXED = 1e-3
+
+
+def cfg_from(G, s):
+    return G.SurveyConfig(**s)
+
+
+def golden_run(G, name, options=None):
+    z, prm = load_case(name)
+    s = survey_from_case(prm)
+    shots = list(range(1, prm["nshot"] + 1))
+    gathers = None
+    if prm["mode"] == 1:
+        src, _ = load_case(prm["data_from"])
+        gathers = [src[f"gather{i}"] for i in shots]
+    out = G.migrate(cfg_from(G, s), options or G.RunOptions(), shots, z["vp0"], z["rho0"], gathers=gathers)
+    return z, prm, out
+
+
+@pytest.mark.parametrize("name", ["caseB", "caseC", "caseD"])
+def test_images_match_reference(rtmlib, name):
+    z, prm, out = golden_run(rtmlib, name)
+    for k in ("image1", "image2s", "image2m", "illum"):
+        assert rel_l2(out[k], z[k]) < TOL_FP32, (k, rel_l2(out[k], z[k]))
+    if prm["mode"] == 0:
+        for i in range(1, prm["nshot"] + 1):
+            assert rel_l2(out["gathers"][i - 1], z[f"gather{i}"]) < TOL_FP32
+
+
+def test_forward_matches_reference_steps(rtmlib):
+    """300 forward steps against the reference's 9-launch step (golden units run)."""
+    z = np.load(os.path.join(GOLDEN, "ref_units.npz"))
+    nxl, nzl, npml, dx, dz, dt, fdom, nt, nsx, nsz, amp, alp = z["units_meta"]
+    nxl, nzl, npml, nt, nsx, nsz = map(int, (nxl, nzl, npml, nt, nsx, nsz))
+    nsteps = int(z["units_meta2"][2])
+    sv = rtmlib.SurveyConfig(nx=nxl, nz=nzl, nt=nt, dx=float(dx), dz=float(dz), dt=float(dt), npml=npml,
+                             fdom=float(fdom), amp=float(amp), alp=float(alp), layout=2,
+                             spx0=(nsx - npml) * float(dx), spz0=(nsz - npml) * float(dz), mode=0)
+    g = rtmlib.geometry(sv, 1)
+    assert (g.nsx, g.nsz) == (nsx, nsz)
+    v = z["model_v"].reshape(nzl, nxl)
+    r = z["model_rho"].reshape(nzl, nxl)
+    p, vx, vz, gat = rtmlib.forward(sv, rtmlib.RunOptions(), 1, v, r, nsteps)
+    X, Z = nxl + 2 * npml, nzl + 2 * npml
+    assert rel_l2(p, z["fwd_p"].reshape(Z, X)) < TOL_FP32
+    assert rel_l2(vx, z["fwd_vx"].reshape(Z, X - 1)) < TOL_FP32
+    assert rel_l2(vz, z["fwd_vz"].reshape(Z - 1, X)) < TOL_FP32
+    assert rel_l2(gat, z["fwd_gather"].reshape(nsteps, nxl)) < TOL_FP32
+
+
+def _random_model(nz, nx, seed):
+    rng = np.random.default_rng(seed)
+    zz = np.arange(nz)[:, None] * 10.0
+    v = 1800 + 0.9 * zz + 150 * rng.random((nz, nx))
+    v[nz // 2:, :] += 500
+    rho = 1900 + 200 * rng.random((nz, nx))
+    return v.astype(np.float32), rho.astype(np.float32)
+
+
+GENERAL = [
+    # general npml, sizes that leave partial tiles, receivers below z = 0, constant density
+    dict(nx=77, nz=45, nt=260, npml=40, layout=2, spx0=300.0, spz0=20.0, dspx=200.0, nshot=2, rdepth=0,
+         rho="const", fdom=25.0, alp=0.1),
+    dict(nx=101, nz=53, nt=240, npml=13, layout=2, spx0=150.0, spz0=35.0, dspx=330.0, nshot=2, rdepth=3,
+         rho="var", fdom=25.0, alp=0.06),
+    # bilateral apertures of different widths in one batch, PML smoothing, ismth reconstruction
+    dict(nx=150, nz=41, nt=220, npml=24, layout=1, spx0=100.0, spz0=20.0, dspx=450.0, nshot=3, rdepth=0,
+         rho="var", offsetmax=900.0, medium_flag=1, ismth=2, fdom=25.0, alp=0.1),
+    # unilateral layouts with a minimum offset
+    dict(nx=120, nz=40, nt=200, npml=20, layout=3, spx0=60.0, spz0=20.0, dspx=300.0, nshot=2, rdepth=0,
+         rho="const", offset=50.0, offsetmax=600.0, fdom=25.0, alp=0.1),
+    dict(nx=120, nz=40, nt=200, npml=20, layout=4, spx0=700.0, spz0=20.0, dspx=300.0, nshot=2, rdepth=0,
+         rho="const", offset=50.0, offsetmax=600.0, fdom=25.0, alp=0.1),
+]
+
+
+def _survey(c, mode):
+    return dict(nx=c["nx"], nz=c["nz"], nt=c["nt"], dx=10.0, dz=10.0, dt=float(np.float32(1e-3)), npml=c["npml"],
+                fdom=c["fdom"], amp=1.0, alp=c["alp"], layout=c["layout"], spx0=c["spx0"], spz0=c["spz0"],
+                dspx=c["dspx"], offset=c.get("offset", 0.0), offsetmax=c.get("offsetmax", 0.0), mode=mode,
+                medium_flag=c.get("medium_flag", 0), ismth=c.get("ismth", 0), direct=1.5, direct0=0.0, mute=1,
+                receiver_depth=c["rdepth"])
+
+
+@pytest.mark.parametrize("ci", range(len(GENERAL)))
+def test_rtm_matches_oracle_general(rtmlib, oracle, ci):
+    c = GENERAL[ci]
+    v, rho = _random_model(c["nz"], c["nx"], ci)
+    if c["rho"] == "const":
+        rho = np.full_like(rho, 2000.0)
+    shots = list(range(1, c["nshot"] + 1))
+    s = _survey(c, 0)
+    ref = oracle.rtm_model(s, shots, v, rho)
+    out = rtmlib.migrate(cfg_from(rtmlib, s), rtmlib.RunOptions(), shots, v, rho)
+    for k in range(len(shots)):
+        assert rel_l2(out["gathers"][k], ref["gathers"][k]) < TOL_FP32
+    for k in ("image1", "image2s", "illum"):
+        assert rel_l2(out[k], ref[k]) < TOL_FP32, (k, rel_l2(out[k], ref[k]))
+    # mode 1 on the modelled data with a smoothed migration model
+    vm = oracle.velsmooth(v, 3)
+    s1 = _survey(c, 1)
+    ref1 = oracle.rtm_model(s1, shots, vm, rho, gathers=ref["gathers"])
+    out1 = rtmlib.migrate(cfg_from(rtmlib, s1), rtmlib.RunOptions(), shots, vm, rho, gathers=ref["gathers"])
+    for k in ("image1", "image2s", "illum"):
+        assert rel_l2(out1[k], ref1[k]) < TOL_FP32, (k, rel_l2(out1[k], ref1[k]))
+
+
+def test_batching_is_bitwise_invariant(rtmlib):
+    """A batch of uneven apertures in one launch gives exactly the per-shot results."""
+    c = GENERAL[2]
+    v, rho = _random_model(c["nz"], c["nx"], 7)
+    s = cfg_from(rtmlib, _survey(c, 0))
+    shots = [1, 2, 3]
+    a = rtmlib.migrate(s, rtmlib.RunOptions(batch=1), shots, v, rho)
+    b = rtmlib.migrate(s, rtmlib.RunOptions(batch=3), shots, v, rho)
+    for k in ("image1", "image2s", "illum"):
+        assert np.array_equal(a[k], b[k]), k
+    for ga, gb in zip(a["gathers"], b["gathers"]):
+        assert np.array_equal(ga, gb)
+    assert a["stats"].batches == 3 and b["stats"].batches == 1
+
+
+@pytest.mark.parametrize("strips,gathers,fp64", [("fp16", "fp16", True), ("bf16", "bf16", True),
+                                                 ("fp16", "fp32", False), ("fp32", "fp32", True)])
+def test_precision_forms_against_fp64_oracle(rtmlib, oracle, strips, gathers, fp64):
+    c = GENERAL[0]
+    v, rho = _random_model(c["nz"], c["nx"], 11)
+    shots = [1, 2]
+    s0 = _survey(c, 0)
+    data = oracle.rtm_model(s0, shots, v, rho)["gathers"]
+    vm = oracle.velsmooth(v, 3)
+    s1 = _survey(c, 1)
+    ref64 = oracle.rtm_model(s1, shots, vm, rho, gathers=data, precision="f64")
+    out = rtmlib.migrate(cfg_from(rtmlib, s1), rtmlib.RunOptions(strip_precision=strips, gather_precision=gathers,
+                                                                 accum_fp64=fp64), shots, vm, rho, gathers=data)
+    tol = TOL_MIXED if (strips != "fp32" or gathers != "fp32") else TOL_FP32
+    if strips == "bf16":
+        tol = 2e-2   # 8-bit mantissa storage; reported, not the north-star form
+    for k in ("image1", "image2s", "illum"):
+        err = rel_l2(out[k], ref64[k])
+        assert err < tol, (k, err)
+    if fp64:
+        f = out["f64"]
+        assert rel_l2(f["image2s"], ref64["image2s"]) < tol
+
+
+def test_reconstructed_source_wavefield_drift(rtmlib, oracle):
+    """The fp16 boundary strips perturb the reconstructed source wavefield only slightly."""
+    c = GENERAL[0]
+    v, rho = _random_model(c["nz"], c["nx"], 12)
+    s = rtmlib.SurveyConfig(**_survey(c, 0))
+    res = {}
+    for prec in ("fp32", "fp16"):
+        with rtmlib.Session(s, rtmlib.RunOptions(strip_precision=prec, batch=1), [1], v, rho) as ss:
+            ss.run()
+            g = rtmlib.geometry(s, 1)
+            res[prec] = ss.wavefields(0, g.nxpad, g.nzpad)[0]
+    npml = c["npml"]
+    inner = (slice(npml, -npml), slice(npml, -npml))
+    drift = rel_l2(res["fp16"][inner], res["fp32"][inner])
+    assert drift < 1e-3, drift
+
+
+def test_dropin_rtm_model_writes_reference_files(rtmlib, tmp_path):
+    """rtm_model() with the reference's argument list: mode 0 writes the gathers the
+    reference wrote (byte for byte in the headers), mode 1 reads them back; the images match
+    the reference's."""
+    z, prm = load_case("caseB")
+    zc, prmc = load_case("caseC")
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        os.makedirs("seisReal")
+        os.makedirs("output")
+        nx, nz = prm["nx"], prm["nz"]
+        imgs = [np.zeros((nz, nx), np.float32) for _ in range(10)]
+        coef = rtmlib.coef_table()
+        wl = np.zeros(prm["nt"], np.float32)
+        L = rtmlib.lib()
+        f = lambda x: C.c_float(float(x))
+
+        def call(p, vp, rho):
+            L.rtm_model(0, p["nshot"], 1, 1, p["mode"], p["medium_flag"], p["layout"], 0, 0, p["ismth"], nx, nz,
+                        p["nt"], f(p["dx"]), f(p["dx"]), f(p["dt"]), p["npml"], f(p["direct"]), f(p["direct0"]),
+                        f(0.25), f(p["fdom"]), f(p["spx0"]), f(p["spz0"]), f(p["dspx"]), f(p["offset"]),
+                        f(p["offsetmax"]), f(p["amp"]), f(p["alp"]), vp.ctypes.data_as(C.c_void_p),
+                        rho.ctypes.data_as(C.c_void_p), coef.ctypes.data_as(C.c_void_p),
+                        wl.ctypes.data_as(C.c_void_p), *[a.ctypes.data_as(C.c_void_p) for a in imgs])
+            assert L.rtm_last_error() == b""
+
+        call(prm, np.ascontiguousarray(z["vp0"]), np.ascontiguousarray(z["rho0"]))
+        for i in (1, 2):
+            raw = np.fromfile(f"seisReal/{i}seisreal.su", np.uint8).reshape(prm["nx"], 240 + 4 * prm["nt"])
+            assert np.array_equal(raw[:, :240], z[f"gather{i}_headers"])
+            data = raw[:, 240:].copy().view(np.float32).reshape(prm["nx"], prm["nt"]).T
+            assert rel_l2(data, z[f"gather{i}"]) < TOL_FP32
+        assert rel_l2(imgs[0], z["image1"]) < TOL_FP32
+        assert rel_l2(imgs[1], z["image2s"]) < TOL_FP32
+        assert rel_l2(imgs[9], z["illum"]) < TOL_FP32
+        hdr = np.fromfile("output/Image1temp.su", np.uint8)
+        assert np.array_equal(hdr[:240], z["image_su_header0"]) and hdr.size == z["image_su_bytes"][0]
+        # mode 1 reads ./seisReal written above (the reference's own caseC run did the same)
+        call(prmc, np.ascontiguousarray(zc["vp0"]), np.ascontiguousarray(zc["rho0"]))
+        assert rel_l2(imgs[1], zc["image2s"]) < TOL_FP32
+        assert rel_l2(imgs[0], zc["image1"]) < TOL_FP32
+    finally:
+        os.chdir(cwd)
+
+
+def test_edge_cases(rtmlib, oracle):
+    v, rho = _random_model(30, 40, 3)
+    base = dict(nx=40, nz=30, nt=2, dx=10.0, dz=10.0, dt=float(np.float32(1e-3)), npml=10, fdom=25.0, amp=1.0,
+                alp=0.1, layout=2, spx0=200.0, spz0=20.0, dspx=0.0, mode=0, direct=1.5, direct0=0.0)
+    # minimum time axis and minimum PML width
+    out = rtmlib.migrate(rtmlib.SurveyConfig(**base), rtmlib.RunOptions(), [1], v, rho)
+    ref = oracle.rtm_model(dict(base, offset=0.0, offsetmax=0.0, medium_flag=0, ismth=0, mute=1, receiver_depth=0),
+                           [1], v, rho)
+    assert rel_l2(out["gathers"][0], ref["gathers"][0]) < TOL_FP32
+    # zero amplitude: everything stays exactly zero
+    out = rtmlib.migrate(rtmlib.SurveyConfig(**dict(base, nt=50, amp=0.0)), rtmlib.RunOptions(), [1], v, rho)
+    assert not out["image1"].any() and not out["gathers"][0].any()
+    # source Gaussian wide enough to cover the whole grid (alp = 0 -> flat source)
+    s = dict(base, nt=40, alp=0.0)
+    out = rtmlib.migrate(rtmlib.SurveyConfig(**s), rtmlib.RunOptions(), [1], v, rho)
+    ref = oracle.rtm_model(dict(s, offset=0.0, offsetmax=0.0, medium_flag=0, ismth=0, mute=1, receiver_depth=0),
+                           [1], v, rho)
+    assert rel_l2(out["gathers"][0], ref["gathers"][0]) < TOL_FP32
+    # mode 1 without data is an error, not a crash
+    with pytest.raises(rtmlib.RtmError, match="gather"):
+        with rtmlib.Session(rtmlib.SurveyConfig(**dict(base, mode=1)), rtmlib.RunOptions(), [1], v, rho) as ss:
+            ss.run()
+    # a survey larger than the device is refused up front (strips of 10^8 steps, ~1 TB)
+    big = dict(base, nt=100_000_000)
+    with pytest.raises(rtmlib.RtmError, match="device memory"):
+        rtmlib.Session(rtmlib.SurveyConfig(**big), rtmlib.RunOptions(), [1], v, rho)
