@@ -139,21 +139,23 @@ def ncu_traffic_per_unit(kernel: str):
 def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int) -> float:
     """Algorithmic DRAM bytes of one launch of `kind` for one shot: every array the kernel
     must read or write, once (4-byte fields; PML split fields excluded as thin bands).
-      vel_*:  read p, 1/rho; read+write vx, vz                  -> 24 B per padded cell
-      pres_*: read vx, vz, kappa; read+write p                  -> 20 B per padded cell
-      backward kernels add the interior reconstruction (vel: read ps, rw vxs, vzs = 20 B;
-      pres: read vxs, vzs, rw ps = 16 B) and pres_bwd the imaging (rw g1, illum)."""
+      vel_fwd, vel_recv:   read p, 1/rho; read+write vx, vz            24 B per padded cell
+      pres_fwd, pres_recv: read vx, vz, kappa; read+write p            20 B per padded cell
+      vel_recon:  read ps, 1/rho; read+write vxs, vzs on the interior  24 B per interior cell
+      pres_recon: read vxs, vzs, kappa; read+write ps on the interior  20 B per interior cell
+      pres_recv adds the imaging: read ps, read+write g1 and illum     4 + 4*accum B per interior cell
+    plus the boundary strips each kernel writes (forward) or reads (reconstruction)."""
     cells, inner = X * Z, nxi * nzi
-    strips = 80 * (nxi + nzi)   # one kernel writes or reads half of the 40*(nxi+nzi) fp32 strips
-    if kind == "vel_fwd":
-        return 24 * cells + strips
-    if kind == "pres_fwd":
-        return 20 * cells + strips
-    if kind == "vel_bwd":
-        return 24 * cells + 20 * inner + strips
-    if kind == "pres_bwd":
-        return 20 * cells + 16 * inner + 4 * accum_bytes * inner + strips + 4 * nrec
-    raise ValueError(kind)
+    strips = 80 * (nxi + nzi)   # vx+vz or p strips of one step, fp32
+    table = {
+        "vel_fwd": 24 * cells + strips,
+        "pres_fwd": 20 * cells + strips,
+        "vel_recon": 24 * inner + strips,
+        "pres_recon": 20 * inner + strips,
+        "vel_recv": 24 * cells,
+        "pres_recv": 20 * cells + (4 + 4 * accum_bytes) * inner + 4 * nrec,
+    }
+    return table[kind]
 
 
 class _CudaArray:
@@ -240,7 +242,7 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
-    kern = {k: ss.kernel_ms(k) for k in ("vel_fwd", "pres_fwd", "vel_bwd", "pres_bwd")}
+    kern = {k: ss.kernel_ms(k) for k in ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv")}
     if args.profile_only:
         ss.close()
         return None

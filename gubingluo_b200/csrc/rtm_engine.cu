@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -90,9 +91,12 @@ struct rtm_session {
     int B = 0;                       // batch size (slots)
     int maxX = 0, maxPitch = 0, Z = 0;
     float *wavelet = nullptr, *coef = nullptr;
+    float coef_host[100];
     void *img1 = nullptr, *img2s = nullptr, *img2m = nullptr, *illum = nullptr;
     ShotDev *d_shots = nullptr;
-    TileRef *d_tiles = nullptr;
+    TileRef *d_tiles = nullptr;      // (shot, tile) list of the velocity kernels
+    TileRef *d_tiles_p = nullptr;    // (shot, tile) list of the pressure kernels
+    int bz_vel = 32, bz_pres = 32;   // rows per tile of the two stencil kernels
     void *d_fin = nullptr;
     int max_tiles = 0;
     std::map<std::string, rtm::KernelTiming> timing;
@@ -235,6 +239,12 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     if (fixed + per_slot > budget) return fail(RTM_ERR_NOMEM, "survey does not fit in device memory");
     int B = (int)std::min<size_t>((size_t)nshots, (budget - fixed) / per_slot);
     if (o.batch > 0) B = std::min(B, o.batch);
+    {
+        const char *e = std::getenv("RTM_B200_BZ_VEL");
+        if (e && *e) ss->bz_vel = std::atoi(e);
+        e = std::getenv("RTM_B200_BZ_PRES");
+        if (e && *e) ss->bz_pres = std::atoi(e);
+    }
     B = std::max(B, 1);
     ss->B = B;
     size_t arena_bytes = fixed + (size_t)B * per_slot;
@@ -251,6 +261,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     float ctab[100];
     if (diffcoef) std::memcpy(ctab, diffcoef, sizeof(ctab));
     else coef_table(ctab);
+    std::memcpy(ss->coef_host, ctab, sizeof(ctab));
     CK(cudaMemcpyAsync(ss->coef, ctab, sizeof(ctab), cudaMemcpyHostToDevice, ss->stream));
     CK(cudaStreamSynchronize(ss->stream));
     // stacked images
@@ -345,11 +356,13 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     }
     // descriptor and tile tables
     ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
-    int tiles_per_shot = ((big.X + RTM_TX - 1) / RTM_TX) * ((big.Z + RTM_TZ - 1) / RTM_TZ);
+    int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + 15) / 16);
     ss->max_tiles = tiles_per_shot * B;
     ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
+    ss->d_tiles_p = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_fin = ss->arena.take(finalize_shot_size() * B);
-    if (!ss->d_shots || !ss->d_tiles || !ss->d_fin) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
+    if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_fin)
+        return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     CK(cudaStreamSynchronize(ss->stream));
     return RTM_OK;
 }
@@ -402,7 +415,7 @@ static void timing_end(rtm_session *ss, cudaEvent_t ev)
 
 // Batch state shared by the phases of one batch.
 struct BatchRun {
-    int k0 = 0, n = 0, ntiles = 0, maxrec = 0;
+    int k0 = 0, n = 0, ntiles = 0, ntiles_p = 0, maxrec = 0;
     std::vector<ShotDev> hd;
     StepArgs a{};
 };
@@ -417,7 +430,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.k0 = k0;
     br.n = n;
     br.hd.assign(n, ShotDev{});
-    std::vector<TileRef> tiles;
+    std::vector<TileRef> tiles, tiles_p;
     br.maxrec = 0;
     for (int j = 0; j < n; j++) {
         ShotState &sh = ss->shots[k0 + j];
@@ -429,7 +442,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         d.nsx = sh.g.nsx; d.nsz = sh.g.nsz;
         d.sbx0 = sh.sbx0; d.sbz0 = sh.sbz0; d.sbnx = sh.sbnx; d.sbnz = sh.sbnz;
         d.rz = sh.g.rz; d.rx0 = sh.g.rx0; d.nrec = sh.g.nrec;
-        d.ntx = (sh.X + RTM_TX - 1) / RTM_TX;
+        d.ntx = (sh.X + RTM_BX - 1) / RTM_BX;
         d.strip_len = sh.strip_len;
         d.inv_rho_f = sh.mf.inv_rho; d.kappa_f = sh.mf.kappa;
         d.inv_rho_b = sh.mb.inv_rho; d.kappa_b = sh.mb.kappa;
@@ -439,8 +452,9 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         d.gather = s.mode == 0 ? sh.gather_raw : sh.gather32;
         d.gather_scale = nullptr;
         d.g1 = sl.g1; d.illum = sl.illum;
-        int ntz = (sh.Z + RTM_TZ - 1) / RTM_TZ;
-        for (int t = 0; t < d.ntx * ntz; t++) tiles.push_back({j, t});
+        const int ntzv = (sh.Z + ss->bz_vel - 1) / ss->bz_vel, ntzp = (sh.Z + ss->bz_pres - 1) / ss->bz_pres;
+        for (int t = 0; t < d.ntx * ntzv; t++) tiles.push_back({j, t});
+        for (int t = 0; t < d.ntx * ntzp; t++) tiles_p.push_back({j, t});
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
         float *f[10] = {sl.a.p, sl.a.vx, sl.a.vz, sl.a.sx, sl.a.sz, sl.b.p, sl.b.vx, sl.b.vz, sl.b.sx, sl.b.sz};
@@ -450,14 +464,17 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         CK(cudaMemsetAsync(sl.illum, 0, ib, st));
     }
     br.ntiles = (int)tiles.size();
+    br.ntiles_p = (int)tiles_p.size();
     CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles, tiles.data(), sizeof(TileRef) * br.ntiles, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ss->d_tiles_p, tiles_p.data(), sizeof(TileRef) * br.ntiles_p, cudaMemcpyHostToDevice, st));
     StepArgs &a = br.a;
     std::memset(&a, 0, sizeof(a));
     a.shots = ss->d_shots;
     a.tiles = ss->d_tiles;
     a.wavelet = ss->wavelet;
     a.coef = ss->coef;
+    for (int i = 0; i < 10; i++) a.c10[i] = ss->coef_host[90 + i];
     a.dt = s.dt;
     a.dtx = s.dt / s.dx;   // rtm_model.cu:73-74
     a.dtz = s.dt / s.dz;
@@ -482,12 +499,15 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
     for (int it = 0; it < nsteps; it++) {
         a.it = it;
         a.ring = it % kRing;
+        const int mode = save ? RTM_WAVE_FWD_SAVE : RTM_WAVE_FWD;
         cudaEvent_t e;
         timing_begin(ss, "vel_fwd", it, &e);
-        launch_vel_fwd(a, br.ntiles, save ? 1 : 0, st);
+        a.tiles = ss->d_tiles;
+        launch_vel(mode, ss->bz_vel, a, br.ntiles, st);
         timing_end(ss, e);
         timing_begin(ss, "pres_fwd", it, &e);
-        launch_pres_fwd(a, br.ntiles, save ? 1 : 0, record ? 1 : 0, st);
+        a.tiles = ss->d_tiles_p;
+        launch_pres(mode, ss->bz_pres, a, br.ntiles_p, record ? 1 : 0, st);
         timing_end(ss, e);
         ss->launches += 2;
         if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
@@ -538,13 +558,25 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     for (int it = s.nt - 2; it >= 0; it--) {
         a.it = it;
         cudaEvent_t e;
-        timing_begin(ss, "vel_bwd", it, &e);
-        launch_vel_bwd(a, br.ntiles, st);
+        // reconstruction of the source wavefield, then the receiver wavefield and imaging
+        // (which reads the reconstructed pressure of the same step)
+        timing_begin(ss, "vel_recon", it, &e);
+        a.tiles = ss->d_tiles;
+        launch_vel(RTM_WAVE_RECON, ss->bz_vel, a, br.ntiles, st);
         timing_end(ss, e);
-        timing_begin(ss, "pres_bwd", it, &e);
-        launch_pres_bwd(a, br.ntiles, st);
+        timing_begin(ss, "pres_recon", it, &e);
+        a.tiles = ss->d_tiles_p;
+        launch_pres(RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_p, 0, st);
         timing_end(ss, e);
-        ss->launches += 2;
+        timing_begin(ss, "vel_recv", it, &e);
+        a.tiles = ss->d_tiles;
+        launch_vel(RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles, st);
+        timing_end(ss, e);
+        timing_begin(ss, "pres_recv", it, &e);
+        a.tiles = ss->d_tiles_p;
+        launch_pres(RTM_WAVE_RECEIVER, ss->bz_pres, a, br.ntiles_p, 0, st);
+        timing_end(ss, e);
+        ss->launches += 4;
     }
     CK(cudaGetLastError());
     std::vector<char> fin(finalize_shot_size() * n);

@@ -4,10 +4,10 @@
 
 #include "rtm_types.h"
 
-void launch_vel_fwd(const StepArgs &a, int ntiles, int save, cudaStream_t s);
-void launch_pres_fwd(const StepArgs &a, int ntiles, int save, int record, cudaStream_t s);
-void launch_vel_bwd(const StepArgs &a, int ntiles, cudaStream_t s);
-void launch_pres_bwd(const StepArgs &a, int ntiles, cudaStream_t s);
+// mode: RtmWaveMode; bz: rows per tile (16, 32 or 64); ntiles: length of the (shot, tile)
+// list built for that bz.
+void launch_vel(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s);
+void launch_pres(int mode, int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s);
 void launch_setup_pml(float *pml, int X, int Z, int npml, float dx, float dz, float dt, float vpmax, cudaStream_t s);
 void launch_setup_source(float *src, int sbx0, int sbz0, int sbnx, int sbnz, int nsx, int nsz, float amp, float alp,
                          float dx2, float dz2, float dt, cudaStream_t s);

@@ -16,26 +16,33 @@
 #include <stdint.h>
 
 #define RTM_RADIUS 10
-#define RTM_TX 32        // tile width  (columns) of the stencil kernels
-#define RTM_TZ 32        // tile height (rows)
+#define RTM_BX 128       // stencil tile width: columns (= threads) per block
+
+// What one launch of the stencil kernels updates.
+enum RtmWaveMode {
+    RTM_WAVE_FWD = 0,        // forward propagation, full grid (modelling)
+    RTM_WAVE_FWD_SAVE = 1,   // forward propagation + boundary strips saved (source pass)
+    RTM_WAVE_RECEIVER = 2,   // receiver back-propagation (+ injection; imaging in the p update)
+    RTM_WAVE_RECON = 3       // source-wavefield reconstruction (interior + restored strips)
+};
 
 enum RtmPrecision { RTM_FP32 = 0, RTM_FP16 = 1, RTM_BF16 = 2 };
 
-// Per-shot PML/edge coefficient block, stored contiguously on the device:
-//   c1x[X], c2x[X]      pressure x-part damping  (1,1 outside the x band)
-//   c1vx[X], c2vx[X]    vx damping               (1,1 outside the x band)
-//   c1z[Z], c2z[Z]      pressure z-part damping
-//   c1vz[Z], c2vz[Z]    vz damping
+// Per-shot PML coefficient block, stored contiguously on the device.  The split-field
+// update is f = (c1*f - D)/c2 with c1 = 1 - dt*d/2, c2 = 2 - c1 (reference kernel.cu:596-598);
+// the kernels multiply by ic2 = 1/c2.  Outside the bands c1 = ic2 = 1.
+//   c1x[X], ic2x[X]     pressure x part       c1vx[X], ic2vx[X]   vx
+//   c1z[Z], ic2z[Z]     pressure z part       c1vz[Z], ic2vz[Z]   vz
 // plus the raw profiles ddx[X], ddz[Z], ddxvx[X], ddzvz[Z] (reference kernel.cu:174-269).
 struct PmlOffsets {
-    int c1x, c2x, c1vx, c2vx, c1z, c2z, c1vz, c2vz, ddx, ddz, ddxvx, ddzvz, total;
+    int c1x, ic2x, c1vx, ic2vx, c1z, ic2z, c1vz, ic2vz, ddx, ddz, ddxvx, ddzvz, total;
 };
 
 __host__ __device__ inline PmlOffsets pml_offsets(int X, int Z)
 {
     PmlOffsets o;
-    o.c1x = 0; o.c2x = X; o.c1vx = 2 * X; o.c2vx = 3 * X;
-    o.c1z = 4 * X; o.c2z = 4 * X + Z; o.c1vz = 4 * X + 2 * Z; o.c2vz = 4 * X + 3 * Z;
+    o.c1x = 0; o.ic2x = X; o.c1vx = 2 * X; o.ic2vx = 3 * X;
+    o.c1z = 4 * X; o.ic2z = 4 * X + Z; o.c1vz = 4 * X + 2 * Z; o.ic2vz = 4 * X + 3 * Z;
     o.ddx = 4 * X + 4 * Z; o.ddz = 5 * X + 4 * Z; o.ddxvx = 5 * X + 5 * Z; o.ddzvz = 6 * X + 5 * Z;
     o.total = 6 * X + 6 * Z;
     return o;
@@ -51,7 +58,7 @@ struct ShotDev {
     int nsx, nsz;
     int sbx0, sbz0, sbnx, sbnz;   // source stamp box (padded coordinates) and its size
     int rz, rx0, nrec;
-    int ntx;                      // tiles along x
+    int ntx;                      // tiles along x (RTM_BX columns each)
     int strip_len;                // 40*(nxi+nzi)
     const float *inv_rho_f, *kappa_f;   // forward (source-pass) model
     const float *inv_rho_b, *kappa_b;   // backward (reconstruction + receiver) model
@@ -78,6 +85,7 @@ struct StepArgs {
     const TileRef *tiles;
     const float *wavelet;   // [nt]
     const float *coef;      // [10][10] zero-padded Liu-Yang table
+    float c10[10];          // full-order (half-order 10) coefficients, read from the constant bank
     float dt, dtx, dtz;
     int it;                 // time index
     int strip_prec, gather_prec, accum_fp64;
