@@ -1,12 +1,14 @@
 // rtm_stencil.cu — the time-step kernels of the RTM hot path (sm_100a).
 //
 // One launch updates one wavefield of every shot of a batch: a flat (shot, tile) work list
-// maps each 128-thread block to a BX x BZ tile of one shot.  Each thread owns one grid
-// column x and marches down the tile's BZ rows:
+// maps each 64-thread block to a BX x BZ tile (128 columns) of one shot.  Each thread owns
+// two adjacent grid columns and marches down the tile's BZ rows:
 //   * the tile and its halo are staged once into shared memory with 16-byte cp.async copies
-//     (zero-filled outside the grid), so every global access is a coalesced 128-byte row;
-//   * x-derivatives read the staged row; z-derivatives read a 20-deep register queue that
-//     the unrolled march rotates without moves (one shared load per row);
+//     (zero-filled outside the grid), so every global access is a coalesced row segment;
+//   * x-derivatives of both columns read 11 8-byte shared words of the staged row;
+//     z-derivatives read two 20-deep register queues that the unrolled march rotates without
+//     moves (one 8-byte shared load per row);
+//   * the per-cell operands of the next row are loaded before the current row is stored;
 //   * the full-order coefficients come from the kernel-parameter constant bank; the reduced
 //     local orders of the outer ten cells (reference cuda_norder*, kernel.cu:271-317) use
 //     rows of the zero-padded coefficient table;
@@ -24,7 +26,8 @@
 
 namespace {
 
-constexpr int BX = RTM_BX;         // threads (= columns) per block
+constexpr int BX = RTM_BX;         // columns per tile
+constexpr int NT = BX / 2;         // threads per block (two adjacent columns each)
 constexpr int WW = BX + 24;        // staged width: columns x0-12 .. x0+BX+11 (16-byte aligned)
 constexpr int R = RTM_RADIUS;
 constexpr int QL = 20;             // register queue length (stencil taps along z)
@@ -48,7 +51,7 @@ template <int NR, int NC>
 __device__ __forceinline__ void stage(float *s, const float *__restrict__ f, int pitch, int zrows, int r0, int c0)
 {
     constexpr int N4 = NC / 4;
-    for (int i = threadIdx.x; i < NR * N4; i += BX) {
+    for (int i = threadIdx.x; i < NR * N4; i += NT) {
         const int r = i / N4, c = (i - r * N4) * 4;
         const int z = r0 + r, x = c0 + c;
         const bool ok = (unsigned)z < (unsigned)zrows && (unsigned)x < (unsigned)pitch;
@@ -103,6 +106,20 @@ __device__ __forceinline__ int strip_row_tb(int z, int npml, int first, int nxi)
     return -1;
 }
 
+// Damped or undamped update f' = (c1*f - d)*ic2; outside the PML c1 = ic2 = 1, which makes
+// this exactly f - d.
+__device__ __forceinline__ float damp(float f, float d, float c1, float ic2) { return (c1 * f - d) * ic2; }
+
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void st2(float *p, float a, float b, bool va, bool vb)
+{
+    if (va && vb) *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+    else {
+        if (va) p[0] = a;
+        if (vb) p[1] = b;
+    }
+}
+
 }  // namespace
 
 // =====================================================================================
@@ -110,118 +127,186 @@ __device__ __forceinline__ int strip_row_tb(int z, int npml, int first, int nxi)
 // (backward model), full grid; 3: reconstruction of the source wavefield (interior only,
 // vx/vz strips of step it+1 restored).
 template <int BZ, int MODE>
-__global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
+__global__ void __launch_bounds__(NT) k_vel(const StepArgs a)
 {
     constexpr int WH = BZ + 19;   // staged rows z0-9 .. z0+BZ+9
     extern __shared__ __align__(16) float sw[];
     __shared__ float s_tab[100];
+    __shared__ float s_c1vz[BZ], s_ic2vz[BZ];
     const TileRef t = a.tiles[blockIdx.x];
-    const ShotDev &S = a.shots[t.shot];
+    const ShotDev S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
     const int x0 = (t.tile % S.ntx) * BX, z0 = (t.tile / S.ntx) * BZ;
     if (MODE == 3 && (z0 + BZ <= npml - R || z0 >= Z - npml + R || x0 + BX <= npml - R || x0 >= X - npml + R))
         return;   // tile outside the reconstruction region (interior + strips)
     const WaveDev W = (MODE == 2) ? S.b : S.a;
     const float *__restrict__ inv_rho = (MODE >= 2) ? S.inv_rho_b : S.inv_rho_f;
+    const PmlOffsets o = pml_offsets(X, Z);
     stage<WH, WW>(sw, W.p, pitch, Z, z0 - 9, x0 - 12);
-    if (threadIdx.x < 100) s_tab[threadIdx.x] = a.coef[threadIdx.x];
+    for (int i = threadIdx.x; i < 100; i += NT) s_tab[i] = a.coef[i];
+    for (int i = threadIdx.x; i < BZ; i += NT) {
+        const int z = min(z0 + i, Z - 2);
+        s_c1vz[i] = S.pml[o.c1vz + z];
+        s_ic2vz[i] = S.pml[o.ic2vz + z];
+    }
     cp_wait_all();
     __syncthreads();
-    const int tx = threadIdx.x, x = x0 + tx;
-    if (x >= X) return;   // no barrier below
+    const int tx = threadIdx.x, xa = x0 + 2 * tx;   // columns xa, xa+1
+    if (xa >= X) return;   // no barrier below
 
-    const PmlOffsets o = pml_offsets(X, Z);
     const int nzi = S.nzi, nxi = S.nxi;
-    // per-column constants: vx order, coefficients and damping
-    const bool has_vx = x < X - 1;
-    const int rx = max(min(min(x + 1, X - 1 - x), R), 1);
-    float cx[R];
+    float *__restrict__ vxp = W.vx;
+    float *__restrict__ vzp = W.vz;
+    // per-column constants
+    bool hvx[2], hvz[2], rvx[2], rvz[2];
+    float c1vx[2], ic2vx[2];
+    int svx[2], svz[2];
+    bool edge_order = false;
 #pragma unroll
-    for (int i = 0; i < R; i++) cx[i] = (rx == R) ? a.c10[i] : s_tab[(rx - 1) * R + i];
-    const bool bandvx = (x < npml) || (x >= X - npml - 1);
-    const float c1vx = bandvx ? S.pml[o.c1vx + x] : 1.0f;
-    const float ic2vx = bandvx ? S.pml[o.ic2vx + x] : 1.0f;
-    const int svx_col = strip_col_vx(x, X, npml, nzi);
-    const int svz_col = (x >= npml && x < X - npml) ? x - npml : -1;
-    const bool rec_vx_col = (x >= npml && x <= X - npml - 2);
-    const bool rec_vz_col = (x >= npml && x < X - npml);
-    const size_t vstrip = 2 * (size_t)R * nzi;   // offset of the vz strips
+    for (int c = 0; c < 2; c++) {
+        const int x = xa + c;
+        hvz[c] = x < X;
+        hvx[c] = x < X - 1;
+        edge_order |= hvx[c] && (x < R - 1 || x > X - R - 1);
+        const bool band = (x < npml) || (x >= X - npml - 1);
+        c1vx[c] = (band && hvx[c]) ? S.pml[o.c1vx + x] : 1.0f;
+        ic2vx[c] = (band && hvx[c]) ? S.pml[o.ic2vx + x] : 1.0f;
+        svx[c] = hvx[c] ? strip_col_vx(x, X, npml, nzi) : -1;
+        svz[c] = (x >= npml && x < X - npml) ? x - npml : -1;
+        rvx[c] = (x >= npml && x <= X - npml - 2);
+        rvz[c] = (x >= npml && x < X - npml);
+    }
+    // vx coefficient rows of the two columns (the reduced orders of the outer ten columns)
+    const float *cx0 = &s_tab[(max(min(min(xa + 1, X - 1 - xa), R), 1) - 1) * R];
+    const float *cx1 = &s_tab[(max(min(min(xa + 2, X - 2 - xa), R), 1) - 1) * R];
+    const size_t vstrip = 2 * (size_t)R * nzi;
     const size_t sbase_next = (size_t)(a.it + 1) * S.strip_len;
+    const float dtx = a.dtx, dtz = a.dtz;
 
-    float q[QL];   // q[(u + k) % QL] = p[z - 9 + k][x]
+    float qa[QL], qb[QL];   // q?[(u + k) % QL] = p[z - 9 + k][xa (+1)]
 #pragma unroll
-    for (int k = 0; k < QL - 1; k++) q[k] = sw[k * WW + tx + 12];
-
+    for (int k = 0; k < QL - 1; k++) {
+        const float2 f = ld2(&sw[k * WW + 2 * tx + 12]);
+        qa[k] = f.x;
+        qb[k] = f.y;
+    }
     const int zend = min(z0 + BZ, Z);
+    // operands of the next PF rows (1/rho, vx, vz of both columns): the loads of row z+PF are
+    // issued while row z is computed, so each warp keeps PF rows of loads in flight
+    constexpr int PF = 4;   // divides QL, so the slot of row z is the compile-time u % PF
+    float2 n_ir[PF], n_vx[PF], n_vz[PF];
+    auto load_row = [&](int z, int slot) {
+        const unsigned id = (unsigned)z * pitch + xa;
+        n_ir[slot] = __ldg(reinterpret_cast<const float2 *>(&inv_rho[id]));
+        n_vx[slot] = ld2(&vxp[id]);
+        n_vz[slot] = ld2(&vzp[id]);
+    };
+#pragma unroll
+    for (int k = 0; k < PF; k++)
+        if (z0 + k < zend) load_row(z0 + k, k);
     for (int zb = z0; zb < zend; zb += QL) {
 #pragma unroll
         for (int u = 0; u < QL; u++) {
             const int z = zb + u;
             if (z >= zend) break;
-            q[(u + QL - 1) % QL] = sw[(z - z0 + 19) * WW + tx + 12];
-            const float *row = &sw[(z - z0 + 9) * WW + tx + 12];
-            const size_t id = (size_t)z * pitch + x;
-            // ---------------- vx
-            if (MODE == 3) {
-                const bool zin = (z >= npml && z < Z - npml);
-                if (zin && rec_vx_col) {   // kernel.cu:318-353 (vx += ...)
-                    float d = 0.0f;
-#pragma unroll
-                    for (int i = 1; i <= R; i++) d += a.c10[i - 1] * (row[i] - row[1 - i]);
-                    d = d * a.dtx * __ldg(&inv_rho[id]);
-                    W.vx[id] += d;
-                } else if (zin && svx_col >= 0) {   // read_d_vxpml, kernel.cu:1294-1320
-                    const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 0] : 1.0f;
-                    W.vx[id] = load_strip(S.strips, sbase_next + svx_col + (size_t)(z - npml) * R, a.strip_prec, sc);
-                }
-            } else if (has_vx) {
-                float d = 0.0f;
-#pragma unroll
-                for (int i = 1; i <= R; i++) d += cx[i - 1] * (row[i] - row[1 - i]);
-                d = d * a.dtx * __ldg(&inv_rho[id]);
-                float v = W.vx[id];
-                v = bandvx ? (c1vx * v - d) * ic2vx : v - d;
-                W.vx[id] = v;
-                if (MODE == 1 && svx_col >= 0 && z >= npml && z < Z - npml)
-                    store_strip(a, S, svx_col + (size_t)(z - npml) * R, v);
+            const int slot = u % PF;
+            const float2 ir = n_ir[slot], ov = n_vx[slot], ow = n_vz[slot];
+            if (z + PF < zend) load_row(z + PF, slot);
+            {
+                const float2 f = ld2(&sw[(z - z0 + 19) * WW + 2 * tx + 12]);
+                qa[(u + QL - 1) % QL] = f.x;
+                qb[(u + QL - 1) % QL] = f.y;
             }
-            // ---------------- vz
-            if (z < Z - 1) {
-                if (MODE == 3) {
-                    if (rec_vz_col && z >= npml && z <= Z - npml - 2) {   // kernel.cu:354-388
-                        float d = 0.0f;
+            // v[k] = p[z][xa - 10 + k], k = 0..21
+            float v[22];
+            const float *rw = &sw[(z - z0 + 9) * WW + 2 * tx + 2];
 #pragma unroll
-                        for (int i = 1; i <= R; i++) d += a.c10[i - 1] * (q[(u + 9 + i) % QL] - q[(u + 10 - i) % QL]);
-                        d = d * a.dtz * __ldg(&inv_rho[id]);
-                        W.vz[id] += d;
-                    } else if (svz_col >= 0) {
+            for (int j = 0; j < 11; j++) {
+                const float2 f = ld2(&rw[2 * j]);
+                v[2 * j] = f.x;
+                v[2 * j + 1] = f.y;
+            }
+            float dx0 = 0.f, dx1 = 0.f, dz0 = 0.f, dz1 = 0.f;
+            if (!edge_order) {
+#pragma unroll
+                for (int i = 1; i <= R; i++) {
+                    dx0 += a.c10[i - 1] * (v[10 + i] - v[11 - i]);
+                    dx1 += a.c10[i - 1] * (v[11 + i] - v[12 - i]);
+                }
+            } else {   // outer ten columns: local order (kernel.cu:542-630 with cuda_norderx)
+#pragma unroll
+                for (int i = 1; i <= R; i++) {
+                    dx0 += cx0[i - 1] * (v[10 + i] - v[11 - i]);
+                    dx1 += cx1[i - 1] * (v[11 + i] - v[12 - i]);
+                }
+            }
+            const int rz = min(min(z + 1, Z - 1 - z), R);
+            if (MODE == 3 || rz == R) {
+#pragma unroll
+                for (int i = 1; i <= R; i++) {
+                    dz0 += a.c10[i - 1] * (qa[(u + 9 + i) % QL] - qa[(u + 10 - i) % QL]);
+                    dz1 += a.c10[i - 1] * (qb[(u + 9 + i) % QL] - qb[(u + 10 - i) % QL]);
+                }
+            } else {   // top/bottom ten rows: local order (cuda_norderz)
+                const float *cz = &s_tab[(rz - 1) * R];
+#pragma unroll
+                for (int i = 1; i <= R; i++) {
+                    dz0 += cz[i - 1] * (qa[(u + 9 + i) % QL] - qa[(u + 10 - i) % QL]);
+                    dz1 += cz[i - 1] * (qb[(u + 9 + i) % QL] - qb[(u + 10 - i) % QL]);
+                }
+            }
+            const unsigned id = (unsigned)z * pitch + xa;
+            if (MODE == 3) {
+                // kernel.cu:318-388 (+=) on the interior; strips of step it+1 elsewhere
+                const bool zin = (z >= npml && z < Z - npml);
+                const bool zinv = (z >= npml && z <= Z - npml - 2);
+                float nvx[2] = {ov.x, ov.y}, nvz[2] = {ow.x, ow.y};
+                bool wvx[2] = {false, false}, wvz[2] = {false, false};
+                const float ddx[2] = {dx0, dx1}, ddz[2] = {dz0, dz1}, irr[2] = {ir.x, ir.y};
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    if (zin && rvx[c]) {
+                        nvx[c] += ddx[c] * dtx * irr[c];
+                        wvx[c] = true;
+                    } else if (zin && svx[c] >= 0) {   // read_d_vxpml, kernel.cu:1294-1320
+                        const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 0] : 1.0f;
+                        nvx[c] = load_strip(S.strips, sbase_next + svx[c] + (size_t)(z - npml) * R, a.strip_prec, sc);
+                        wvx[c] = true;
+                    }
+                    if (zinv && rvz[c]) {
+                        nvz[c] += ddz[c] * dtz * irr[c];
+                        wvz[c] = true;
+                    } else if (svz[c] >= 0 && z < Z - 1) {   // read_d_vzpml, kernel.cu:1321-1347
                         const int srow = strip_row_tb(z, npml, Z - npml - 1, nxi);
-                        if (srow >= 0) {   // read_d_vzpml, kernel.cu:1321-1347
+                        if (srow >= 0) {
                             const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 1] : 1.0f;
-                            W.vz[id] = load_strip(S.strips, sbase_next + vstrip + srow + svz_col, a.strip_prec, sc);
+                            nvz[c] = load_strip(S.strips, sbase_next + vstrip + srow + svz[c], a.strip_prec, sc);
+                            wvz[c] = true;
                         }
                     }
-                } else {
-                    const int rz = min(min(z + 1, Z - 1 - z), R);
-                    float d = 0.0f;
-                    if (rz == R) {
-#pragma unroll
-                        for (int i = 1; i <= R; i++) d += a.c10[i - 1] * (q[(u + 9 + i) % QL] - q[(u + 10 - i) % QL]);
-                    } else {
-                        const float *c = &s_tab[(rz - 1) * R];
-#pragma unroll
-                        for (int i = 1; i <= R; i++) d += c[i - 1] * (q[(u + 9 + i) % QL] - q[(u + 10 - i) % QL]);
-                    }
-                    d = d * a.dtz * __ldg(&inv_rho[id]);
-                    float v = W.vz[id];
-                    const bool bandvz = (z < npml) || (z >= Z - npml - 1);
-                    if (bandvz) v = (S.pml[o.c1vz + z] * v - d) * S.pml[o.ic2vz + z];
-                    else v = v - d;
-                    W.vz[id] = v;
-                    if (MODE == 1 && svz_col >= 0) {
-                        const int srow = strip_row_tb(z, npml, Z - npml - 1, nxi);
-                        if (srow >= 0) store_strip(a, S, vstrip + srow + svz_col, v);
-                    }
+                }
+                st2(&vxp[id], nvx[0], nvx[1], wvx[0], wvx[1]);
+                st2(&vzp[id], nvz[0], nvz[1], wvz[0], wvz[1]);
+                continue;
+            }
+            // kernel.cu:430-500 (interior) and :542-713 (PML): f' = (c1*f - d)*ic2
+            const float nvx0 = damp(ov.x, dx0 * dtx * ir.x, c1vx[0], ic2vx[0]);
+            const float nvx1 = damp(ov.y, dx1 * dtx * ir.y, c1vx[1], ic2vx[1]);
+            st2(&vxp[id], nvx0, nvx1, hvx[0], hvx[1]);
+            const bool zv = z < Z - 1;
+            const float c1z = s_c1vz[z - z0], ic2z = s_ic2vz[z - z0];
+            const float nvz0 = damp(ow.x, dz0 * dtz * ir.x, c1z, ic2z);
+            const float nvz1 = damp(ow.y, dz1 * dtz * ir.y, c1z, ic2z);
+            st2(&vzp[id], nvz0, nvz1, zv && hvz[0], zv && hvz[1]);
+            if (MODE == 1) {   // save_d_vxpml / save_d_vzpml, kernel.cu:1186-1239
+                if (z >= npml && z < Z - npml) {
+                    if (svx[0] >= 0) store_strip(a, S, svx[0] + (size_t)(z - npml) * R, nvx0);
+                    if (svx[1] >= 0) store_strip(a, S, svx[1] + (size_t)(z - npml) * R, nvx1);
+                }
+                const int srow = strip_row_tb(z, npml, Z - npml - 1, nxi);
+                if (srow >= 0 && zv) {
+                    if (svz[0] >= 0) store_strip(a, S, vstrip + srow + svz[0], nvz0);
+                    if (svz[1] >= 0) store_strip(a, S, vstrip + srow + svz[1], nvz1);
                 }
             }
         }
@@ -233,8 +318,8 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
 // 1: forward + strip save; 2: receiver (backward model): overwrite the receiver row with
 // dt*gather[it], then image g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p
 // strips of step it restored, source subtracted).
-template <int BZ, int MODE>
-__global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
+template <int BZ, int MODE, typename ACC>
+__global__ void __launch_bounds__(NT) k_pres(const StepArgs a, int record)
 {
     constexpr int XH = BZ;        // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + 20;   // vz rows z0-10 .. z0+BZ+9, columns x0 .. x0+BX-1
@@ -242,166 +327,248 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
     float *svx = sm;
     float *svz = sm + XH * WW;
     __shared__ float s_tab[100];
+    __shared__ float s_c1z[BZ], s_ic2z[BZ];
     const TileRef t = a.tiles[blockIdx.x];
-    const ShotDev &S = a.shots[t.shot];
+    const ShotDev S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
     const int x0 = (t.tile % S.ntx) * BX, z0 = (t.tile / S.ntx) * BZ;
     if (MODE == 3 && (z0 + BZ <= npml - R || z0 >= Z - npml + R || x0 + BX <= npml - R || x0 >= X - npml + R))
         return;
     const WaveDev W = (MODE == 2) ? S.b : S.a;
     const float *__restrict__ kappa = (MODE >= 2) ? S.kappa_b : S.kappa_f;
+    const PmlOffsets o = pml_offsets(X, Z);
     stage<XH, WW>(svx, W.vx, pitch, Z, z0, x0 - 12);
     stage<ZH, BX>(svz, W.vz, pitch, Z, z0 - 10, x0);
-    if (threadIdx.x < 100) s_tab[threadIdx.x] = a.coef[threadIdx.x];
+    for (int i = threadIdx.x; i < 100; i += NT) s_tab[i] = a.coef[i];
+    for (int i = threadIdx.x; i < BZ; i += NT) {
+        const int z = min(z0 + i, Z - 1);
+        s_c1z[i] = S.pml[o.c1z + z];
+        s_ic2z[i] = S.pml[o.ic2z + z];
+    }
     cp_wait_all();
     __syncthreads();
-    const int tx = threadIdx.x, x = x0 + tx;
-    if (x >= X) return;
+    const int tx = threadIdx.x, xa = x0 + 2 * tx;
+    if (xa >= X) return;
 
-    const PmlOffsets o = pml_offsets(X, Z);
     const int nzi = S.nzi, nxi = S.nxi;
-    const int rpx = max(min(min(x, X - 1 - x), R), 1);
-    float cp[R];
+    float *__restrict__ pp = W.p;
+    float *__restrict__ sxp = W.sx;
+    float *__restrict__ szp = W.sz;
+    const float *__restrict__ psp = S.a.p;
+    ACC *__restrict__ g1p = (ACC *)S.g1;
+    ACC *__restrict__ ilp = (ACC *)S.illum;
+    // per-column constants
+    bool upd[2], xb[2], xin[2], srcc[2], recc[2], valid[2];
+    float c1x[2], ic2x[2];
+    int splr[2], sptb[2];
+    bool edge_order = false;
 #pragma unroll
-    for (int i = 0; i < R; i++) cp[i] = (rpx == R) ? a.c10[i] : s_tab[(rpx - 1) * R + i];
-    const bool xedge = (x < 1) || (x > X - 2);
-    const bool xb = (x < npml) || (x >= X - npml);
-    const float c1x = xb ? S.pml[o.c1x + x] : 1.0f;
-    const float ic2x = xb ? S.pml[o.ic2x + x] : 1.0f;
-    const bool in_src_col = (unsigned)(x - S.sbx0) < (unsigned)S.sbnx;
-    const bool rec_col = (x >= S.rx0) && (x < S.rx0 + S.nrec);
-    const int splr_col = strip_col_plr(x, X, npml, nzi);
-    const int sptb_col = (x >= npml && x < X - npml) ? x - npml : -1;
-    const size_t pstrip = 2 * (size_t)R * nzi + 2 * (size_t)R * nxi;   // offset of the p strips
+    for (int c = 0; c < 2; c++) {
+        const int x = xa + c;
+        valid[c] = x < X;
+        upd[c] = x >= 1 && x <= X - 2;
+        edge_order |= upd[c] && (x < R || x > X - 1 - R);
+        xb[c] = (x < npml) || (x >= X - npml);
+        xin[c] = valid[c] && !xb[c];
+        c1x[c] = (xb[c] && valid[c]) ? S.pml[o.c1x + x] : 1.0f;
+        ic2x[c] = (xb[c] && valid[c]) ? S.pml[o.ic2x + x] : 1.0f;
+        srcc[c] = valid[c] && (unsigned)(x - S.sbx0) < (unsigned)S.sbnx;
+        recc[c] = (x >= S.rx0) && (x < S.rx0 + S.nrec);
+        splr[c] = valid[c] ? strip_col_plr(x, X, npml, nzi) : -1;
+        sptb[c] = xin[c] ? x - npml : -1;
+    }
+    const int rpx0 = max(min(min(xa, X - 1 - xa), R), 1), rpx1 = max(min(min(xa + 1, X - 2 - xa), R), 1);
+    const size_t pstrip = 2 * (size_t)R * nzi + 2 * (size_t)R * nxi;
     const size_t ptb = pstrip + 2 * (size_t)R * nzi;
-    const bool xin = (x >= npml && x < X - npml);
     const float wit = a.wavelet[a.it];
+    const float dtx = a.dtx, dtz = a.dtz;
+    const bool any_band = xb[0] || xb[1];
 
-    float q[QL];   // q[(u + k) % QL] = vz[z - 10 + k][x]
+    float qa[QL], qb[QL];   // q?[(u + k) % QL] = vz[z - 10 + k][xa (+1)]
 #pragma unroll
-    for (int k = 0; k < QL - 1; k++) q[k] = svz[k * BX + tx];
-
+    for (int k = 0; k < QL - 1; k++) {
+        const float2 f = ld2(&svz[k * BX + 2 * tx]);
+        qa[k] = f.x;
+        qb[k] = f.y;
+    }
     const int zend = min(z0 + BZ, Z);
+    // operands of the next row
+    float2 n_kap = make_float2(0.f, 0.f), n_p = n_kap, n_s1 = n_kap, n_s2 = n_kap, n_ps = n_kap;
+    ACC n_g1[2] = {0, 0}, n_il[2] = {0, 0};
+    auto load_row = [&](int z) {
+        const unsigned id = (unsigned)z * pitch + xa;
+        const bool zin = (z >= npml && z < Z - npml);
+        n_kap = __ldg(reinterpret_cast<const float2 *>(&kappa[id]));
+        n_p = ld2(&pp[id]);
+        if (MODE != 3 && (any_band || !zin)) {
+            n_s1 = ld2(&sxp[id]);
+            n_s2 = ld2(&szp[id]);
+        }
+        if (MODE == 2 && zin && (xin[0] || xin[1])) {
+            n_ps = __ldg(reinterpret_cast<const float2 *>(&psp[id]));
+            const size_t im = (size_t)(z - npml) * nxi + (xa - npml);
+            if (xin[0]) { n_g1[0] = g1p[im]; n_il[0] = ilp[im]; }
+            if (xin[1]) { n_g1[1] = g1p[im + 1]; n_il[1] = ilp[im + 1]; }
+        }
+    };
+    load_row(z0);
     for (int zb = z0; zb < zend; zb += QL) {
 #pragma unroll
         for (int u = 0; u < QL; u++) {
             const int z = zb + u;
             if (z >= zend) break;
-            q[(u + QL - 1) % QL] = svz[(z - z0 + 19) * BX + tx];
-            const float *row = &svx[(z - z0) * WW + tx + 12];
-            const size_t id = (size_t)z * pitch + x;
-            const bool zin = (z >= npml && z < Z - npml);
-            if (MODE == 3) {
-                // ---------------- reconstruction of the source pressure
-                bool wr = false;
-                float ps = 0.0f;
-                if (zin && xin) {   // kernel.cu:389-429 (p += ...)
-                    float dxs = 0.0f, dzs = 0.0f;
+            const float2 kap = n_kap, op = n_p, os1 = n_s1, os2 = n_s2, ops = n_ps;
+            const ACC og1[2] = {n_g1[0], n_g1[1]}, oil[2] = {n_il[0], n_il[1]};
+            if (z + 1 < zend) load_row(z + 1);
+            {
+                const float2 f = ld2(&svz[(z - z0 + 19) * BX + 2 * tx]);
+                qa[(u + QL - 1) % QL] = f.x;
+                qb[(u + QL - 1) % QL] = f.y;
+            }
+            // w[k] = vx[z][xa - 10 + k], k = 0..21
+            float w[22];
+            const float *rw = &svx[(z - z0) * WW + 2 * tx + 2];
 #pragma unroll
-                    for (int i = 1; i <= R; i++) {
-                        dxs += a.c10[i - 1] * (row[i - 1] - row[-i]);
-                        dzs += a.c10[i - 1] * (q[(u + 9 + i) % QL] - q[(u + 10 - i) % QL]);
+            for (int j = 0; j < 11; j++) {
+                const float2 f = ld2(&rw[2 * j]);
+                w[2 * j] = f.x;
+                w[2 * j + 1] = f.y;
+            }
+            const int rpz = min(min(z, Z - 1 - z), R);
+            float dx0 = 0.f, dx1 = 0.f, dz0 = 0.f, dz1 = 0.f;
+            if (MODE == 3 || (!edge_order && rpz == R)) {
+#pragma unroll
+                for (int i = 1; i <= R; i++) {
+                    dx0 += a.c10[i - 1] * (w[9 + i] - w[10 - i]);
+                    dx1 += a.c10[i - 1] * (w[10 + i] - w[11 - i]);
+                    dz0 += a.c10[i - 1] * (qa[(u + 9 + i) % QL] - qa[(u + 10 - i) % QL]);
+                    dz1 += a.c10[i - 1] * (qb[(u + 9 + i) % QL] - qb[(u + 10 - i) % QL]);
+                }
+            } else {   // local order near the outer edge (kernel.cu:714-1185 with cuda_norder)
+                const float *c0 = &s_tab[(max(min(rpx0, rpz), 1) - 1) * R];
+                const float *c1 = &s_tab[(max(min(rpx1, rpz), 1) - 1) * R];
+#pragma unroll
+                for (int i = 1; i <= R; i++) {
+                    dx0 += c0[i - 1] * (w[9 + i] - w[10 - i]);
+                    dx1 += c1[i - 1] * (w[10 + i] - w[11 - i]);
+                    dz0 += c0[i - 1] * (qa[(u + 9 + i) % QL] - qa[(u + 10 - i) % QL]);
+                    dz1 += c1[i - 1] * (qb[(u + 9 + i) % QL] - qb[(u + 10 - i) % QL]);
+                }
+            }
+            const unsigned id = (unsigned)z * pitch + xa;
+            const bool zin = (z >= npml && z < Z - npml);
+            const bool srcr = (unsigned)(z - S.sbz0) < (unsigned)S.sbnz;
+            const float ddx[2] = {dx0 * dtx, dx1 * dtx}, ddz[2] = {dz0 * dtz, dz1 * dtz};
+            const float kk[2] = {kap.x, kap.y}, p0[2] = {op.x, op.y};
+            if (MODE == 3) {
+                // ---------------- reconstruction: kernel.cu:389-429, strips of step it, source
+                float ps[2] = {p0[0], p0[1]};
+                bool wr[2] = {false, false};
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    if (zin && xin[c]) {
+                        ps[c] = p0[c] + (ddx[c] * kk[c] + ddz[c] * kk[c]);
+                        wr[c] = true;
+                    } else {
+                        long si = -1;
+                        int kind = 2;
+                        if (zin && splr[c] >= 0) si = (long)(pstrip + splr[c] + (size_t)(z - npml) * R);
+                        else if (sptb[c] >= 0) {
+                            const int srow = strip_row_tb(z, npml, Z - npml, nxi);
+                            if (srow >= 0) { si = (long)(ptb + srow + sptb[c]); kind = 3; }
+                        }
+                        if (si >= 0) {   // read_d_ppmllr / read_d_ppmltb, kernel.cu:1348-1400
+                            const float sc = a.strip_prec ? S.strip_scale[(size_t)a.it * 4 + kind] : 1.0f;
+                            ps[c] = load_strip(S.strips, (size_t)a.it * S.strip_len + si, a.strip_prec, sc);
+                            wr[c] = true;
+                        }
                     }
-                    const float kap = __ldg(&kappa[id]);
-                    dxs = dxs * a.dtx * kap;
-                    dzs = dzs * a.dtz * kap;
-                    ps = W.p[id] + (dxs + dzs);
-                    wr = true;
-                } else {   // read_d_ppmllr / read_d_ppmltb (step it), kernel.cu:1348-1400
-                    long si = -1;
-                    int kind = 2;
-                    if (zin && splr_col >= 0) si = (long)(pstrip + splr_col + (size_t)(z - npml) * R);
-                    else if (sptb_col >= 0) {
-                        const int srow = strip_row_tb(z, npml, Z - npml, nxi);
-                        if (srow >= 0) { si = (long)(ptb + srow + sptb_col); kind = 3; }
-                    }
-                    if (si >= 0) {
-                        const float sc = a.strip_prec ? S.strip_scale[(size_t)a.it * 4 + kind] : 1.0f;
-                        ps = load_strip(S.strips, (size_t)a.it * S.strip_len + si, a.strip_prec, sc);
-                        wr = true;
+                    if (srcr && srcc[c]) {   // kernel.cu:36-47 (subtract)
+                        ps[c] -= S.src[(z - S.sbz0) * S.sbnx + (xa + c - S.sbx0)] * wit;
+                        wr[c] = true;
                     }
                 }
-                if (in_src_col && (unsigned)(z - S.sbz0) < (unsigned)S.sbnz) {   // kernel.cu:36-47 (subtract)
-                    if (!wr) ps = W.p[id];
-                    ps -= S.src[(z - S.sbz0) * S.sbnx + (x - S.sbx0)] * wit;
-                    wr = true;
-                }
-                if (wr) W.p[id] = ps;
+                st2(&pp[id], ps[0], ps[1], wr[0], wr[1]);
                 continue;
             }
             // ---------------- full-grid pressure update with split-field PML
-            const bool zedge = (z < 1) || (z > Z - 2);
-            float p;
-            bool wr = false;
-            if (!xedge && !zedge) {
-                const int rpz = min(min(z, Z - 1 - z), R);
-                float dxs = 0.0f, dzs = 0.0f;
-                if (rpz == R) {
+            const bool zupd = z >= 1 && z <= Z - 2;
+            float pn[2] = {p0[0], p0[1]};
+            bool wr[2] = {false, false};
+            if (zupd) {
+                if (zin && !any_band) {   // interior, kernel.cu:501-541
 #pragma unroll
-                    for (int i = 1; i <= R; i++) {
-                        dxs += cp[i - 1] * (row[i - 1] - row[-i]);
-                        dzs += cp[i - 1] * (q[(u + 9 + i) % QL] - q[(u + 10 - i) % QL]);
+                    for (int c = 0; c < 2; c++) {
+                        pn[c] = p0[c] - (ddx[c] * kk[c] + ddz[c] * kk[c]);
+                        wr[c] = upd[c];
                     }
-                } else {
-                    const float *c = &s_tab[(min(rpx, rpz) - 1) * R];
+                } else {                  // split-field PML, kernel.cu:714-1185
+                    const float c1z = s_c1z[z - z0], ic2z = s_ic2z[z - z0];
+                    const float s1o[2] = {os1.x, os1.y}, s2o[2] = {os2.x, os2.y};
+                    float s1n[2], s2n[2];
 #pragma unroll
-                    for (int i = 1; i <= R; i++) {
-                        dxs += c[i - 1] * (row[i - 1] - row[-i]);
-                        dzs += c[i - 1] * (q[(u + 9 + i) % QL] - q[(u + 10 - i) % QL]);
+                    for (int c = 0; c < 2; c++) {
+                        const float dxs = ddx[c] * kk[c], dzs = ddz[c] * kk[c];
+                        if (zin && !xb[c]) {
+                            pn[c] = p0[c] - (dxs + dzs);
+                            s1n[c] = s1o[c];
+                            s2n[c] = s2o[c];
+                        } else {
+                            s1n[c] = damp(s1o[c], dxs, c1x[c], ic2x[c]);
+                            s2n[c] = damp(s2o[c], dzs, c1z, ic2z);
+                            pn[c] = s1n[c] + s2n[c];
+                        }
+                        wr[c] = upd[c];
                     }
+                    const bool sb0 = upd[0] && (xb[0] || !zin), sb1 = upd[1] && (xb[1] || !zin);
+                    st2(&sxp[id], s1n[0], s1n[1], sb0, sb1);
+                    st2(&szp[id], s2n[0], s2n[1], sb0, sb1);
                 }
-                const float kap = __ldg(&kappa[id]);
-                dxs = dxs * a.dtx * kap;
-                dzs = dzs * a.dtz * kap;
-                const bool zb_ = !zin;
-                if (!xb && !zb_) {
-                    p = W.p[id] - (dxs + dzs);
-                } else {
-                    float s1 = W.sx[id], s2 = W.sz[id];
-                    s1 = xb ? (c1x * s1 - dxs) * ic2x : s1 - dxs;
-                    s2 = zb_ ? (S.pml[o.c1z + z] * s2 - dzs) * S.pml[o.ic2z + z] : s2 - dzs;
-                    W.sx[id] = s1;
-                    W.sz[id] = s2;
-                    p = s1 + s2;
-                }
-                wr = true;
             }
             if (MODE != 2) {
-                if (in_src_col && (unsigned)(z - S.sbz0) < (unsigned)S.sbnz) {   // kernel.cu:36-47 (add)
-                    if (!wr) p = W.p[id];
-                    p += S.src[(z - S.sbz0) * S.sbnx + (x - S.sbx0)] * wit;
-                    wr = true;
+                if (srcr) {   // kernel.cu:36-47 (add)
+#pragma unroll
+                    for (int c = 0; c < 2; c++)
+                        if (srcc[c]) {
+                            pn[c] += S.src[(z - S.sbz0) * S.sbnx + (xa + c - S.sbx0)] * wit;
+                            wr[c] = true;
+                        }
                 }
-                if (wr) W.p[id] = p;
-                if (record && z == S.rz && rec_col)   // kernel.cu:48-71
-                    ((float *)S.gather)[(size_t)a.it * S.nrec + (x - S.rx0)] = p;
-                if (MODE == 1) {
-                    if (zin && splr_col >= 0) {
-                        store_strip(a, S, pstrip + splr_col + (size_t)(z - npml) * R, wr ? p : W.p[id]);
-                    } else if (sptb_col >= 0) {
-                        const int srow = strip_row_tb(z, npml, Z - npml, nxi);
-                        if (srow >= 0) store_strip(a, S, ptb + srow + sptb_col, wr ? p : W.p[id]);
+                st2(&pp[id], pn[0], pn[1], wr[0], wr[1]);
+                if (record && z == S.rz) {   // kernel.cu:48-71
+#pragma unroll
+                    for (int c = 0; c < 2; c++)
+                        if (recc[c]) ((float *)S.gather)[(size_t)a.it * S.nrec + (xa + c - S.rx0)] = pn[c];
+                }
+                if (MODE == 1) {   // save_d_ppmllr / save_d_ppmltb, kernel.cu:1240-1293
+#pragma unroll
+                    for (int c = 0; c < 2; c++) {
+                        if (zin && splr[c] >= 0) store_strip(a, S, pstrip + splr[c] + (size_t)(z - npml) * R, pn[c]);
+                        else if (sptb[c] >= 0) {
+                            const int srow = strip_row_tb(z, npml, Z - npml, nxi);
+                            if (srow >= 0) store_strip(a, S, ptb + srow + sptb[c], pn[c]);
+                        }
                     }
                 }
             } else {
-                if (z == S.rz && rec_col) {   // kernel.cu:72-95 (overwrite)
-                    p = a.dt * gather_at(a, S, x - S.rx0);
-                    wr = true;
+                if (z == S.rz) {   // kernel.cu:72-95 (overwrite)
+#pragma unroll
+                    for (int c = 0; c < 2; c++)
+                        if (recc[c]) {
+                            pn[c] = a.dt * gather_at(a, S, xa + c - S.rx0);
+                            wr[c] = true;
+                        }
                 }
-                if (wr) W.p[id] = p;
-                if (zin && xin) {   // kernel.cu:1401-1416
-                    if (!wr) p = W.p[id];
-                    const float ps = S.a.p[id];
-                    const size_t im = (size_t)(z - npml) * nxi + (x - npml);
-                    if (a.accum_fp64) {
-                        double *g1 = (double *)S.g1, *il = (double *)S.illum;
-                        g1[im] += (double)ps * (double)p;
-                        il[im] += (double)ps * (double)ps;
-                    } else {
-                        float *g1 = (float *)S.g1, *il = (float *)S.illum;
-                        g1[im] += ps * p;
-                        il[im] += ps * ps;
-                    }
+                st2(&pp[id], pn[0], pn[1], wr[0], wr[1]);
+                if (zin) {   // kernel.cu:1401-1416
+                    const size_t im = (size_t)(z - npml) * nxi + (xa - npml);
+                    const float pss[2] = {ops.x, ops.y};
+#pragma unroll
+                    for (int c = 0; c < 2; c++)
+                        if (xin[c]) {
+                            g1p[im + c] = og1[c] + (ACC)pss[c] * (ACC)pn[c];
+                            ilp[im + c] = oil[c] + (ACC)pss[c] * (ACC)pss[c];
+                        }
                 }
             }
         }
@@ -423,17 +590,24 @@ static void vel_launch(const StepArgs &a, int ntiles, cudaStream_t s)
         cudaFuncSetAttribute(k_vel<BZ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_smem<BZ>());
         init = true;
     }
-    k_vel<BZ, MODE><<<ntiles, BX, vel_smem<BZ>(), s>>>(a);
+    k_vel<BZ, MODE><<<ntiles, NT, vel_smem<BZ>(), s>>>(a);
+}
+template <int BZ, int MODE, typename ACC>
+static void pres_launch_t(const StepArgs &a, int ntiles, int record, cudaStream_t s)
+{
+    static bool init = false;
+    if (!init) {
+        cudaFuncSetAttribute(k_pres<BZ, MODE, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pres_smem<BZ>());
+        init = true;
+    }
+    k_pres<BZ, MODE, ACC><<<ntiles, NT, pres_smem<BZ>(), s>>>(a, record);
 }
 template <int BZ, int MODE>
 static void pres_launch(const StepArgs &a, int ntiles, int record, cudaStream_t s)
 {
-    static bool init = false;
-    if (!init) {
-        cudaFuncSetAttribute(k_pres<BZ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_smem<BZ>());
-        init = true;
-    }
-    k_pres<BZ, MODE><<<ntiles, BX, pres_smem<BZ>(), s>>>(a, record);
+    if (MODE == 2 && a.accum_fp64) pres_launch_t<BZ, MODE, double>(a, ntiles, record, s);
+    else pres_launch_t<BZ, MODE, float>(a, ntiles, record, s);
 }
 
 template <int MODE>
