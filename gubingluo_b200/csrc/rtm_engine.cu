@@ -96,7 +96,7 @@ struct rtm_session {
     ShotDev *d_shots = nullptr;
     TileRef *d_tiles = nullptr;      // (shot, tile) list of the velocity kernels
     TileRef *d_tiles_p = nullptr;    // (shot, tile) list of the pressure kernels
-    int bz_vel = 32, bz_pres = 32;   // rows per tile of the two stencil kernels
+    int bz_vel = 16, bz_pres = 16;   // rows per tile of the two stencil kernels
     void *d_fin = nullptr;
     int max_tiles = 0;
     std::map<std::string, rtm::KernelTiming> timing;
