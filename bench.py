@@ -123,10 +123,11 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_unit(kernel: str):
-    """DRAM bytes per cell of one launch of `kernel` from the committed ncu summary
-    (profiles/ncu_<kernel>.txt, line 'dram_bytes_per_cell=<float>'), or None."""
-    path = os.path.join(ROOT, "profiles", f"ncu_{kernel}.txt")
+def ncu_traffic_per_unit(kernel: str, X: int, Z: int):
+    """DRAM bytes per padded cell of one launch of `kernel` on an X x Z grid from the committed
+    ncu summary (profiles/ncu_<kernel>_<X>x<Z>.txt, line 'dram_bytes_per_cell=<float>'), or
+    None when no capture of that kernel on that grid is committed."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel}_{X}x{Z}.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -144,12 +145,13 @@ def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum
       vel_recon:  read ps, 1/rho; read+write vxs, vzs on the interior  24 B per interior cell
       pres_recon: read vxs, vzs, kappa; read+write ps on the interior  20 B per interior cell
       pres_recv adds the imaging: read ps, read+write g1 and illum     4 + 4*accum B per interior cell
-    plus the boundary strips each kernel writes (forward) or reads (reconstruction)."""
+    plus the boundary strips the reconstruction kernels read (the forward strips are written
+    by a separate copy kernel)."""
     cells, inner = X * Z, nxi * nzi
     strips = 80 * (nxi + nzi)   # vx+vz or p strips of one step, fp32
     table = {
-        "vel_fwd": 24 * cells + strips,
-        "pres_fwd": 20 * cells + strips,
+        "vel_fwd": 24 * cells,
+        "pres_fwd": 20 * cells,
         "vel_recon": 24 * inner + strips,
         "pres_recon": 20 * inner + strips,
         "vel_recv": 24 * cells,
@@ -295,7 +297,7 @@ def run_ours(args, rank, world, local_rank):
     bytes_launch = nshots_launch * kernel_bytes(dom, X, Z, nxi, nzi, nrec, accum_bytes)
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_hbm_peak()
-    per_cell = ncu_traffic_per_unit(dom)
+    per_cell = ncu_traffic_per_unit(dom, X, Z)
     roofline = {"kernel": f"k_{dom}", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None if per_cell is None else round(per_cell * nshots_launch * X * Z),

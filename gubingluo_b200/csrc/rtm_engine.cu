@@ -415,7 +415,7 @@ static void timing_end(rtm_session *ss, cudaEvent_t ev)
 
 // Batch state shared by the phases of one batch.
 struct BatchRun {
-    int k0 = 0, n = 0, ntiles = 0, ntiles_p = 0, maxrec = 0;
+    int k0 = 0, n = 0, ntiles = 0, ntiles_p = 0, maxrec = 0, max_strip_len = 0;
     std::vector<ShotDev> hd;
     StepArgs a{};
 };
@@ -432,6 +432,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.hd.assign(n, ShotDev{});
     std::vector<TileRef> tiles, tiles_p;
     br.maxrec = 0;
+    br.max_strip_len = 0;
     for (int j = 0; j < n; j++) {
         ShotState &sh = ss->shots[k0 + j];
         Slot &sl = ss->slots[j];
@@ -456,6 +457,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         for (int t = 0; t < d.ntx * ntzv; t++) tiles.push_back({j, t});
         for (int t = 0; t < d.ntx * ntzp; t++) tiles_p.push_back({j, t});
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
+        br.max_strip_len = std::max(br.max_strip_len, sh.strip_len);
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
         float *f[10] = {sl.a.p, sl.a.vx, sl.a.vz, sl.a.sx, sl.a.sz, sl.b.p, sl.b.vx, sl.b.vz, sl.b.sx, sl.b.sz};
         for (float *p : f) CK(cudaMemsetAsync(p, 0, fb, st));
@@ -488,9 +490,10 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
 }
 
 // Source pass (rtm_model.cu:322-346): nsteps forward steps with the source added; strips
-// saved every step when `save`; the gather recorded when `record` (mode 0 fuses the
-// reference's separate modelling pass, rtm_model.cu:266-290, which is the same
-// computation in the same model, into this pass).
+// saved after every step when `save` (one small copy kernel, so the stencil kernels carry no
+// strip logic); the gather recorded when `record` (mode 0 fuses the reference's separate
+// modelling pass, rtm_model.cu:266-290, which is the same computation in the same model,
+// into this pass).
 static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, bool record)
 {
     const rtm_options &o = ss->o;
@@ -499,7 +502,7 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
     for (int it = 0; it < nsteps; it++) {
         a.it = it;
         a.ring = it % kRing;
-        const int mode = save ? RTM_WAVE_FWD_SAVE : RTM_WAVE_FWD;
+        const int mode = RTM_WAVE_FWD;
         cudaEvent_t e;
         timing_begin(ss, "vel_fwd", it, &e);
         a.tiles = ss->d_tiles;
@@ -510,6 +513,10 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
         launch_pres(mode, ss->bz_pres, a, br.ntiles_p, record ? 1 : 0, st);
         timing_end(ss, e);
         ss->launches += 2;
+        if (save) {
+            launch_strip_save(ss->d_shots, br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
+            ss->launches++;
+        }
         if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
             launch_strip_pack(ss->d_shots, br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
             ss->launches++;

@@ -10,8 +10,6 @@
 
 namespace {
 
-__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
-
 __device__ __forceinline__ float load_gather(const StepArgs &a, const ShotDev &S, int j)
 {
     size_t idx = (size_t)a.it * S.nrec + j;
@@ -115,6 +113,46 @@ __global__ void k_mute(float *g, const float *vrow, int X, int nsx, int nsz, int
     cut = cut > temp ? cut : temp;
     cut = cut < nt ? cut : nt;
     for (int it = blockIdx.y; it < nt && it <= cut; it += gridDim.y) g[(size_t)it * nrec + idx] = 0.0f;
+}
+
+// =====================================================================================
+// Boundary strips of the source pass (reference save_d_vxpml / save_d_vzpml /
+// save_d_ppmllr / save_d_ppmltb, kernel.cu:1186-1293): after step `it` of every shot of a
+// batch, copy the ten cells inside each PML edge of vx, vz and p into the step's strip
+// record, laid out [vx lr 2][nzi][10] [vz tb 2][10][nxi] [p lr 2][nzi][10] [p tb 2][10][nxi].
+// fp32 strips go straight to strips[it]; fp16/bf16 strips go to the fp32 staging ring slot
+// `ring` and are packed later.  Grid (ceil(strip_len / 256), nshots).
+__global__ void k_strip_save(const ShotDev *shots, int it, int ring, int prec)
+{
+    const ShotDev &S = shots[blockIdx.y];
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= S.strip_len) return;
+    const int X = S.X, Z = S.Z, npml = S.npml, nxi = S.nxi, nzi = S.nzi, pitch = S.pitch;
+    const int lr = R * nzi, tb = R * nxi;
+    int k = idx, z, x;
+    const float *f;
+    if (k < 2 * lr || (k >= 2 * lr + 2 * tb && k < 4 * lr + 2 * tb)) {   // left/right strips
+        const bool pstrip = k >= 2 * lr;
+        if (pstrip) k -= 2 * lr + 2 * tb;
+        const int side = k / lr, rem = k - side * lr;
+        z = npml + rem / R;
+        const int c = rem % R;
+        // vx right strip starts at X-npml-1 (vx has X-1 columns), p right strip at X-npml
+        x = side == 0 ? npml - R + c : (pstrip ? X - npml : X - npml - 1) + c;
+        f = pstrip ? S.a.p : S.a.vx;
+    } else {                                                             // top/bottom strips
+        const bool pstrip = k >= 4 * lr + 2 * tb;
+        k -= pstrip ? 4 * lr + 2 * tb : 2 * lr;
+        const int side = k / tb, rem = k - side * tb;
+        const int r = rem / nxi;
+        x = npml + (rem - r * nxi);
+        // vz bottom strip starts at Z-npml-1 (vz has Z-1 rows), p bottom strip at Z-npml
+        z = side == 0 ? npml - R + r : (pstrip ? Z - npml : Z - npml - 1) + r;
+        f = pstrip ? S.a.p : S.a.vz;
+    }
+    const float v = f[(size_t)z * pitch + x];
+    if (prec == RTM_FP32) ((float *)S.strips)[(size_t)it * S.strip_len + idx] = v;
+    else S.strip_stage[(size_t)ring * S.strip_len + idx] = v;
 }
 
 // =====================================================================================
@@ -299,6 +337,12 @@ void launch_mute(float *g, const float *vrow, int X, int nsx, int nsz, int nt, i
 {
     dim3 grid((nrec + 127) / 128, 64);
     k_mute<<<grid, 128, 0, s>>>(g, vrow, X, nsx, nsz, nt, rz, rx0, nrec, nw, tlength, dx2, dz2, rdt);
+}
+void launch_strip_save(const ShotDev *shots, int nshots, int max_strip_len, int it, int ring, int prec,
+                       cudaStream_t s)
+{
+    dim3 grid((max_strip_len + 255) / 256, nshots);
+    k_strip_save<<<grid, 256, 0, s>>>(shots, it, ring, prec);
 }
 void launch_strip_pack(const ShotDev *shots, int nshots, int it0, int ring0, int nsteps, int prec, cudaStream_t s)
 {

@@ -14,6 +14,8 @@ void launch_setup_source(float *src, int sbx0, int sbz0, int sbnx, int sbnz, int
 void launch_ricker(float *w, float fdom, float dt, int nt, cudaStream_t s);
 void launch_mute(float *g, const float *vrow, int X, int nsx, int nsz, int nt, int rz, int rx0, int nrec, int nw,
                  int tlength, float dx2, float dz2, float rdt, cudaStream_t s);
+void launch_strip_save(const ShotDev *shots, int nshots, int max_strip_len, int it, int ring, int prec,
+                       cudaStream_t s);
 void launch_strip_pack(const ShotDev *shots, int nshots, int it0, int ring0, int nsteps, int prec, cudaStream_t s);
 void launch_gather_pack(const float *g, void *out, float *scale, int nt, int nrec, int prec, cudaStream_t s);
 void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void *image1, void *image2s, void *image2m,

@@ -8,16 +8,17 @@
 //   * x-derivatives read the staged row; z-derivatives read a (2R+U-1)-deep register window
 //     that advances U rows per unrolled group (one shared load per row, a few register moves
 //     per group), which keeps the loop body small enough for the instruction cache;
-//   * the per-cell operands of a group of U rows are loaded at the start of the group, so
-//     their latency overlaps the group's stencil arithmetic;
+//   * the per-cell operands of the next group of U rows are loaded while the current group is
+//     computed (the first group's while the tile is staged);
 //   * the full-order coefficients come from the kernel-parameter constant bank.  Cells whose
 //     local order is reduced (the outer ten of the grid, reference cuda_norder*,
 //     kernel.cu:271-317) and rows left over after the last full group take a compact
 //     one-row path that reads its coefficients from a row of the zero-padded table;
-//   * PML damping, split pressure, source, receivers, strips and imaging are per-row or
-//     per-column predicates of the same kernel.
+//   * PML damping, split pressure, source, receivers, strip restore and imaging are per-row
+//     or per-column predicates of the same kernel (strips are saved by k_strip_save after
+//     each forward step).
 // Reference equivalents (gubingluo kernel.cu): forward v :430-500 + :542-713, forward p
-// :501-541 + :714-1185, reconstruction :318-429, strips :1186-1400, source :36-47,
+// :501-541 + :714-1185, reconstruction :318-429, strip restore :1294-1400, source :36-47,
 // receivers :48-95, cross-correlation :1401-1416.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -33,6 +34,7 @@ constexpr int WW = BX + 24;         // staged width: columns x0-12 .. x0+BX+11 (
 constexpr int R = RTM_RADIUS;
 constexpr int U = 4;                // rows per unrolled group
 constexpr int QN = 2 * R + U - 1;   // z window: the 2R taps of U consecutive rows
+
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -66,12 +68,6 @@ __device__ __forceinline__ float load_strip(const void *base, size_t idx, int pr
     if (prec == RTM_FP16) return __half2float(((const __half *)base)[idx]) * scale;
     if (prec == RTM_BF16) return __bfloat162float(((const __nv_bfloat16 *)base)[idx]) * scale;
     return ((const float *)base)[idx];
-}
-
-__device__ __forceinline__ void store_strip(const StepArgs &a, const ShotDev &S, size_t idx, float v)
-{
-    if (a.strip_prec == RTM_FP32) ((float *)S.strips)[(size_t)a.it * S.strip_len + idx] = v;
-    else S.strip_stage[(size_t)a.ring * S.strip_len + idx] = v;
 }
 
 __device__ __forceinline__ float gather_at(const StepArgs &a, const ShotDev &S, int j)
@@ -126,17 +122,43 @@ __device__ __forceinline__ void advance(float (&q)[QN], const float *s, int dz, 
     }
 }
 
+// Shot integers used inside the row loops, read once per thread.
+struct ShotK {
+    int nxi, nzi, strip_len;
+    int sbx0, sbnx, sbz0, sbnz;   // source box
+    int rz, rx0, nrec;            // receiver line
+};
+
+__device__ __forceinline__ ShotK shot_ints(const ShotDev &S)
+{
+    ShotK k;
+    k.nxi = S.nxi; k.nzi = S.nzi; k.strip_len = S.strip_len;
+    k.sbx0 = S.sbx0; k.sbnx = S.sbnx; k.sbz0 = S.sbz0; k.sbnz = S.sbnz;
+    k.rz = S.rz; k.rx0 = S.rx0; k.nrec = S.nrec;
+    return k;
+}
+
+// Sum_{i=1..R} c(i-1) * (f(i) - g(i)) in tap order; c is a coefficient accessor.
+template <typename C, typename F, typename G>
+__device__ __forceinline__ float tap_sum(C c, F f, G g)
+{
+    float s0 = 0.f;
+#pragma unroll
+    for (int i = 1; i <= R; i++) s0 += c(i - 1) * (f(i) - g(i));
+    return s0;
+}
+
 // Per-column constants of the velocity update.
 struct VelCol {
     bool hvx;            // column x carries a vx cell (x < X-1)
     float c1vx, ic2vx;   // vx damping of this column
-    int svx, svz;        // strip columns (-1: none)
+    int svx, svz;        // strip columns of the reconstruction (-1: none)
     bool rvx, rvz;       // reconstruction-interior columns
 };
 
 // Velocity update of one cell (x, z) from the raw derivative sums dx, dz.
 template <int MODE>
-__device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, const VelCol &cc,
+__device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, const ShotK &k, const VelCol &cc,
                                           float *__restrict__ vxp, float *__restrict__ vzp, unsigned id, int z,
                                           int Z, int npml, float dx, float dz, float ir, float ov, float ow,
                                           float c1z, float ic2z)
@@ -149,16 +171,16 @@ __device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, c
         if (zin && cc.rvx) vxp[id] = ov + dx * dtx * ir;
         else if (zin && cc.svx >= 0) {   // read_d_vxpml, kernel.cu:1294-1320
             const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 0] : 1.0f;
-            vxp[id] = load_strip(S.strips, (size_t)(a.it + 1) * S.strip_len + cc.svx + (size_t)(z - npml) * R,
+            vxp[id] = load_strip(S.strips, (size_t)(a.it + 1) * k.strip_len + cc.svx + (size_t)(z - npml) * R,
                                  a.strip_prec, sc);
         }
         if (zinv && cc.rvz) vzp[id] = ow + dz * dtz * ir;
         else if (cc.svz >= 0 && z < Z - 1) {   // read_d_vzpml, kernel.cu:1321-1347
-            const int srow = strip_row_tb(z, npml, Z - npml - 1, S.nxi);
+            const int srow = strip_row_tb(z, npml, Z - npml - 1, k.nxi);
             if (srow >= 0) {
                 const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 1] : 1.0f;
                 vzp[id] = load_strip(S.strips,
-                                     (size_t)(a.it + 1) * S.strip_len + 2 * (size_t)R * S.nzi + srow + cc.svz,
+                                     (size_t)(a.it + 1) * k.strip_len + 2 * (size_t)R * k.nzi + srow + cc.svz,
                                      a.strip_prec, sc);
             }
         }
@@ -167,16 +189,8 @@ __device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, c
     // kernel.cu:430-500 (interior) and :542-713 (PML): f' = (c1*f - d)*ic2
     const float nvx = damp(ov, dx * dtx * ir, cc.c1vx, cc.ic2vx);
     if (cc.hvx) vxp[id] = nvx;
-    const bool zv = z < Z - 1;
     const float nvz = damp(ow, dz * dtz * ir, c1z, ic2z);
-    if (zv) vzp[id] = nvz;
-    if (MODE == 1) {   // save_d_vxpml / save_d_vzpml, kernel.cu:1186-1239
-        if (cc.svx >= 0 && z >= npml && z < Z - npml) store_strip(a, S, cc.svx + (size_t)(z - npml) * R, nvx);
-        if (cc.svz >= 0 && zv) {
-            const int srow = strip_row_tb(z, npml, Z - npml - 1, S.nxi);
-            if (srow >= 0) store_strip(a, S, 2 * (size_t)R * S.nzi + srow + cc.svz, nvz);
-        }
-    }
+    if (z < Z - 1) vzp[id] = nvz;
 }
 
 // Per-column constants of the pressure update.
@@ -184,20 +198,14 @@ struct PresCol {
     bool xb, xin;        // column in the x PML band / in the image interior
     bool srcc, recc;     // column in the source box / on the receiver line
     float c1x, ic2x;     // x damping of this column
-    int splr, sptb;      // strip columns (-1: none)
-};
-
-// Per-row constants of the pressure update that come from the shot.
-struct PresRow {
-    int sbz0, sbnz, rz;   // source box rows, receiver row
-    float wit;            // wavelet sample of this step
+    int splr, sptb;      // strip columns of the reconstruction (-1: none)
 };
 
 // Pressure update of one cell (x, z) from the raw derivative sums dx, dz; `upd` is false on
 // the grid's edge rows and columns, which keep their pressure (kernel.cu:714-1185).
 template <int MODE, typename ACC>
-__device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, const PresCol &cc,
-                                           const PresRow &rr, float *__restrict__ pp, float *__restrict__ sxp,
+__device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, const ShotK &k, const PresCol &cc,
+                                           float wit, float *__restrict__ pp, float *__restrict__ sxp,
                                            float *__restrict__ szp, ACC *__restrict__ g1p, ACC *__restrict__ ilp,
                                            unsigned id, int x, int z, int Z, int npml, bool upd, float dx,
                                            float dz, float kk, float p0, float s1o, float s2o, float ps, ACC og1,
@@ -205,7 +213,7 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
 {
     const float ddx = dx * a.dtx, ddz = dz * a.dtz;
     const bool zin = (z >= npml && z < Z - npml);
-    const bool srcr = (unsigned)(z - rr.sbz0) < (unsigned)rr.sbnz;
+    const bool srcr = (unsigned)(z - k.sbz0) < (unsigned)k.sbnz;
     if (MODE == 3) {
         // reconstruction: kernel.cu:389-429, strips of step it, source subtracted
         float pn = p0;
@@ -214,25 +222,25 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
             pn = p0 + (ddx * kk + ddz * kk);
             wr = true;
         } else {
-            const size_t pstrip = 2 * (size_t)R * S.nzi + 2 * (size_t)R * S.nxi;
+            const size_t pstrip = 2 * (size_t)R * k.nzi + 2 * (size_t)R * k.nxi;
             long si = -1;
             int kind = 2;
             if (zin && cc.splr >= 0) si = (long)(pstrip + cc.splr + (size_t)(z - npml) * R);
             else if (cc.sptb >= 0) {
-                const int srow = strip_row_tb(z, npml, Z - npml, S.nxi);
+                const int srow = strip_row_tb(z, npml, Z - npml, k.nxi);
                 if (srow >= 0) {
-                    si = (long)(pstrip + 2 * (size_t)R * S.nzi + srow + cc.sptb);
+                    si = (long)(pstrip + 2 * (size_t)R * k.nzi + srow + cc.sptb);
                     kind = 3;
                 }
             }
             if (si >= 0) {   // read_d_ppmllr / read_d_ppmltb, kernel.cu:1348-1400
                 const float sc = a.strip_prec ? S.strip_scale[(size_t)a.it * 4 + kind] : 1.0f;
-                pn = load_strip(S.strips, (size_t)a.it * S.strip_len + si, a.strip_prec, sc);
+                pn = load_strip(S.strips, (size_t)a.it * k.strip_len + si, a.strip_prec, sc);
                 wr = true;
             }
         }
         if (srcr && cc.srcc) {   // kernel.cu:36-47 (subtract)
-            pn -= S.src[(z - rr.sbz0) * S.sbnx + (x - S.sbx0)] * rr.wit;
+            pn -= S.src[(z - k.sbz0) * k.sbnx + (x - k.sbx0)] * wit;
             wr = true;
         }
         if (wr) pp[id] = pn;
@@ -253,30 +261,22 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
         }
         wr = true;
     }
-    if (MODE != 2) {
+    if (MODE == 0) {
         if (srcr && cc.srcc) {   // kernel.cu:36-47 (add)
-            pn += S.src[(z - rr.sbz0) * S.sbnx + (x - S.sbx0)] * rr.wit;
+            pn += S.src[(z - k.sbz0) * k.sbnx + (x - k.sbx0)] * wit;
             wr = true;
         }
         if (wr) pp[id] = pn;
-        if (record && z == rr.rz && cc.recc)   // kernel.cu:48-71
-            ((float *)S.gather)[(size_t)a.it * S.nrec + (x - S.rx0)] = pn;
-        if (MODE == 1) {   // save_d_ppmllr / save_d_ppmltb, kernel.cu:1240-1293
-            const size_t pstrip = 2 * (size_t)R * S.nzi + 2 * (size_t)R * S.nxi;
-            if (zin && cc.splr >= 0) store_strip(a, S, pstrip + cc.splr + (size_t)(z - npml) * R, pn);
-            else if (cc.sptb >= 0) {
-                const int srow = strip_row_tb(z, npml, Z - npml, S.nxi);
-                if (srow >= 0) store_strip(a, S, pstrip + 2 * (size_t)R * S.nzi + srow + cc.sptb, pn);
-            }
-        }
+        if (record && z == k.rz && cc.recc)   // kernel.cu:48-71
+            ((float *)S.gather)[(size_t)a.it * k.nrec + (x - k.rx0)] = pn;
     } else {
-        if (z == rr.rz && cc.recc) {   // kernel.cu:72-95 (overwrite)
-            pn = a.dt * gather_at(a, S, x - S.rx0);
+        if (z == k.rz && cc.recc) {   // kernel.cu:72-95 (overwrite)
+            pn = a.dt * gather_at(a, S, x - k.rx0);
             wr = true;
         }
         if (wr) pp[id] = pn;
         if (zin && cc.xin) {   // kernel.cu:1401-1416
-            const size_t im = (size_t)(z - npml) * S.nxi + (x - npml);
+            const size_t im = (size_t)(z - npml) * k.nxi + (x - npml);
             g1p[im] = og1 + (ACC)ps * (ACC)pn;
             ilp[im] = oil + (ACC)ps * (ACC)ps;
         }
@@ -286,9 +286,9 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
 }  // namespace
 
 // =====================================================================================
-// Velocity update.  MODE 0: forward, full grid; 1: forward + strip save; 2: receiver
-// (backward model), full grid; 3: reconstruction of the source wavefield (interior only,
-// vx/vz strips of step it+1 restored).
+// Velocity update.  MODE 0: forward, full grid; 2: receiver (backward model), full grid;
+// 3: reconstruction of the source wavefield (interior only, vx/vz strips of step it+1
+// restored).
 template <int BZ, int MODE>
 __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
 {
@@ -312,11 +312,8 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
         s_c1vz[i] = S.pml[o.c1vz + z];
         s_ic2vz[i] = S.pml[o.ic2vz + z];
     }
-    cp_wait_all();
-    __syncthreads();
     const int tx = threadIdx.x, x = x0 + tx;
-    if (x >= X) return;   // no barrier below
-
+    const ShotK k = shot_ints(S);
     float *__restrict__ vxp = W.vx;
     float *__restrict__ vzp = W.vz;
     VelCol cc;
@@ -326,7 +323,7 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
         cc.c1vx = (band && cc.hvx) ? S.pml[o.c1vx + x] : 1.0f;
         cc.ic2vx = (band && cc.hvx) ? S.pml[o.ic2vx + x] : 1.0f;
     }
-    cc.svx = ((MODE == 1 || MODE == 3) && cc.hvx) ? strip_col_vx(x, X, npml, S.nzi) : -1;
+    cc.svx = (MODE == 3 && cc.hvx) ? strip_col_vx(x, X, npml, k.nzi) : -1;
     cc.svz = (x >= npml && x < X - npml) ? x - npml : -1;
     cc.rvx = (x >= npml && x <= X - npml - 2);
     cc.rvz = (x >= npml && x < X - npml);
@@ -343,10 +340,26 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
             zf1 = max(zf0, min(zend, Z - R));   // ... and Z-1-z >= R
         }
     }
+    // operands of the first unrolled group, loaded while the tile is staged
+    float cir[U], cov[U], cow[U];
+    auto load_group = [&](int zg, float(&gir)[U], float(&gov)[U], float(&gow)[U]) {
+        const unsigned g0 = (unsigned)zg * pitch + x;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            gir[u] = __ldg(&inv_rho[g0 + u * pitch]);
+            gov[u] = vxp[g0 + u * pitch];
+            gow[u] = vzp[g0 + u * pitch];
+        }
+    };
+    if (x < X && zf0 + U <= zf1) load_group(zf0, cir, cov, cow);
+    cp_wait_all();
+    __syncthreads();
+    if (x >= X) return;   // no barrier below
+
     const float *col = &sw[tx + 12];   // staged column x: col[r*WW] = p[z0-9+r][x]
     float q[QN];                        // q[k] = p[z-9+k][x] at the current row z
 #pragma unroll
-    for (int k = 0; k < QN; k++) q[k] = col[k * WW];
+    for (int j = 0; j < QN; j++) q[j] = col[j * WW];
 
     // one-row path: any row, local orders from the coefficient table
     auto one_row = [&](int z) {
@@ -362,7 +375,8 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
             dx += cx[i - 1] * (rw[i] - rw[1 - i]);
             dz += cz[i - 1] * (q[9 + i] - q[10 - i]);
         }
-        vel_apply<MODE>(a, S, cc, vxp, vzp, id, z, Z, npml, dx, dz, ir, ov, ow, s_c1vz[z - z0], s_ic2vz[z - z0]);
+        vel_apply<MODE>(a, S, k, cc, vxp, vzp, id, z, Z, npml, dx, dz, ir, ov, ow, s_c1vz[z - z0],
+                        s_ic2vz[z - z0]);
     };
 
     int z = z0;
@@ -371,27 +385,29 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
         advance<1, WW>(q, col, z + 1 - z0, z + 1 < zend);
     }
     for (; z + U <= zf1; z += U) {
-        float ir[U], ov[U], ow[U];
+        float nir[U], nov[U], now[U];
+        const bool more = z + 2 * U <= zf1;
+        if (more) load_group(z + U, nir, nov, now);
         const unsigned id0 = (unsigned)z * pitch + x;
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            ir[u] = __ldg(&inv_rho[id0 + u * pitch]);
-            ov[u] = vxp[id0 + u * pitch];
-            ow[u] = vzp[id0 + u * pitch];
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
             const float *rw = &col[(z + u - z0 + 9) * WW];
-            float dx = 0.f, dz = 0.f;
-#pragma unroll
-            for (int i = 1; i <= R; i++) {
-                dx += a.c10[i - 1] * (rw[i] - rw[1 - i]);
-                dz += a.c10[i - 1] * (q[u + 9 + i] - q[u + 10 - i]);
-            }
-            vel_apply<MODE>(a, S, cc, vxp, vzp, id0 + u * pitch, z + u, Z, npml, dx, dz, ir[u], ov[u], ow[u],
+            const float dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i]; },
+                                     [&](int i) { return rw[1 - i]; });
+            const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                                     [&](int i) { return q[u + 10 - i]; });
+            vel_apply<MODE>(a, S, k, cc, vxp, vzp, id0 + u * pitch, z + u, Z, npml, dx, dz, cir[u], cov[u], cow[u],
                             s_c1vz[z + u - z0], s_ic2vz[z + u - z0]);
         }
         advance<U, WW>(q, col, z + U - z0, z + U < zend);
+        if (more) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                cir[u] = nir[u];
+                cov[u] = nov[u];
+                cow[u] = now[u];
+            }
+        }
     }
     for (; z < zend; z++) {
         one_row(z);
@@ -401,9 +417,9 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
 
 // =====================================================================================
 // Pressure update.  MODE 0: forward (+ source, + receiver sampling when `record`);
-// 1: forward + strip save; 2: receiver (backward model): overwrite the receiver row with
-// dt*gather[it], then image g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p
-// strips of step it restored, source subtracted).
+// 2: receiver (backward model): overwrite the receiver row with dt*gather[it], then image
+// g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p strips of step it restored,
+// source subtracted).
 template <int BZ, int MODE, typename ACC>
 __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
 {
@@ -431,32 +447,24 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
         s_c1z[i] = S.pml[o.c1z + z];
         s_ic2z[i] = S.pml[o.ic2z + z];
     }
-    cp_wait_all();
-    __syncthreads();
     const int tx = threadIdx.x, x = x0 + tx;
-    if (x >= X) return;
-
+    const ShotK k = shot_ints(S);
     float *__restrict__ pp = W.p;
     float *__restrict__ sxp = W.sx;
     float *__restrict__ szp = W.sz;
     const float *__restrict__ psp = S.a.p;
     ACC *__restrict__ g1p = (ACC *)S.g1;
     ACC *__restrict__ ilp = (ACC *)S.illum;
-    const int nxi = S.nxi;
     PresCol cc;
     cc.xb = (x < npml) || (x >= X - npml);
     cc.xin = !cc.xb;
-    cc.c1x = cc.xb ? S.pml[o.c1x + x] : 1.0f;
-    cc.ic2x = cc.xb ? S.pml[o.ic2x + x] : 1.0f;
-    cc.srcc = (unsigned)(x - S.sbx0) < (unsigned)S.sbnx;
-    cc.recc = (x >= S.rx0) && (x < S.rx0 + S.nrec);
-    cc.splr = (MODE == 1 || MODE == 3) ? strip_col_plr(x, X, npml, S.nzi) : -1;
+    cc.c1x = (cc.xb && x < X) ? S.pml[o.c1x + x] : 1.0f;
+    cc.ic2x = (cc.xb && x < X) ? S.pml[o.ic2x + x] : 1.0f;
+    cc.srcc = (unsigned)(x - k.sbx0) < (unsigned)k.sbnx;
+    cc.recc = (x >= k.rx0) && (x < k.rx0 + k.nrec);
+    cc.splr = (MODE == 3) ? strip_col_plr(x, X, npml, k.nzi) : -1;
     cc.sptb = cc.xin ? x - npml : -1;
-    PresRow rr;
-    rr.sbz0 = S.sbz0;
-    rr.sbnz = S.sbnz;
-    rr.rz = S.rz;
-    rr.wit = a.wavelet[a.it];
+    const float wit = a.wavelet[a.it];
     // local order of this column (cuda_norder): full unless within ten cells of the edge
     const int rpx = min(min(x, X - 1 - x), R);
     const int zend = min(z0 + BZ, Z);
@@ -468,11 +476,43 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
             zf1 = max(zf0, min(zend, Z - R));
         }
     }
+    // operands of an unrolled group of rows
+    float ckk[U], cp0[U], cs1[U], cs2[U], cps[U];
+    ACC cg1[U], cil[U];
+    auto load_group = [&](int zg, float(&gkk)[U], float(&gp0)[U], float(&gs1)[U], float(&gs2)[U],
+                          float(&gps)[U], ACC(&gg1)[U], ACC(&gil)[U]) {
+        const unsigned g0 = (unsigned)zg * pitch + x;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned id = g0 + u * pitch;
+            const int zz = zg + u;
+            const bool zin = (zz >= npml && zz < Z - npml);
+            const bool band = cc.xb || !zin;
+            gkk[u] = __ldg(&kappa[id]);
+            gp0[u] = pp[id];
+            gs1[u] = (MODE != 3 && band) ? sxp[id] : 0.f;
+            gs2[u] = (MODE != 3 && band) ? szp[id] : 0.f;
+            gps[u] = 0.f;
+            gg1[u] = 0;
+            gil[u] = 0;
+            if (MODE == 2 && zin && cc.xin) {
+                const size_t im = (size_t)(zz - npml) * k.nxi + (x - npml);
+                gps[u] = __ldg(&psp[id]);
+                gg1[u] = g1p[im];
+                gil[u] = ilp[im];
+            }
+        }
+    };
+    if (x < X && zf0 + U <= zf1) load_group(zf0, ckk, cp0, cs1, cs2, cps, cg1, cil);
+    cp_wait_all();
+    __syncthreads();
+    if (x >= X) return;
+
     const float *colx = &svx[tx + 12];   // colx[r*WW] = vx[z0+r][x]
     const float *colz = &svz[tx];        // colz[r*BX] = vz[z0-10+r][x]
     float q[QN];                          // q[k] = vz[z-10+k][x] at the current row z
 #pragma unroll
-    for (int k = 0; k < QN; k++) q[k] = colz[k * BX];
+    for (int j = 0; j < QN; j++) q[j] = colz[j * BX];
 
     auto one_row = [&](int z) {
         const unsigned id = (unsigned)z * pitch + x;
@@ -483,7 +523,7 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
         float ps = 0.f;
         ACC og1 = 0, oil = 0;
         if (MODE == 2 && zin && cc.xin) {
-            const size_t im = (size_t)(z - npml) * nxi + (x - npml);
+            const size_t im = (size_t)(z - npml) * k.nxi + (x - npml);
             ps = __ldg(&psp[id]);
             og1 = g1p[im];
             oil = ilp[im];
@@ -498,8 +538,8 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
             dx += c[i - 1] * (rw[i - 1] - rw[-i]);
             dz += c[i - 1] * (q[9 + i] - q[10 - i]);
         }
-        pres_apply<MODE, ACC>(a, S, cc, rr, pp, sxp, szp, g1p, ilp, id, x, z, Z, npml, rp > 0, dx, dz, kk, p0, s1o,
-                              s2o, ps, og1, oil, s_c1z[z - z0], s_ic2z[z - z0], record);
+        pres_apply<MODE, ACC>(a, S, k, cc, wit, pp, sxp, szp, g1p, ilp, id, x, z, Z, npml, rp > 0, dx, dz, kk, p0,
+                              s1o, s2o, ps, og1, oil, s_c1z[z - z0], s_ic2z[z - z0], record);
     };
 
     int z = z0;
@@ -508,43 +548,35 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
         advance<1, BX>(q, colz, z + 1 - z0, z + 1 < zend);
     }
     for (; z + U <= zf1; z += U) {
-        float kk[U], p0[U], s1[U], s2[U], ps[U];
-        ACC g1[U], il[U];
+        float nkk[U], np0[U], ns1[U], ns2[U], nps[U];
+        ACC ng1[U], nil[U];
+        const bool more = z + 2 * U <= zf1;
+        if (more) load_group(z + U, nkk, np0, ns1, ns2, nps, ng1, nil);
         const unsigned id0 = (unsigned)z * pitch + x;
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const unsigned id = id0 + u * pitch;
-            const int zz = z + u;
-            const bool zin = (zz >= npml && zz < Z - npml);
-            const bool band = cc.xb || !zin;
-            kk[u] = __ldg(&kappa[id]);
-            p0[u] = pp[id];
-            s1[u] = (MODE != 3 && band) ? sxp[id] : 0.f;
-            s2[u] = (MODE != 3 && band) ? szp[id] : 0.f;
-            ps[u] = 0.f;
-            g1[u] = 0;
-            il[u] = 0;
-            if (MODE == 2 && zin && cc.xin) {
-                const size_t im = (size_t)(zz - npml) * nxi + (x - npml);
-                ps[u] = __ldg(&psp[id]);
-                g1[u] = g1p[im];
-                il[u] = ilp[im];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
             const float *rw = &colx[(z + u - z0) * WW];
-            float dx = 0.f, dz = 0.f;
-#pragma unroll
-            for (int i = 1; i <= R; i++) {
-                dx += a.c10[i - 1] * (rw[i - 1] - rw[-i]);
-                dz += a.c10[i - 1] * (q[u + 9 + i] - q[u + 10 - i]);
-            }
-            pres_apply<MODE, ACC>(a, S, cc, rr, pp, sxp, szp, g1p, ilp, id0 + u * pitch, x, z + u, Z, npml, true,
-                                  dx, dz, kk[u], p0[u], s1[u], s2[u], ps[u], g1[u], il[u], s_c1z[z + u - z0],
+            const float dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i - 1]; },
+                                     [&](int i) { return rw[-i]; });
+            const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                                     [&](int i) { return q[u + 10 - i]; });
+            pres_apply<MODE, ACC>(a, S, k, cc, wit, pp, sxp, szp, g1p, ilp, id0 + u * pitch, x, z + u, Z, npml, true,
+                                  dx, dz, ckk[u], cp0[u], cs1[u], cs2[u], cps[u], cg1[u], cil[u], s_c1z[z + u - z0],
                                   s_ic2z[z + u - z0], record);
         }
         advance<U, BX>(q, colz, z + U - z0, z + U < zend);
+        if (more) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                ckk[u] = nkk[u];
+                cp0[u] = np0[u];
+                cs1[u] = ns1[u];
+                cs2[u] = ns2[u];
+                cps[u] = nps[u];
+                cg1[u] = ng1[u];
+                cil[u] = nil[u];
+            }
+        }
     }
     for (; z < zend; z++) {
         one_row(z);
@@ -611,7 +643,6 @@ void launch_vel(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s)
 {
     switch (mode) {
     case RTM_WAVE_FWD: vel_dispatch<0>(bz, a, ntiles, s); break;
-    case RTM_WAVE_FWD_SAVE: vel_dispatch<1>(bz, a, ntiles, s); break;
     case RTM_WAVE_RECEIVER: vel_dispatch<2>(bz, a, ntiles, s); break;
     default: vel_dispatch<3>(bz, a, ntiles, s); break;
     }
@@ -620,7 +651,6 @@ void launch_pres(int mode, int bz, const StepArgs &a, int ntiles, int record, cu
 {
     switch (mode) {
     case RTM_WAVE_FWD: pres_dispatch<0>(bz, a, ntiles, record, s); break;
-    case RTM_WAVE_FWD_SAVE: pres_dispatch<1>(bz, a, ntiles, record, s); break;
     case RTM_WAVE_RECEIVER: pres_dispatch<2>(bz, a, ntiles, 0, s); break;
     default: pres_dispatch<3>(bz, a, ntiles, 0, s); break;
     }

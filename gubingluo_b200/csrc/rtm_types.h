@@ -20,8 +20,8 @@
 
 // What one launch of the stencil kernels updates.
 enum RtmWaveMode {
-    RTM_WAVE_FWD = 0,        // forward propagation, full grid (modelling)
-    RTM_WAVE_FWD_SAVE = 1,   // forward propagation + boundary strips saved (source pass)
+    RTM_WAVE_FWD = 0,        // forward propagation, full grid (modelling and source pass;
+                             // the source pass saves its strips with k_strip_save)
     RTM_WAVE_RECEIVER = 2,   // receiver back-propagation (+ injection; imaging in the p update)
     RTM_WAVE_RECON = 3       // source-wavefield reconstruction (interior + restored strips)
 };
