@@ -181,8 +181,11 @@ def run_ours(args, rank, world, local_rank):
     s, all_shots, v_true, v_mig, rho, meta = synthetic.config(args.config, nt=args.nt or None)
     B = args.shots_per_step
     K, W = args.steps, args.warmup
-    # this rank's shots: every world-th shot of the survey, repeated as needed
-    mine = all_shots[rank::world] or all_shots[:1]
+    # this rank's shots: longest-processing-time partition of the survey by shot cost
+    # (nt * X * Z), repeated as needed to fill the steps
+    from gubingluo_b200 import shards
+    parts = shards.lpt_shards(shards.shot_costs(G.SurveyConfig(**{**s.__dict__, "mode": 1}), all_shots), world)
+    mine = [all_shots[i] for i in parts[rank]] or all_shots[:1]
     need = B * (K + W)
     uniq = mine[: min(len(mine), need)]
     step_shots = [uniq[(i * B + j) % len(uniq)] for i in range(K + W) for j in range(B)]
@@ -211,18 +214,17 @@ def run_ours(args, rank, world, local_rank):
                  for k in ("image1", "image2s", "illum")] if dist else []
 
     def reduce_images():
+        # the one exchange step: sum of the ranks' stacked images, after all of their shots
         if dist:
             with torch.cuda.stream(stream):
-                for t in img_views:
-                    dist.all_reduce(t)
+                shards.allreduce_images(img_views, dist)
 
     def step(i):
-        st = ss.run_range(i * B, B)
-        reduce_images()
-        return st
+        return ss.run_range(i * B, B)
 
     for i in range(W):
         step(i)
+    ss.reset_images()   # the images of the timed run hold the timed shots only
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
@@ -238,6 +240,7 @@ def run_ours(args, rank, world, local_rank):
     launches = 0
     for i in range(W, W + K):
         launches += step(i).kernel_launches
+    reduce_images()
     e1.record(stream)
     torch.cuda.synchronize()
     clock_info = clocks.stop()
@@ -267,6 +270,7 @@ def run_ours(args, rank, world, local_rank):
         img_host = torch.empty((s.nz, s.nx), dtype=torch.float32, pin_memory=True)
         h2d = B * s.nt * nrec * 4
         d2h = s.nz * s.nx * 4
+        ss.reset_images()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -277,6 +281,7 @@ def run_ours(args, rank, world, local_rank):
                 G._check(G.lib().rtm_session_set_gather(ss.h, k, host[step_shots[k]].data_ptr()))
             step(i)
             G._check(G.lib().rtm_session_get_images(ss.h, None, img_host.data_ptr(), None, None))
+        reduce_images()
         e1.record(stream)
         torch.cuda.synchronize()
         ms_e2e = e0.elapsed_time(e1)
