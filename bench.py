@@ -10,7 +10,8 @@ One step migrates --shots-per-step shots per GPU (mode 1: recorded gathers in, s
 out).  `value` times K steps with the gathers already resident in device memory; `e2e` times
 K steps through the same public C-ABI with each step's gathers copied from pinned host memory
 and the stacked image read back.  Under torchrun each rank migrates its own shots (weak
-scaling); the partial images are summed across ranks with an NCCL all-reduce every step.
+scaling); the ranks' partial images are summed with one NCCL all-reduce after the timed
+steps (inside the timed region).
 
 --impl reference times the reference's CPU path on the host cores.  The reference has no CPU
 implementation of the stencil or imaging (its host code is serial model preparation and file
