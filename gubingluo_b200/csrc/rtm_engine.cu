@@ -96,7 +96,7 @@ struct rtm_session {
     ShotDev *d_shots = nullptr;
     TileRef *d_tiles = nullptr;      // (shot, tile) list of the velocity kernels
     TileRef *d_tiles_p = nullptr;    // (shot, tile) list of the pressure kernels
-    int bz_vel = 16, bz_pres = 16;   // rows per tile of the two stencil kernels
+    int bz_vel = 32, bz_pres = 16;   // rows per tile of the two stencil kernels
     void *d_fin = nullptr;
     int max_tiles = 0;
     std::map<std::string, rtm::KernelTiming> timing;
@@ -165,7 +165,9 @@ static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, i
         b += (size_t)s.nt * 4 * sizeof(float) + 256;
         b += (size_t)kRing * strip_len * sizeof(float) + 256;
     }
-    b += 2 * ((size_t)nxi * nzi * (o.accum_fp64 ? 8 : 4) + 256);
+    b += 2 * ((size_t)pitch * Z * (o.accum_fp64 ? 8 : 4) + 256);   // g1, illum on the padded grid
+    (void)nxi;
+    (void)nzi;
     return b;
 }
 
@@ -349,7 +351,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             sl.strip_scale = (float *)ss->arena.take((size_t)s.nt * 4 * 4);
             sl.strip_stage = (float *)ss->arena.take((size_t)kRing * big.strip_len * 4);
         }
-        size_t ib = (size_t)big.nxi * big.nzi * (o.accum_fp64 ? 8 : 4);
+        size_t ib = (size_t)big.pitch * big.Z * (o.accum_fp64 ? 8 : 4);
         sl.g1 = ss->arena.take(ib);
         sl.illum = ss->arena.take(ib);
         if (!sl.strips || !sl.g1 || !sl.illum) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
@@ -461,7 +463,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
         float *f[10] = {sl.a.p, sl.a.vx, sl.a.vz, sl.a.sx, sl.a.sz, sl.b.p, sl.b.vx, sl.b.vz, sl.b.sx, sl.b.sz};
         for (float *p : f) CK(cudaMemsetAsync(p, 0, fb, st));
-        size_t ib = (size_t)sh.nxi * sh.nzi * (o.accum_fp64 ? 8 : 4);
+        size_t ib = (size_t)sh.pitch * sh.Z * (o.accum_fp64 ? 8 : 4);
         CK(cudaMemsetAsync(sl.g1, 0, ib, st));
         CK(cudaMemsetAsync(sl.illum, 0, ib, st));
     }
@@ -592,7 +594,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         int nwin = 50;   // rtm_model.cu:70, :464-465
         while (2 * nwin >= sh.nxi) nwin -= 3;
         fill_finalize_shot(fin.data() + j * finalize_shot_size(), ss->slots[j].g1, ss->slots[j].illum, sh.g.nx1,
-                           sh.nxi, nwin);
+                           sh.nxi, nwin, sh.pitch, s.npml);
     }
     CK(cudaMemcpyAsync(ss->d_fin, fin.data(), fin.size(), cudaMemcpyHostToDevice, st));
     launch_finalize(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->img1, ss->img2s, ss->img2m, ss->illum, st);

@@ -241,8 +241,8 @@ __global__ void k_gather_pack(const float *g, void *out, float *scale, int nt, i
 // image cell walks the batch's shots in order, so overlapping apertures stack in a fixed
 // order.  Images are fp32 (reference) or fp64.
 struct FinalizeShot {
-    const void *g1, *illum;
-    int nx1, nxi, nwin;
+    const void *g1, *illum;   // [Z][pitch]: interior cell (iz, lx) at (iz+npml)*pitch + lx+npml
+    int nx1, nxi, nwin, pitch, npml;
 };
 
 __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, int fp64, void *image1,
@@ -261,7 +261,7 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
             if (lx < nwin) tp = expf(-alpha * alpha * (nwin - lx) * (nwin - lx));
             if (lx >= nxl - nwin && lx < nxl) tp = expf(-alpha * alpha * (lx - nxl + nwin + 1) * (lx - nxl + nwin + 1));
             if (lx >= nwin && lx < nxl - nwin) tp = 1.0f;
-            const size_t ip = (size_t)iz * nxl + lx;
+            const size_t ip = (size_t)(iz + f.npml) * f.pitch + lx + f.npml;
             if (fp64) {
                 double g = ((const double *)f.g1)[ip] * (double)tp;
                 double il = ((const double *)f.illum)[ip] * (double)tp;
@@ -374,7 +374,8 @@ void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float d
     k_inject<<<grid, 128, 0, s>>>(shots, it, dt, gather_prec);
 }
 size_t finalize_shot_size() { return sizeof(FinalizeShot); }
-void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin)
+void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin, int pitch,
+                        int npml)
 {
     FinalizeShot f;
     f.g1 = g1;
@@ -382,5 +383,7 @@ void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, i
     f.nx1 = nx1;
     f.nxi = nxi;
     f.nwin = nwin;
+    f.pitch = pitch;
+    f.npml = npml;
     *(FinalizeShot *)dst = f;
 }

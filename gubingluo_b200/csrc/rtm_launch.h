@@ -23,4 +23,5 @@ void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void 
 void launch_laplace(const float *in, float *out, int nx, int nz, int dx, int dz, cudaStream_t s);
 void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float dt, int gather_prec, cudaStream_t s);
 size_t finalize_shot_size();
-void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin);
+void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin, int pitch,
+                        int npml);

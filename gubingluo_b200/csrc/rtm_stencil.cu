@@ -10,10 +10,11 @@
 //     per group), which keeps the loop body small enough for the instruction cache;
 //   * the per-cell operands of the next group of U rows are loaded while the current group is
 //     computed (the first group's while the tile is staged);
-//   * the full-order coefficients come from the kernel-parameter constant bank.  Cells whose
-//     local order is reduced (the outer ten of the grid, reference cuda_norder*,
-//     kernel.cu:271-317) and rows left over after the last full group take a compact
-//     one-row path that reads its coefficients from a row of the zero-padded table;
+//   * the full-order coefficients come from the kernel-parameter constant bank.  Tiles that
+//     reach the outer ten cells of the grid, where the local order is reduced (reference
+//     cuda_norder*, kernel.cu:271-317), run the same groups with coefficients from rows of the
+//     zero-padded table (the choice is per tile, so warps do not diverge); rows left over
+//     after the last whole group take a compact one-row path;
 //   * PML damping, split pressure, source, receivers, strip restore and imaging are per-row
 //     or per-column predicates of the same kernel (strips are saved by k_strip_save after
 //     each forward step).
@@ -275,10 +276,9 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
             wr = true;
         }
         if (wr) pp[id] = pn;
-        if (zin && cc.xin) {   // kernel.cu:1401-1416
-            const size_t im = (size_t)(z - npml) * k.nxi + (x - npml);
-            g1p[im] = og1 + (ACC)ps * (ACC)pn;
-            ilp[im] = oil + (ACC)ps * (ACC)ps;
+        if (zin && cc.xin) {   // kernel.cu:1401-1416 (accumulators on the padded grid)
+            g1p[id] = og1 + (ACC)ps * (ACC)pn;
+            ilp[id] = oil + (ACC)ps * (ACC)ps;
         }
     }
 }
@@ -289,8 +289,10 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
 // Velocity update.  MODE 0: forward, full grid; 2: receiver (backward model), full grid;
 // 3: reconstruction of the source wavefield (interior only, vx/vz strips of step it+1
 // restored).
+// Register budgets (measured): 6 blocks per SM for the full-grid passes, 5 for the
+// reconstruction, whose strip restore needs more registers.
 template <int BZ, int MODE>
-__global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
+__global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 {
     constexpr int WH = BZ + QN - 1;   // staged rows z0-9 .. z0+BZ+QN-11
     extern __shared__ __align__(16) float sw[];
@@ -330,16 +332,12 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
     // vx order of this column (cuda_norderx): full unless within ten cells of the edge
     const int ox = min(min(x + 1, X - 1 - x), R);
     const int zend = min(z0 + BZ, Z);
-    // rows [zf0, zf1) take the unrolled full-order path.  The reconstruction writes only
-    // cells at least npml >= R from the edge, where every order is full.
-    int zf0 = z0, zf1 = zend;
-    if (MODE != 3) {
-        if (ox < R) zf0 = zf1 = zend;   // whole column on the one-row path
-        else {
-            zf0 = max(z0, R - 1);               // vz order (cuda_norderz): z+1 >= R ...
-            zf1 = max(zf0, min(zend, Z - R));   // ... and Z-1-z >= R
-        }
-    }
+    // Tiles that reach the outer ten cells of the grid take the table-coefficient form of the
+    // unrolled groups: vx order per column (cuda_norderx), vz order per row (cuda_norderz).
+    // The reconstruction writes only cells at least npml >= R from the edge, where every
+    // order is full.
+    const bool edge_tile = MODE != 3 && (x0 < R || x0 + BX > X - R || z0 < R || zend > Z - R);
+    const float *cxe = &s_tab[(max(ox, 1) - 1) * R];
     // operands of the first unrolled group, loaded while the tile is staged
     float cir[U], cov[U], cow[U];
     auto load_group = [&](int zg, float(&gir)[U], float(&gov)[U], float(&gow)[U]) {
@@ -351,7 +349,7 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
             gow[u] = vzp[g0 + u * pitch];
         }
     };
-    if (x < X && zf0 + U <= zf1) load_group(zf0, cir, cov, cow);
+    if (x < X && z0 + U <= zend) load_group(z0, cir, cov, cow);
     cp_wait_all();
     __syncthreads();
     if (x >= X) return;   // no barrier below
@@ -361,7 +359,7 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
 #pragma unroll
     for (int j = 0; j < QN; j++) q[j] = col[j * WW];
 
-    // one-row path: any row, local orders from the coefficient table
+    // one-row path for the rows after the last whole group: local orders from the table
     auto one_row = [&](int z) {
         const unsigned id = (unsigned)z * pitch + x;
         const float ir = __ldg(&inv_rho[id]), ov = vxp[id], ow = vzp[id];
@@ -380,22 +378,28 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
     };
 
     int z = z0;
-    for (; z < zf0; z++) {
-        one_row(z);
-        advance<1, WW>(q, col, z + 1 - z0, z + 1 < zend);
-    }
-    for (; z + U <= zf1; z += U) {
+    for (; z + U <= zend; z += U) {
         float nir[U], nov[U], now[U];
-        const bool more = z + 2 * U <= zf1;
+        const bool more = z + 2 * U <= zend;
         if (more) load_group(z + U, nir, nov, now);
         const unsigned id0 = (unsigned)z * pitch + x;
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const float *rw = &col[(z + u - z0 + 9) * WW];
-            const float dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i]; },
-                                     [&](int i) { return rw[1 - i]; });
-            const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
-                                     [&](int i) { return q[u + 10 - i]; });
+            float dx, dz;
+            if (!edge_tile) {
+                dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i]; },
+                             [&](int i) { return rw[1 - i]; });
+                dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                             [&](int i) { return q[u + 10 - i]; });
+            } else {
+                const int zz = z + u, oz = min(min(zz + 1, Z - 1 - zz), R);
+                const float *cze = &s_tab[(max(oz, 1) - 1) * R];
+                dx = tap_sum([&](int j) { return cxe[j]; }, [&](int i) { return rw[i]; },
+                             [&](int i) { return rw[1 - i]; });
+                dz = tap_sum([&](int j) { return cze[j]; }, [&](int i) { return q[u + 9 + i]; },
+                             [&](int i) { return q[u + 10 - i]; });
+            }
             vel_apply<MODE>(a, S, k, cc, vxp, vzp, id0 + u * pitch, z + u, Z, npml, dx, dz, cir[u], cov[u], cow[u],
                             s_c1vz[z + u - z0], s_ic2vz[z + u - z0]);
         }
@@ -420,8 +424,11 @@ __global__ void __launch_bounds__(BX) k_vel(const StepArgs a)
 // 2: receiver (backward model): overwrite the receiver row with dt*gather[it], then image
 // g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p strips of step it restored,
 // source subtracted).
+// Register budgets (measured): 6 blocks per SM for the reconstruction, 5 for the receiver
+// pass (4 with fp64 accumulators, which would spill at 5); the forward pass is left to the
+// compiler, which was faster than any bound tried.
 template <int BZ, int MODE, typename ACC>
-__global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
+__global__ void __launch_bounds__(BX, MODE == 3 ? 6 : (MODE == 0 ? 0 : (sizeof(ACC) == 8 ? 4 : 5))) k_pres(const StepArgs a, int record)
 {
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QN - 1;   // vz rows z0-10 .. z0+BZ+QN-12, columns x0 .. x0+BX-1
@@ -468,14 +475,8 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
     // local order of this column (cuda_norder): full unless within ten cells of the edge
     const int rpx = min(min(x, X - 1 - x), R);
     const int zend = min(z0 + BZ, Z);
-    int zf0 = z0, zf1 = zend;
-    if (MODE != 3) {
-        if (rpx < R) zf0 = zf1 = zend;
-        else {
-            zf0 = max(z0, R);
-            zf1 = max(zf0, min(zend, Z - R));
-        }
-    }
+    // tiles that reach the outer ten cells take the table-coefficient form of the groups
+    const bool edge_tile = MODE != 3 && (x0 < R || x0 + BX > X - R || z0 < R || zend > Z - R);
     // operands of an unrolled group of rows
     float ckk[U], cp0[U], cs1[U], cs2[U], cps[U];
     ACC cg1[U], cil[U];
@@ -496,14 +497,13 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
             gg1[u] = 0;
             gil[u] = 0;
             if (MODE == 2 && zin && cc.xin) {
-                const size_t im = (size_t)(zz - npml) * k.nxi + (x - npml);
                 gps[u] = __ldg(&psp[id]);
-                gg1[u] = g1p[im];
-                gil[u] = ilp[im];
+                gg1[u] = g1p[id];
+                gil[u] = ilp[id];
             }
         }
     };
-    if (x < X && zf0 + U <= zf1) load_group(zf0, ckk, cp0, cs1, cs2, cps, cg1, cil);
+    if (x < X && z0 + U <= zend) load_group(z0, ckk, cp0, cs1, cs2, cps, cg1, cil);
     cp_wait_all();
     __syncthreads();
     if (x >= X) return;
@@ -514,6 +514,7 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
 #pragma unroll
     for (int j = 0; j < QN; j++) q[j] = colz[j * BX];
 
+    // one-row path for the rows after the last whole group: local orders from the table
     auto one_row = [&](int z) {
         const unsigned id = (unsigned)z * pitch + x;
         const bool zin = (z >= npml && z < Z - npml);
@@ -523,10 +524,9 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
         float ps = 0.f;
         ACC og1 = 0, oil = 0;
         if (MODE == 2 && zin && cc.xin) {
-            const size_t im = (size_t)(z - npml) * k.nxi + (x - npml);
             ps = __ldg(&psp[id]);
-            og1 = g1p[im];
-            oil = ilp[im];
+            og1 = g1p[id];
+            oil = ilp[id];
         }
         const float *rw = &colx[(z - z0) * WW];
         const int rpz = min(min(z, Z - 1 - z), R);
@@ -543,24 +543,32 @@ __global__ void __launch_bounds__(BX) k_pres(const StepArgs a, int record)
     };
 
     int z = z0;
-    for (; z < zf0; z++) {
-        one_row(z);
-        advance<1, BX>(q, colz, z + 1 - z0, z + 1 < zend);
-    }
-    for (; z + U <= zf1; z += U) {
+    for (; z + U <= zend; z += U) {
         float nkk[U], np0[U], ns1[U], ns2[U], nps[U];
         ACC ng1[U], nil[U];
-        const bool more = z + 2 * U <= zf1;
+        const bool more = z + 2 * U <= zend;
         if (more) load_group(z + U, nkk, np0, ns1, ns2, nps, ng1, nil);
         const unsigned id0 = (unsigned)z * pitch + x;
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const float *rw = &colx[(z + u - z0) * WW];
-            const float dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i - 1]; },
-                                     [&](int i) { return rw[-i]; });
-            const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
-                                     [&](int i) { return q[u + 10 - i]; });
-            pres_apply<MODE, ACC>(a, S, k, cc, wit, pp, sxp, szp, g1p, ilp, id0 + u * pitch, x, z + u, Z, npml, true,
+            float dx, dz;
+            bool upd = true;
+            if (!edge_tile) {
+                dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i - 1]; },
+                             [&](int i) { return rw[-i]; });
+                dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                             [&](int i) { return q[u + 10 - i]; });
+            } else {   // local order min(x, z distance to the edge, R); none on the edge itself
+                const int zz = z + u, rp = min(rpx, min(min(zz, Z - 1 - zz), R));
+                const float *cf = &s_tab[(max(rp, 1) - 1) * R];
+                upd = rp > 0;
+                dx = tap_sum([&](int j) { return cf[j]; }, [&](int i) { return rw[i - 1]; },
+                             [&](int i) { return rw[-i]; });
+                dz = tap_sum([&](int j) { return cf[j]; }, [&](int i) { return q[u + 9 + i]; },
+                             [&](int i) { return q[u + 10 - i]; });
+            }
+            pres_apply<MODE, ACC>(a, S, k, cc, wit, pp, sxp, szp, g1p, ilp, id0 + u * pitch, x, z + u, Z, npml, upd,
                                   dx, dz, ckk[u], cp0[u], cs1[u], cs2[u], cps[u], cg1[u], cil[u], s_c1z[z + u - z0],
                                   s_ic2z[z + u - z0], record);
         }

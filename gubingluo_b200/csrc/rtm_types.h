@@ -71,7 +71,7 @@ struct ShotDev {
     float *strip_stage;                 // fp32 staging ring for fp16/bf16 strips [ring][strip_len]
     void *gather;                       // [nt][nrec] of the gather precision
     float *gather_scale;                // [nt]
-    void *g1, *illum;                   // [nzi][nxi] float or double accumulators
+    void *g1, *illum;                   // [Z][pitch] float or double accumulators (interior cells used)
 };
 
 struct TileRef {
