@@ -1,6 +1,8 @@
 // rtm_engine.cu — host engine: sessions, device memory, batching of shots and the
 // per-pass time loops (reference shot driver rtm_model.cu:117-569, re-designed so that a
 // batch of shots shares every launch and all boundary strips stay in HBM).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -11,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -98,6 +101,8 @@ struct rtm_session {
     TileRef *d_tiles_p = nullptr;    // (shot, tile) list of the pressure kernels
     int bz_vel = 32, bz_pres = 16;   // rows per tile of the two stencil kernels
     void *d_fin = nullptr;
+    void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
+    int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
     int max_tiles = 0;
     std::map<std::string, rtm::KernelTiming> timing;
     int launches = 0;
@@ -106,6 +111,55 @@ struct rtm_session {
 };
 
 namespace rtm {
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link to
+// libcuda needed).
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// Tensor map of one [Z][pitch] fp32 field for boxes of box_w x box_h elements.  Rows and
+// columns outside the field read as zero (the stencil kernels rely on it at the grid edge).
+static int encode_field_map(void *out, float *field, int pitch, int Z, int box_w, int box_h)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    if (!enc) return fail(RTM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    // TMA needs a 16-byte aligned base, a row stride that is a multiple of 16 bytes and a box
+    // row of a multiple of 16 bytes; boxes are at most 256 elements per dimension
+    if (((uintptr_t)field & 15) || (pitch * 4) % 16 || (box_w * 4) % 16 || box_w > 256 || box_h > 256)
+        return fail(RTM_ERR_ARG, "tensor map: misaligned field or box");
+    cuuint64_t dim[2] = {(cuuint64_t)pitch, (cuuint64_t)Z};
+    cuuint64_t stride[1] = {(cuuint64_t)pitch * 4};
+    cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
+    cuuint32_t estride[2] = {1, 1};
+    CUresult r = enc((CUtensorMap *)out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, field, dim, stride, box, estride,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(RTM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return RTM_OK;
+}
+
+// Read and clear the kernels' error flag (after the stream has been synchronised).
+static int check_kernel_flag(rtm_session *ss)
+{
+    int flag = 0;
+    CK(cudaMemcpy(&flag, ss->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        CK(cudaMemset(ss->d_err, 0, sizeof(int)));
+        return fail(RTM_ERR_CUDA, "a stencil kernel gave up waiting for its tile (TMA copy did not complete)");
+    }
+    return RTM_OK;
+}
 
 static int check_survey(const rtm_survey &s)
 {
@@ -246,6 +300,8 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         if (e && *e) ss->bz_vel = std::atoi(e);
         e = std::getenv("RTM_B200_BZ_PRES");
         if (e && *e) ss->bz_pres = std::atoi(e);
+        for (int bz : {ss->bz_vel, ss->bz_pres})
+            if (bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 16, 32 or 64");
     }
     B = std::max(B, 1);
     ss->B = B;
@@ -356,8 +412,12 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         sl.illum = ss->arena.take(ib);
         if (!sl.strips || !sl.g1 || !sl.illum) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
     }
-    // descriptor and tile tables
+    // descriptor and tile tables, tensor maps, kernel error flag
     ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
+    ss->d_tmaps = ss->arena.take((size_t)B * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
+    ss->d_err = (int *)ss->arena.take(sizeof(int));
+    if (!ss->d_tmaps || !ss->d_err) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
+    CK(cudaMemsetAsync(ss->d_err, 0, sizeof(int), ss->stream));
     int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + 15) / 16);
     ss->max_tiles = tiles_per_shot * B;
     ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
@@ -433,6 +493,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.n = n;
     br.hd.assign(n, ShotDev{});
     std::vector<TileRef> tiles, tiles_p;
+    std::vector<unsigned char> maps((size_t)n * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
     br.maxrec = 0;
     br.max_strip_len = 0;
     for (int j = 0; j < n; j++) {
@@ -455,6 +516,20 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         d.gather = s.mode == 0 ? sh.gather_raw : sh.gather32;
         d.gather_scale = nullptr;
         d.g1 = sl.g1; d.illum = sl.illum;
+        // tensor maps of the fields the stencil kernels stage, for this shot's row pitch
+        {
+            const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA, ph = ss->bz_pres + RTM_STAGE_ZEXTRA;
+            struct { float *f; int w, h; } m[RTM_TMAP_COUNT] = {
+                {sl.a.p, RTM_STAGE_W, vh}, {sl.a.vx, RTM_STAGE_W, ss->bz_pres}, {sl.a.vz, RTM_BX, ph},
+                {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph}};
+            for (int t = 0; t < RTM_TMAP_COUNT; t++) {
+                CUtensorMap cm;
+                int rc = encode_field_map(&cm, m[t].f, sh.pitch, sh.Z, m[t].w, m[t].h);
+                if (rc) return rc;
+                std::memcpy(&maps[((size_t)j * RTM_TMAP_COUNT + t) * RTM_TMAP_BYTES], &cm, RTM_TMAP_BYTES);
+            }
+            d.tmaps = (const char *)ss->d_tmaps + (size_t)j * RTM_TMAP_COUNT * RTM_TMAP_BYTES;
+        }
         const int ntzv = (sh.Z + ss->bz_vel - 1) / ss->bz_vel, ntzp = (sh.Z + ss->bz_pres - 1) / ss->bz_pres;
         for (int t = 0; t < d.ntx * ntzv; t++) tiles.push_back({j, t});
         for (int t = 0; t < d.ntx * ntzp; t++) tiles_p.push_back({j, t});
@@ -470,6 +545,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.ntiles = (int)tiles.size();
     br.ntiles_p = (int)tiles_p.size();
     CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ss->d_tmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles, tiles.data(), sizeof(TileRef) * br.ntiles, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles_p, tiles_p.data(), sizeof(TileRef) * br.ntiles_p, cudaMemcpyHostToDevice, st));
     StepArgs &a = br.a;
@@ -485,6 +561,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     a.strip_prec = o.strip_precision;
     a.gather_prec = RTM_PREC_FP32;
     a.accum_fp64 = o.accum_fp64;
+    a.err = ss->d_err;
     ss->last_batch_n = n;
     ss->last_batch_shots.clear();
     for (int j = 0; j < n; j++) ss->last_batch_shots.push_back(k0 + j);
@@ -611,7 +688,7 @@ static int run_batch(rtm_session *ss, int k0, int n)
     if ((rc = batch_forward(ss, br, ss->s.nt, true, ss->s.mode == 0))) return rc;
     if ((rc = batch_backward(ss, br))) return rc;
     CK(cudaStreamSynchronize(ss->stream));
-    return RTM_OK;
+    return check_kernel_flag(ss);
 }
 
 int session_batch_size(rtm_session *ss) { return ss ? ss->B : 0; }
@@ -625,7 +702,7 @@ static int model_range(rtm_session *ss, int k0, int n)
     if (rc) return rc;
     if ((rc = batch_forward(ss, br, ss->s.nt, false, true))) return rc;
     CK(cudaStreamSynchronize(ss->stream));
-    return RTM_OK;
+    return check_kernel_flag(ss);
 }
 
 // Run shots [k0, k0+n) (n <= batch size) as one batch.
@@ -894,6 +971,7 @@ int rtm_forward(const rtm_survey *s, const rtm_options *o, int ishot, const floa
     if (!(rc = batch_setup(ss, 0, 1, br)) && !(rc = batch_forward(ss, br, nsteps, false, true))) {
         cudaError_t e = cudaStreamSynchronize(ss->stream);
         if (e != cudaSuccess) rc = fail(RTM_ERR_CUDA, cudaGetErrorString(e));
+        if (!rc) rc = check_kernel_flag(ss);
         const size_t w = sizeof(float);
         if (!rc && p && cudaMemcpy2D(p, sh.X * w, sl.a.p, sh.pitch * w, sh.X * w, sh.Z, cudaMemcpyDeviceToHost))
             rc = fail(RTM_ERR_CUDA, "copy p");

@@ -3,8 +3,9 @@
 // One launch updates one wavefield of every shot of a batch: a flat (shot, tile) work list
 // maps each 128-thread block to a BX x BZ tile of one shot.  Each thread owns one grid
 // column x and marches down the tile's BZ rows:
-//   * the tile and its halo are staged once into shared memory with 16-byte cp.async copies
-//     (zero-filled outside the grid), so every global access is a coalesced row segment;
+//   * the tile and its halo are staged once into shared memory by the tensor memory
+//     accelerator (2-D cp.async.bulk.tensor boxes issued by one thread, completion on an
+//     mbarrier; rows and columns outside the field arrive as zeros);
 //   * x-derivatives read the staged row; z-derivatives read a (2R+U-1)-deep register window
 //     that advances U rows per unrolled group (one shared load per row, a few register moves
 //     per group), which keeps the loop body small enough for the instruction cache;
@@ -31,37 +32,64 @@
 namespace {
 
 constexpr int BX = RTM_BX;          // threads (= columns) per block
-constexpr int WW = BX + 24;         // staged width: columns x0-12 .. x0+BX+11 (16-byte aligned)
+constexpr int WW = RTM_STAGE_W;     // staged width: columns x0-12 .. x0+BX+11 (16-byte aligned)
 constexpr int R = RTM_RADIUS;
-constexpr int U = 4;                // rows per unrolled group
+constexpr int U = RTM_GROUP;        // rows per unrolled group
 constexpr int QN = 2 * R + U - 1;   // z window: the 2R taps of U consecutive rows
+static_assert(QN - 1 == RTM_STAGE_ZEXTRA, "staged rows beyond a tile must cover the z window");
+static_assert(WW == BX + 24, "staged width");
+constexpr long kWaitLimit = 1L << 22;   // polls of a tile's TMA barrier before giving up
 
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void cp16(float *dst, const float *src, bool ok)
+// ---- TMA tile staging ------------------------------------------------------------------
+// One thread of the block initialises an mbarrier, announces the bytes of the tile's boxes and
+// issues the 2-D TMA copies (cp.async.bulk.tensor, no multicast; boxes start at x0-12 or x0, a
+// multiple of 4 floats, and rows or columns outside the field arrive as zeros); every thread
+// then polls the barrier, at most kWaitLimit times.
+__device__ __forceinline__ void mbar_init(unsigned long long *bar)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-                 "r"(ok ? 16 : 0));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void cp_wait_all()
+__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes)
 {
-    asm volatile("cp.async.commit_group;\n" ::);
-    asm volatile("cp.async.wait_group 0;\n" ::);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
 }
-
-// Rows [r0, r0+NR) and columns [c0, c0+NC) of field f into s[NR][NC]; c0 and NC are
-// multiples of 4, rows outside [0, zrows) and columns outside [0, pitch) read as zero.
-template <int NR, int NC>
-__device__ __forceinline__ void stage(float *s, const float *__restrict__ f, int pitch, int zrows, int r0, int c0)
+__device__ __forceinline__ void tma_box(float *dst, const void *tmap, int x, int y, unsigned long long *bar)
 {
-    constexpr int N4 = NC / 4;
-    for (int i = threadIdx.x; i < NR * N4; i += BX) {
-        const int r = i / N4, c = (i - r * N4) * 4;
-        const int z = r0 + r, x = c0 + c;
-        const bool ok = (unsigned)z < (unsigned)zrows && (unsigned)x < (unsigned)pitch;
-        cp16(&s[r * NC + c], ok ? f + (size_t)z * pitch + x : f, ok);
-    }
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];\n" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_done(unsigned long long *bar)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar))
+        : "memory");
+    return ok != 0;
+}
+// Wait for the tile; on giving up, flag the error, wait once more (bounded) for the copies
+// still in flight and report false, so that the block returns without computing.
+__device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err)
+{
+    for (long i = 0; i < kWaitLimit; i++)
+        if (mbar_done(bar)) return true;
+    atomicExch(err, 1);
+    for (long i = 0; i < kWaitLimit; i++)
+        if (mbar_done(bar)) break;
+    return false;
+}
+__device__ __forceinline__ const void *tmap_of(const ShotDev &S, int which)
+{
+    return (const char *)S.tmaps + which * RTM_TMAP_BYTES;
 }
 
 __device__ __forceinline__ float load_strip(const void *base, size_t idx, int prec, float scale)
@@ -295,7 +323,8 @@ template <int BZ, int MODE>
 __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 {
     constexpr int WH = BZ + QN - 1;   // staged rows z0-9 .. z0+BZ+QN-11
-    extern __shared__ __align__(16) float sw[];
+    extern __shared__ __align__(128) float sw[];
+    __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1vz[BZ], s_ic2vz[BZ];
     const TileRef t = a.tiles[blockIdx.x];
@@ -307,7 +336,11 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
     const WaveDev W = (MODE == 2) ? S.b : S.a;
     const float *__restrict__ inv_rho = (MODE >= 2) ? S.inv_rho_b : S.inv_rho_f;
     const PmlOffsets o = pml_offsets(X, Z);
-    stage<WH, WW>(sw, W.p, pitch, Z, z0 - 9, x0 - 12);
+    if (threadIdx.x == 0) {   // p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139
+        mbar_init(&s_bar);
+        mbar_expect(&s_bar, WH * WW * sizeof(float));
+        tma_box(sw, tmap_of(S, MODE == 2 ? RTM_TMAP_B_P : RTM_TMAP_A_P), x0 - 12, z0 - 9, &s_bar);
+    }
     for (int i = threadIdx.x; i < 100; i += BX) s_tab[i] = a.coef[i];
     for (int i = threadIdx.x; i < BZ; i += BX) {
         const int z = min(z0 + i, Z - 2);
@@ -350,9 +383,8 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
         }
     };
     if (x < X && z0 + U <= zend) load_group(z0, cir, cov, cow);
-    cp_wait_all();
     __syncthreads();
-    if (x >= X) return;   // no barrier below
+    if (!tile_wait(&s_bar, a.err) || x >= X) return;   // no barrier below
 
     const float *col = &sw[tx + 12];   // staged column x: col[r*WW] = p[z0-9+r][x]
     float q[QN];                        // q[k] = p[z-9+k][x] at the current row z
@@ -432,9 +464,10 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 6 : (MODE == 0 ? 0 : (sizeof(A
 {
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QN - 1;   // vz rows z0-10 .. z0+BZ+QN-12, columns x0 .. x0+BX-1
-    extern __shared__ __align__(16) float sm[];
+    extern __shared__ __align__(128) float sm[];
     float *svx = sm;
-    float *svz = sm + XH * WW;
+    float *svz = sm + XH * WW;   // XH * WW * 4 bytes is a multiple of 128
+    __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1z[BZ], s_ic2z[BZ];
     const TileRef t = a.tiles[blockIdx.x];
@@ -446,8 +479,12 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 6 : (MODE == 0 ? 0 : (sizeof(A
     const WaveDev W = (MODE == 2) ? S.b : S.a;
     const float *__restrict__ kappa = (MODE >= 2) ? S.kappa_b : S.kappa_f;
     const PmlOffsets o = pml_offsets(X, Z);
-    stage<XH, WW>(svx, W.vx, pitch, Z, z0, x0 - 12);
-    stage<ZH, BX>(svz, W.vz, pitch, Z, z0 - 10, x0);
+    if (threadIdx.x == 0) {   // vx rows z0 .. z0+BZ-1 (columns x0-12 ..), vz rows z0-10 .. z0+BZ+11
+        mbar_init(&s_bar);
+        mbar_expect(&s_bar, (XH * WW + ZH * BX) * sizeof(float));
+        tma_box(svx, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VX : RTM_TMAP_A_VX), x0 - 12, z0, &s_bar);
+        tma_box(svz, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VZ : RTM_TMAP_A_VZ), x0, z0 - 10, &s_bar);
+    }
     for (int i = threadIdx.x; i < 100; i += BX) s_tab[i] = a.coef[i];
     for (int i = threadIdx.x; i < BZ; i += BX) {
         const int z = min(z0 + i, Z - 1);
@@ -504,9 +541,8 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 6 : (MODE == 0 ? 0 : (sizeof(A
         }
     };
     if (x < X && z0 + U <= zend) load_group(z0, ckk, cp0, cs1, cs2, cps, cg1, cil);
-    cp_wait_all();
     __syncthreads();
-    if (x >= X) return;
+    if (!tile_wait(&s_bar, a.err) || x >= X) return;
 
     const float *colx = &svx[tx + 12];   // colx[r*WW] = vx[z0+r][x]
     const float *colz = &svz[tx];        // colz[r*BX] = vz[z0-10+r][x]

@@ -17,6 +17,9 @@
 
 #define RTM_RADIUS 10
 #define RTM_BX 128       // stencil tile width: columns (= threads) per block
+#define RTM_GROUP 4      // rows per unrolled group of the stencil kernels
+#define RTM_STAGE_W (RTM_BX + 24)                             // staged width: columns x0-12 .. x0+BX+11
+#define RTM_STAGE_ZEXTRA (2 * RTM_RADIUS + RTM_GROUP - 2)   // staged rows beyond a tile's BZ (z window)
 
 // What one launch of the stencil kernels updates.
 enum RtmWaveMode {
@@ -72,7 +75,16 @@ struct ShotDev {
     void *gather;                       // [nt][nrec] of the gather precision
     float *gather_scale;                // [nt]
     void *g1, *illum;                   // [Z][pitch] float or double accumulators (interior cells used)
+    const void *tmaps;                  // RTM_TMAP_COUNT TMA tensor maps (128 B each) of this shot's slot
 };
+
+// TMA tensor maps of one slot: the staged fields of the two wavefields with the box each
+// stencil kernel loads (velocity: p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139;
+// pressure: vx rows z0 .. z0+BZ-1 with the same columns, vz rows z0-10 .. z0+BZ+11,
+// columns x0 .. x0+127).
+enum RtmTmap { RTM_TMAP_A_P = 0, RTM_TMAP_A_VX, RTM_TMAP_A_VZ, RTM_TMAP_B_P, RTM_TMAP_B_VX, RTM_TMAP_B_VZ,
+               RTM_TMAP_COUNT };
+#define RTM_TMAP_BYTES 128
 
 struct TileRef {
     int shot;
@@ -90,4 +102,5 @@ struct StepArgs {
     int it;                 // time index
     int strip_prec, gather_prec, accum_fp64;
     int ring;               // staging-ring slot for fp16/bf16 strips
+    int *err;               // device error flag: set non-zero by a kernel whose bounded wait gave up
 };
