@@ -99,7 +99,7 @@ struct rtm_session {
     ShotDev *d_shots = nullptr;
     TileRef *d_tiles = nullptr;      // (shot, tile) list of the velocity kernels
     TileRef *d_tiles_p = nullptr;    // (shot, tile) list of the pressure kernels
-    int bz_vel = 32, bz_pres = 16;   // rows per tile of the two stencil kernels
+    int bz_vel = 16, bz_pres = 16;   // rows per tile of the two stencil kernels
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -301,7 +301,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         e = std::getenv("RTM_B200_BZ_PRES");
         if (e && *e) ss->bz_pres = std::atoi(e);
         for (int bz : {ss->bz_vel, ss->bz_pres})
-            if (bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 16, 32 or 64");
+            if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
     }
     B = std::max(B, 1);
     ss->B = B;
@@ -418,7 +418,8 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->d_err = (int *)ss->arena.take(sizeof(int));
     if (!ss->d_tmaps || !ss->d_err) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     CK(cudaMemsetAsync(ss->d_err, 0, sizeof(int), ss->stream));
-    int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + 15) / 16);
+    const int bz_min = std::min(ss->bz_vel, ss->bz_pres);
+    int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + bz_min - 1) / bz_min);
     ss->max_tiles = tiles_per_shot * B;
     ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_tiles_p = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);

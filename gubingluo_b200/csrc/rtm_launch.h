@@ -4,7 +4,7 @@
 
 #include "rtm_types.h"
 
-// mode: RtmWaveMode; bz: rows per tile (16, 32 or 64); ntiles: length of the (shot, tile)
+// mode: RtmWaveMode; bz: rows per tile (8, 16, 32 or 64); ntiles: length of the (shot, tile)
 // list built for that bz.
 void launch_vel(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s);
 void launch_pres(int mode, int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s);

@@ -672,6 +672,7 @@ template <int MODE>
 static void vel_dispatch(int bz, const StepArgs &a, int ntiles, cudaStream_t s)
 {
     if (bz == 16) vel_launch<16, MODE>(a, ntiles, s);
+    else if (bz == 8) vel_launch<8, MODE>(a, ntiles, s);
     else if (bz == 64) vel_launch<64, MODE>(a, ntiles, s);
     else vel_launch<32, MODE>(a, ntiles, s);
 }
@@ -679,6 +680,7 @@ template <int MODE>
 static void pres_dispatch(int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s)
 {
     if (bz == 16) pres_launch<16, MODE>(a, ntiles, record, s);
+    else if (bz == 8) pres_launch<8, MODE>(a, ntiles, record, s);
     else if (bz == 64) pres_launch<64, MODE>(a, ntiles, record, s);
     else pres_launch<32, MODE>(a, ntiles, record, s);
 }
