@@ -97,8 +97,10 @@ struct rtm_session {
     float coef_host[100];
     void *img1 = nullptr, *img2s = nullptr, *img2m = nullptr, *illum = nullptr;
     ShotDev *d_shots = nullptr;
-    TileRef *d_tiles = nullptr;      // (shot, tile) list of the velocity kernels
-    TileRef *d_tiles_p = nullptr;    // (shot, tile) list of the pressure kernels
+    TileRef *d_tiles = nullptr;      // tiles of the velocity kernels (whole padded grid)
+    TileRef *d_tiles_p = nullptr;    // tiles of the pressure kernels (whole padded grid)
+    TileRef *d_tiles_r = nullptr;    // velocity tiles of the reconstruction region (interior + strips)
+    TileRef *d_tiles_pr = nullptr;   // pressure tiles of the reconstruction region
     int bz_vel = 16, bz_pres = 16;   // rows per tile of the two stencil kernels
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
@@ -423,8 +425,10 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->max_tiles = tiles_per_shot * B;
     ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_tiles_p = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
+    ss->d_tiles_r = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
+    ss->d_tiles_pr = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_fin = ss->arena.take(finalize_shot_size() * B);
-    if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_fin)
+    if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_tiles_r || !ss->d_tiles_pr || !ss->d_fin)
         return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     CK(cudaStreamSynchronize(ss->stream));
     return RTM_OK;
@@ -478,7 +482,7 @@ static void timing_end(rtm_session *ss, cudaEvent_t ev)
 
 // Batch state shared by the phases of one batch.
 struct BatchRun {
-    int k0 = 0, n = 0, ntiles = 0, ntiles_p = 0, maxrec = 0, max_strip_len = 0;
+    int k0 = 0, n = 0, ntiles = 0, ntiles_p = 0, ntiles_r = 0, ntiles_pr = 0, maxrec = 0, max_strip_len = 0;
     std::vector<ShotDev> hd;
     StepArgs a{};
 };
@@ -493,7 +497,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.k0 = k0;
     br.n = n;
     br.hd.assign(n, ShotDev{});
-    std::vector<TileRef> tiles, tiles_p;
+    std::vector<TileRef> tiles, tiles_p, tiles_r, tiles_pr;
     std::vector<unsigned char> maps((size_t)n * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
     br.maxrec = 0;
     br.max_strip_len = 0;
@@ -531,9 +535,18 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
             }
             d.tmaps = (const char *)ss->d_tmaps + (size_t)j * RTM_TMAP_COUNT * RTM_TMAP_BYTES;
         }
-        const int ntzv = (sh.Z + ss->bz_vel - 1) / ss->bz_vel, ntzp = (sh.Z + ss->bz_pres - 1) / ss->bz_pres;
-        for (int t = 0; t < d.ntx * ntzv; t++) tiles.push_back({j, t});
-        for (int t = 0; t < d.ntx * ntzp; t++) tiles_p.push_back({j, t});
+        // whole-grid tiles, and the reconstruction's tiles: it writes only the interior and the
+        // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10)
+        const int xr0 = (s.npml - RTM_RADIUS) & ~3, xr1 = sh.X - s.npml + RTM_RADIUS;
+        const int zr0 = s.npml - RTM_RADIUS, zr1 = sh.Z - s.npml + RTM_RADIUS;
+        auto add_tiles = [&](std::vector<TileRef> &v, int bz, int xa, int xb, int za, int zb) {
+            for (int z0 = za; z0 < zb; z0 += bz)
+                for (int x0 = xa; x0 < xb; x0 += RTM_BX) v.push_back({j, x0, z0});
+        };
+        add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
+        add_tiles(tiles_p, ss->bz_pres, 0, sh.X, 0, sh.Z);
+        add_tiles(tiles_r, ss->bz_vel, xr0, xr1, zr0, zr1);
+        add_tiles(tiles_pr, ss->bz_pres, xr0, xr1, zr0, zr1);
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
         br.max_strip_len = std::max(br.max_strip_len, sh.strip_len);
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
@@ -545,10 +558,14 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     }
     br.ntiles = (int)tiles.size();
     br.ntiles_p = (int)tiles_p.size();
+    br.ntiles_r = (int)tiles_r.size();
+    br.ntiles_pr = (int)tiles_pr.size();
     CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles, tiles.data(), sizeof(TileRef) * br.ntiles, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles_p, tiles_p.data(), sizeof(TileRef) * br.ntiles_p, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ss->d_tiles_r, tiles_r.data(), sizeof(TileRef) * br.ntiles_r, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ss->d_tiles_pr, tiles_pr.data(), sizeof(TileRef) * br.ntiles_pr, cudaMemcpyHostToDevice, st));
     StepArgs &a = br.a;
     std::memset(&a, 0, sizeof(a));
     a.shots = ss->d_shots;
@@ -648,12 +665,12 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         // reconstruction of the source wavefield, then the receiver wavefield and imaging
         // (which reads the reconstructed pressure of the same step)
         timing_begin(ss, "vel_recon", it, &e);
-        a.tiles = ss->d_tiles;
-        launch_vel(RTM_WAVE_RECON, ss->bz_vel, a, br.ntiles, st);
+        a.tiles = ss->d_tiles_r;
+        launch_vel(RTM_WAVE_RECON, ss->bz_vel, a, br.ntiles_r, st);
         timing_end(ss, e);
         timing_begin(ss, "pres_recon", it, &e);
-        a.tiles = ss->d_tiles_p;
-        launch_pres(RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_p, 0, st);
+        a.tiles = ss->d_tiles_pr;
+        launch_pres(RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0, st);
         timing_end(ss, e);
         timing_begin(ss, "vel_recv", it, &e);
         a.tiles = ss->d_tiles;

@@ -327,12 +327,10 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1vz[BZ], s_ic2vz[BZ];
-    const TileRef t = a.tiles[blockIdx.x];
+    const TileRef t = a.tiles[blockIdx.x];   // reconstruction: tiles of the interior + strips only
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
-    const int x0 = (t.tile % S.ntx) * BX, z0 = (t.tile / S.ntx) * BZ;
-    if (MODE == 3 && (z0 + BZ <= npml - R || z0 >= Z - npml + R || x0 + BX <= npml - R || x0 >= X - npml + R))
-        return;   // tile outside the reconstruction region (interior + strips)
+    const int x0 = t.x0, z0 = t.z0;
     const WaveDev W = (MODE == 2) ? S.b : S.a;
     const float *__restrict__ inv_rho = (MODE >= 2) ? S.inv_rho_b : S.inv_rho_f;
     const PmlOffsets o = pml_offsets(X, Z);
@@ -470,12 +468,10 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 6 : (MODE == 0 ? 0 : (sizeof(A
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1z[BZ], s_ic2z[BZ];
-    const TileRef t = a.tiles[blockIdx.x];
+    const TileRef t = a.tiles[blockIdx.x];   // reconstruction: tiles of the interior + strips only
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
-    const int x0 = (t.tile % S.ntx) * BX, z0 = (t.tile / S.ntx) * BZ;
-    if (MODE == 3 && (z0 + BZ <= npml - R || z0 >= Z - npml + R || x0 + BX <= npml - R || x0 >= X - npml + R))
-        return;
+    const int x0 = t.x0, z0 = t.z0;
     const WaveDev W = (MODE == 2) ? S.b : S.a;
     const float *__restrict__ kappa = (MODE >= 2) ? S.kappa_b : S.kappa_f;
     const PmlOffsets o = pml_offsets(X, Z);

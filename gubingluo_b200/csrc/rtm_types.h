@@ -86,9 +86,11 @@ enum RtmTmap { RTM_TMAP_A_P = 0, RTM_TMAP_A_VX, RTM_TMAP_A_VZ, RTM_TMAP_B_P, RTM
                RTM_TMAP_COUNT };
 #define RTM_TMAP_BYTES 128
 
+// One block's work: the tile of `shot` whose top-left cell is (x0, z0).  x0 is a multiple of
+// 4, so the staged box (from x0-12) starts on a 16-byte boundary.
 struct TileRef {
     int shot;
-    int tile;
+    int x0, z0;
 };
 
 // Kernel-wide constants of one launch.
