@@ -10,7 +10,8 @@
 //     matching cudaFree performs.
 // The image travels through one fixed scratch area that is part of this translation unit's
 // device image: a file-scope __device__ array of kScratchCells cells for the input copy and as
-// many for the filtered result (48 MiB per device in all).  Images above kScratchCells cells
+// many for the filtered result (48 MiB per device in all, kept by every GPU on which this
+// library's device code is loaded until the process exits).  Images above kScratchCells cells
 // are refused.  Nothing in the scratch has to start at zero: every call copies the whole image
 // in, and the kernel writes every output cell (the border included).  There is one scratch
 // area per device, so calls on the same device must not overlap in time: two concurrent calls
@@ -32,10 +33,12 @@ static __device__ __align__(256) float g_scratch[2 * kScratchCells];
 
 // Same arithmetic as the host filter: sums of float neighbours, the centre term and the
 // division in double, each axis rounded to float before the two are added; border cells 0.
-__global__ void k_laplace_scratch(int nx, int nz, int dx, int dz)
+// `scratch` is the device address of g_scratch (the host looks it up; in host code the
+// array's name stands for a host-side shadow, not for device memory).
+__global__ void k_laplace_scratch(float *scratch, int nx, int nz, int dx, int dz)
 {
-    const float *in = g_scratch;
-    float *out = g_scratch + kScratchCells;
+    const float *in = scratch;
+    float *out = scratch + kScratchCells;
     const long n = (long)nx * nz;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const int iz = (int)(i / nx), ix = (int)(i - (long)iz * nx);
@@ -88,7 +91,7 @@ extern "C" int rtm_laplace_image_noalloc(float *image, int nx, int nz, int dx, i
     if ((e = cudaMemcpy(base, image, bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
         return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
     const int blocks = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
-    k_laplace_scratch<<<blocks, 256>>>(nx, nz, dx, dz);
+    k_laplace_scratch<<<blocks, 256>>>(base, nx, nz, dx, dz);
     if ((e = cudaGetLastError()) != cudaSuccess) return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
     if ((e = cudaMemcpy(image, base + kScratchCells, bytes, cudaMemcpyDeviceToHost)) != cudaSuccess)
         return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
