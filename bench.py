@@ -6,8 +6,8 @@ source-illumination-normalised imaging), synthetic seeded model.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step migrates --shots-per-step shots per GPU (mode 1: recorded gathers in, stacked images
-out).  `value` times K steps with the gathers already resident in device memory; `e2e` times
+One step migrates --shots-per-step shots per GPU as one batch (default 64: the whole survey;
+mode 1: recorded gathers in, stacked images out).  `value` times K steps with the gathers already resident in device memory; `e2e` times
 K steps through the same public C-ABI with each step's gathers copied from pinned host memory
 and the stacked image read back.  Under torchrun each rank migrates its own shots (weak
 scaling); the ranks' partial images are summed with one NCCL all-reduce after the timed
@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
-    ap.add_argument("--shots-per-step", type=int, default=16)
+    ap.add_argument("--shots-per-step", type=int, default=64,
+                    help="shots per step and GPU, run as one batch (default: the whole 64-shot survey)")
     ap.add_argument("--batch", type=int, default=0, help="shots per launch (0: all shots of a step)")
     ap.add_argument("--nt", type=int, default=0, help="override nt (quick runs only)")
     ap.add_argument("--strips", default="fp32", choices=["fp32", "fp16", "bf16"])
