@@ -64,6 +64,11 @@ def lib():
         for name in ("orc_shot_f32", "orc_shot_f64"):
             getattr(L, name).argtypes = [C.POINTER(OrcShot)] + [_vp] * 6 + [C.c_int, _vp, C.c_int, C.c_int,
                                                                              C.c_int] + [_vp] * 4
+        for name in ("orc_shot_ex_f32", "orc_shot_ex_f64"):
+            getattr(L, name).argtypes = [C.POINTER(OrcShot)] + [_vp] * 6 + [C.c_int, _vp, C.c_int, C.c_int,
+                                                                             C.c_int] + [_vp] * 4 + [C.c_int] + [_vp] * 4
+        for name in ("orc_finalize_extra_f32", "orc_finalize_extra_f64"):
+            getattr(L, name).argtypes = [_vp] * 5 + [C.c_int] * 4 + [_vp] * 7
         for name in ("orc_forward_f32", "orc_forward_f64"):
             getattr(L, name).argtypes = [C.POINTER(OrcShot), _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp]
         L.orc_finalize_f32.argtypes = [_vp, _vp] + [C.c_int] * 4 + [_vp] * 3
@@ -168,9 +173,11 @@ def forward(shot: OrcShot, vp2, rho, nsteps, precision="f32", coef=None, wavelet
 
 
 def shot(shot: OrcShot, vp2f, rhof, vp2b=None, rhob=None, mode=1, gather=None, mute=1, nw=0,
-         tlength=0, precision="f32", coef=None, wavelet=None, want_fields=False):
+         tlength=0, precision="f32", coef=None, wavelet=None, want_fields=False, extra=0):
     """One shot of RTM (source pass, backward loop, imaging); returns dict with g1, illum,
-    gather (modelled in mode 0) and optionally the final ps/p wavefields."""
+    gather (modelled in mode 0) and optionally the final ps/p wavefields.  extra = 1 or 2
+    adds the decomposition, Poynting and energy-norm images g2, g3, g3t, g4 (2: with the
+    reference's indexing of vx and vz)."""
     dt = np.float32 if precision == "f32" else np.float64
     nzi, nxi = shot.Z - 2 * shot.npml, shot.X - 2 * shot.npml
     g1 = np.zeros((nzi, nxi), dt)
@@ -185,27 +192,31 @@ def shot(shot: OrcShot, vp2f, rhof, vp2b=None, rhob=None, mode=1, gather=None, m
     vp2f, rhof = f32(vp2f), f32(rhof)
     vp2b = vp2f if vp2b is None else f32(vp2b)
     rhob = rhof if rhob is None else f32(rhob)
-    fn = lib().orc_shot_f32 if precision == "f32" else lib().orc_shot_f64
+    ex = [np.zeros((nzi, nxi), dt) for _ in range(4)] if extra else [None] * 4
+    fn = lib().orc_shot_ex_f32 if precision == "f32" else lib().orc_shot_ex_f64
     rc = fn(C.byref(shot), _p(vp2f), _p(rhof), _p(vp2b), _p(rhob), _p(coef),
             _p(None if wavelet is None else f32(wavelet)), mode, _p(gather), mute, nw, tlength,
-            _p(g1), _p(il), _p(ps), _p(pr))
+            _p(g1), _p(il), _p(ps), _p(pr), extra, *[_p(a) for a in ex])
     if rc:
         raise MemoryError("oracle allocation failed")
-    return dict(g1=g1, illum=il, gather=gather, ps=ps, p=pr)
+    return dict(g1=g1, illum=il, gather=gather, ps=ps, p=pr, g2=ex[0], g3=ex[1], g3t=ex[2], g4=ex[3])
 
 
 def rtm_model(survey: dict, shots, vp, rho, vp_mig=None, rho_mig=None, gathers=None,
-              precision="f32", keep_fields=False):
+              precision="f32", keep_fields=False, extra=0):
     """Restatement of the reference's rtm_model shot loop for one layout (mode 0 models each
     gather in (vp, rho) first; mode 1 migrates ``gathers``).  ``survey`` keys: nx nz nt dx dz
     dt npml fdom amp alp layout spx0 spz0 dspx offset offsetmax mode medium_flag ismth direct
-    direct0 mute receiver_depth.  Returns stacked images (+ gathers)."""
+    direct0 mute receiver_depth.  Returns stacked images (+ gathers); with extra = 1 or 2
+    also image3s, image4s, image5s, image3m, image4m, image5m and imagetrue."""
     s = survey
     nx, nz = s["nx"], s["nz"]
     acc = np.float32 if precision == "f32" else np.float64
     image1 = np.zeros((nz, nx), acc)
     image2s = np.zeros((nz, nx), acc)
     illum = np.zeros((nz, nx), acc)
+    xnames = ("image3s", "image4s", "image5s", "image3m", "image4m", "image5m", "imagetrue")
+    ximg = {k: np.zeros((nz, nx), acc) for k in xnames} if extra else {}
     out_gathers, fields = [], []
     nw = int(np.float32(s["direct"]) / (np.float32(s["fdom"]) * np.float32(s["dt"])))
     tlength = int(np.float32(s["direct0"]) / np.float32(s["dt"]))
@@ -230,15 +241,20 @@ def rtm_model(survey: dict, shots, vp, rho, vp_mig=None, rho_mig=None, gathers=N
                          s["amp"], s["alp"], s["fdom"], rz, g.rx0, g.nrec, vpmax)
         r = globals()["shot"](sh, vp2f, rhof, vp2b, rhob, mode=s["mode"],
                               gather=None if s["mode"] == 0 else gathers[k], mute=s.get("mute", 1),
-                              nw=nw, tlength=tlength, precision=precision, want_fields=keep_fields)
+                              nw=nw, tlength=tlength, precision=precision, want_fields=keep_fields,
+                              extra=extra)
         out_gathers.append(r["gather"])
         if keep_fields:
             fields.append((r["ps"], r["p"]))
         fin = lib().orc_finalize_f32 if precision == "f32" else lib().orc_finalize_f64
         img2m = np.zeros_like(image1)
         fin(_p(r["g1"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1, _p(image1), _p(image2s), _p(illum))
+        if extra:   # after fin, which tapered r["illum"] in place
+            fx = lib().orc_finalize_extra_f32 if precision == "f32" else lib().orc_finalize_extra_f64
+            fx(_p(r["g2"]), _p(r["g3"]), _p(r["g4"]), _p(r["g3t"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1,
+               *[_p(ximg[k]) for k in xnames])
     return dict(image1=image1, image2s=image2s, image2m=image1.copy(), illum=illum,
-                gathers=out_gathers, fields=fields)
+                gathers=out_gathers, fields=fields, **ximg)
 
 
 # ---- the reference's own host code (compiled from its sources) ----

@@ -555,6 +555,35 @@ void orc_finalize_f64(double *g1, double *illum, int nxlen, int nz, int nx, int 
     free(taper);
 }
 
+#define FIN_EXTRA(T, NAME)                                                                              \
+    void NAME(T *g2, T *g3, T *g4, T *g3t, const T *illum, int nxlen, int nz, int nx, int nx1, T *image3s,     \
+              T *image4s, T *image5s, T *image3m, T *image4m, T *image5m, T *imagetrue)                     \
+    {                                                                                                          \
+        int ix, iz;                                                                                            \
+        float *taper = (float *)malloc(sizeof(float) * nxlen);                                                 \
+        orc_taper(taper, nxlen, orc_taper_nwin(nxlen), 0.06f);                                                 \
+        for (iz = 0; iz < nz; iz++)                                                                            \
+            for (ix = 0; ix < nxlen; ix++) {                                                                   \
+                size_t ip = (size_t)iz * nxlen + ix, jf = (size_t)iz * nx + ix + nx1;                          \
+                g2[ip] *= taper[ix];                                                                           \
+                g3[ip] *= taper[ix];                                                                           \
+                g4[ip] *= taper[ix];                                                                           \
+                g3t[ip] *= taper[ix];                                                                          \
+                image3s[jf] = (T)(image3s[jf] + g2[ip] / (illum[ip] + 1.0e-6));                                \
+                image4s[jf] = (T)(image4s[jf] + g3[ip] / (illum[ip] + 1.0e-6));                                \
+                image5s[jf] = (T)(image5s[jf] + g4[ip] / (illum[ip] + 1.0e-6));                                \
+                image3m[jf] += g2[ip];                                                                         \
+                image4m[jf] += g3[ip];                                                                         \
+                image5m[jf] += g4[ip];                                                                         \
+                imagetrue[jf] += g3t[ip];                                                                      \
+            }                                                                                                  \
+        free(taper);                                                                                           \
+    }
+/* cuda_taper_image + cuda_applyics / cuda_applyic for the extra images (kernel.cu:1556-1604) */
+FIN_EXTRA(float, orc_finalize_extra_f32)
+FIN_EXTRA(double, orc_finalize_extra_f64)
+#undef FIN_EXTRA
+
 /* ---- precision-templated hot path ---- */
 #define R float
 #define SFX(x) x##_f32

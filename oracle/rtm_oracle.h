@@ -102,6 +102,23 @@ int orc_shot_f64(const orc_shot *s, const float *vp2f, const float *rhof,
                  const float *wavelet, int mode, float *gather, int mute, int nw,
                  int tlength, double *g1, double *illum, double *ps_out, double *p_out);
 
+/* orc_shot with the extra imaging conditions of the reference's backward loop
+ * (rtm_model.cu:450-455, kernel.cu:1417-1522) accumulated into g2 (wavefield decomposition),
+ * g3 (Poynting angle weighting, all angle bins summed), g3t (its true-amplitude variant) and
+ * g4 (energy norm), nz*nxlen each, when extra != 0.  extra == 2 reproduces the reference's
+ * indexing (vx read at the pressure cell's flat index on the (X-1)-wide vx arrays; receiver
+ * vz in the source term of the Poynting vector); extra == 1 reads both at their own cells. */
+int orc_shot_ex_f32(const orc_shot *s, const float *vp2f, const float *rhof,
+                    const float *vp2b, const float *rhob, const float *coef,
+                    const float *wavelet, int mode, float *gather, int mute, int nw,
+                    int tlength, float *g1, float *illum, float *ps_out, float *p_out,
+                    int extra, float *g2, float *g3, float *g3t, float *g4);
+int orc_shot_ex_f64(const orc_shot *s, const float *vp2f, const float *rhof,
+                    const float *vp2b, const float *rhob, const float *coef,
+                    const float *wavelet, int mode, float *gather, int mute, int nw,
+                    int tlength, double *g1, double *illum, double *ps_out, double *p_out,
+                    int extra, double *g2, double *g3, double *g3t, double *g4);
+
 /* Forward modelling only, nsteps steps from rest (source added, no strips).
  * Returns the final p (Z*X), vx (Z*(X-1)), vz ((Z-1)*X) and the gather (nsteps*nrec). */
 int orc_forward_f32(const orc_shot *s, const float *vp2, const float *rho, const float *coef,
@@ -118,6 +135,17 @@ void orc_finalize_f32(float *g1, float *illum, int nxlen, int nz, int nx, int nx
                       float *image1, float *image2s, float *illum_total);
 void orc_finalize_f64(double *g1, double *illum, int nxlen, int nz, int nx, int nx1,
                       double *image1, double *image2s, double *illum_total);
+
+/* The extra images of one shot (rtm_model.cu:466-487; kernel.cu:1556-1604): taper g2, g3, g4
+ * and g3t like g1, then image3s/4s/5s += g2/g3/g4 / (illum + 1e-6) with the shot's tapered
+ * illumination (call after orc_finalize, which tapers illum in place), image3m/4m/5m +=
+ * g2/g3/g4 and imagetrue += g3t, at column offset nx1. */
+void orc_finalize_extra_f32(float *g2, float *g3, float *g4, float *g3t, const float *illum, int nxlen, int nz,
+                            int nx, int nx1, float *image3s, float *image4s, float *image5s, float *image3m,
+                            float *image4m, float *image5m, float *imagetrue);
+void orc_finalize_extra_f64(double *g2, double *g3, double *g4, double *g3t, const double *illum, int nxlen,
+                            int nz, int nx, int nx1, double *image3s, double *image4s, double *image5s,
+                            double *image3m, double *image4m, double *image5m, double *imagetrue);
 
 /* Threads used by the OpenMP loops (1 when built without OpenMP). */
 int orc_num_threads(void);

@@ -343,6 +343,80 @@ static R *SFX(make_wavelet)(const orc_shot *s, const float *wavelet)
     return w;
 }
 
+/* Single-precision math in the float build (the reference's CUDA kernels call sqrtf, acosf,
+ * cosf and sinf), double precision in the double build. */
+static R SFX(m_sqrt)(R x) { return sizeof(R) == 4 ? (R)sqrtf((float)x) : (R)sqrt((double)x); }
+static R SFX(m_acos)(R x) { return sizeof(R) == 4 ? (R)acosf((float)x) : (R)acos((double)x); }
+static R SFX(m_cos)(R x) { return sizeof(R) == 4 ? (R)cosf((float)x) : (R)cos((double)x); }
+static R SFX(m_sin)(R x) { return sizeof(R) == 4 ? (R)sinf((float)x) : (R)sin((double)x); }
+
+/* The extra imaging conditions of one backward step, on the interior, after the receiver
+ * update (rtm_model.cu:450-455):
+ *   g2  wavefield decomposition (cuda_wavefield_decomposition, kernel.cu:1417-1451): the
+ *       up-down, down-up, left-right and right-left products; the reference keeps four
+ *       arrays and adds them after the last step (cuda_stack_udlr, :1523-1533), here they
+ *       go into one;
+ *   g3  Poynting-vector angle weighting ps p cos(theta) (cuda_poynting, :1452-1485); the
+ *       reference bins it by whole degrees of theta in 61 arrays and adds the bins after the
+ *       last step (cuda_stack_theta, :1534-1545), here it goes straight into the sum;
+ *   g3t its "true amplitude" variant ps p 16 pi v / sin(theta);
+ *   g4  energy norm (cuda_energynorm, :1486-1522): -(dps)(dp)/(dt^2 v^2) + grad ps . grad p
+ *       with the change over the step and centred first differences.
+ * extra == 2 reads vx as the reference does: at the pressure cell's flat index z*X + x on
+ * the (X-1)-wide vx arrays, and with the receiver's vz in the source term of the Poynting
+ * vector.  extra == 1 reads vx at its own cell (z, x) and the source's vz.  The operand
+ * types follow the reference's expressions (float values, double literals). */
+static void SFX(extra_imaging)(const SFX(wave) *ws, const SFX(wave) *w, const R *ps_pre, const R *p_pre,
+                               const R *vp2, int X, int Z, int npml, float dx, float dz, float dt, int extra,
+                               R *g2, R *g3, R *g3t, R *g4)
+{
+    const int nzi = Z - 2 * npml, nxi = X - 2 * npml;
+    int iz;
+#pragma omp parallel for schedule(static)
+    for (iz = 0; iz < nzi; iz++) {
+        int ix;
+        for (ix = 0; ix < nxi; ix++) {
+            const int idz = iz + npml, idx = ix + npml;
+            const size_t id = (size_t)idz * X + idx, im = (size_t)iz * nxi + ix;
+            const size_t ivx = extra == 2 ? id : (size_t)idz * (X - 1) + idx;
+            const R ps = ws->p[id], p = w->p[id];
+            const R vxs = ws->vx[ivx], vx = w->vx[ivx], vzs = ws->vz[id], vz = w->vz[id];
+            /* decomposition */
+            const R vectxs = -ps * vxs, vectzs = -ps * vzs, vectxr = -p * vx, vectzr = -p * vz;
+            const R psu = vectzs < 0 ? ps : 0, psd = vectzs > 0 ? ps : 0;
+            const R psl = vectxs < 0 ? ps : 0, psr = vectxs > 0 ? ps : 0;
+            const R pu = vectzr < 0 ? p : 0, pd = vectzr > 0 ? p : 0;
+            const R pl = vectxr < 0 ? p : 0, pr = vectxr > 0 ? p : 0;
+            g2[im] += psu * pd + psd * pu + psl * pr + psr * pl;
+            /* Poynting angle */
+            {
+                const R ksx = ps * vxs, ksz = ps * (extra == 2 ? vz : vzs), krx = p * vx, krz = p * vz;
+                const R q = (ksx * ksx + ksz * ksz) * (krx * krx + krz * krz);
+                const double den = SFX(m_sqrt)(q) > 0 ? (double)SFX(m_sqrt)(q) : 1.0e-6;
+                R wt = (R)((double)(ksx * krx + ksz * krz) / den);
+                if (wt >= -1.0 && wt <= 1.0) {
+                    wt = (R)(0.5 * (double)SFX(m_acos)(wt));
+                    wt = (R)(ORC_PI / 2.0 - (double)wt);
+                    if (wt > 0 && wt <= ORC_PI / 3.0) {
+                        g3[im] += ps * p * SFX(m_cos)(wt);
+                        g3t[im] = (R)((double)g3t[im] + (double)(ps * p) * 16.0 * ORC_PI *
+                                                           (double)SFX(m_sqrt)(vp2[id]) / (double)SFX(m_sin)(wt));
+                    }
+                }
+            }
+            /* energy norm */
+            {
+                const R psx = (R)(0.5 * (double)(ws->p[id + 1] - ws->p[id - 1]) / dx);
+                const R psz = (R)(0.5 * (double)(ws->p[id + X] - ws->p[id - X]) / dz);
+                const R px = (R)(0.5 * (double)(w->p[id + 1] - w->p[id - 1]) / dx);
+                const R pz = (R)(0.5 * (double)(w->p[id + X] - w->p[id - X]) / dz);
+                const R rdt = (R)dt;
+                g4[im] += -(ps - ps_pre[id]) * (p - p_pre[id]) / (rdt * rdt * vp2[id]) + psx * px + psz * pz;
+            }
+        }
+    }
+}
+
 int SFX(orc_forward)(const orc_shot *s, const float *vp2, const float *rho, const float *coef,
                      const float *wavelet, int nsteps, R *p, R *vx, R *vz, R *gather)
 {
@@ -372,10 +446,10 @@ int SFX(orc_forward)(const orc_shot *s, const float *vp2, const float *rho, cons
     return 0;
 }
 
-int SFX(orc_shot)(const orc_shot *s, const float *vp2f, const float *rhof, const float *vp2b,
-                  const float *rhob, const float *coef, const float *wavelet, int mode,
-                  float *gather, int mute, int nw, int tlength, R *g1, R *illum, R *ps_out,
-                  R *p_out)
+int SFX(orc_shot_ex)(const orc_shot *s, const float *vp2f, const float *rhof, const float *vp2b,
+                     const float *rhob, const float *coef, const float *wavelet, int mode,
+                     float *gather, int mute, int nw, int tlength, R *g1, R *illum, R *ps_out,
+                     R *p_out, int extra, R *g2, R *g3, R *g3t, R *g4)
 {
     const int X = s->X, Z = s->Z, npml = s->npml, nt = s->nt;
     const int nzi = Z - 2 * npml, nxi = X - 2 * npml;
@@ -392,7 +466,9 @@ int SFX(orc_shot)(const orc_shot *s, const float *vp2f, const float *rhof, const
     R *svz = (R *)malloc(sizeof(R) * lh * nt), *sptb = (R *)malloc(sizeof(R) * lh * nt);
     R *rec = (R *)malloc(sizeof(R) * (size_t)nt * s->nrec);
     float *mig = (float *)malloc(sizeof(float) * (size_t)nt * s->nrec);
-    if (!svx || !splr || !svz || !sptb || !rec || !mig) return -1;
+    R *ps_pre = extra ? (R *)malloc(sizeof(R) * n) : NULL, *p_pre = extra ? (R *)malloc(sizeof(R) * n) : NULL;
+    if (!svx || !splr || !svz || !sptb || !rec || !mig || (extra && (!ps_pre || !p_pre || !g2 || !g3 || !g3t || !g4)))
+        return -1;
 
     SFX(ctx_init)(&c, s, coef);
     SFX(wave_alloc)(&w, X, Z, npml);
@@ -427,10 +503,16 @@ int SFX(orc_shot)(const orc_shot *s, const float *vp2f, const float *rhof, const
     SFX(wave_free)(&w);
     SFX(wave_alloc)(&w, X, Z, npml);
     for (i = 0; i < (size_t)nzi * nxi; i++) { g1[i] = 0; illum[i] = 0; }
+    if (extra)
+        for (i = 0; i < (size_t)nzi * nxi; i++) { g2[i] = 0; g3[i] = 0; g3t[i] = 0; g4[i] = 0; }
     c.vp2 = m_vp2b; c.rho = m_rhob;
     for (j = 0; j < s->nrec; j++)                               /* kernel.cu:72-79 */
         w.p[(size_t)s->rz * X + s->rx0 + j] = c.dt * rec[(size_t)(nt - 1) * s->nrec + j];
     for (it = nt - 2; it >= 0; it--) {
+        if (extra) {   /* the pressures before this step, for the energy norm (rtm_model.cu:419-420) */
+            memcpy(ps_pre, ws.p, sizeof(R) * n);
+            memcpy(p_pre, w.p, sizeof(R) * n);
+        }
         SFX(strips_io)(&ws, X, Z, npml, svx + lv * (it + 1), svz + lh * (it + 1), NULL, NULL, 0, 1);
         SFX(bwd_v)(&ws, &c);
         SFX(strips_io)(&ws, X, Z, npml, NULL, NULL, splr + lv * it, sptb + lh * it, 0, 2);
@@ -453,6 +535,9 @@ int SFX(orc_shot)(const orc_shot *s, const float *vp2f, const float *rhof, const
                 }
             }
         }
+        if (extra)
+            SFX(extra_imaging)(&ws, &w, ps_pre, p_pre, m_vp2b, X, Z, npml, s->dx, s->dz, s->dt, extra, g2, g3, g3t,
+                               g4);
     }
     if (ps_out) memcpy(ps_out, ws.p, sizeof(R) * n);
     if (p_out) memcpy(p_out, w.p, sizeof(R) * n);
@@ -462,5 +547,15 @@ int SFX(orc_shot)(const orc_shot *s, const float *vp2f, const float *rhof, const
     SFX(ctx_free)(&c);
     free(m_vp2f); free(m_rhof); free(m_vp2b); free(m_rhob);
     free(src); free(wl); free(svx); free(splr); free(svz); free(sptb); free(rec); free(mig);
+    free(ps_pre); free(p_pre);
     return 0;
+}
+
+int SFX(orc_shot)(const orc_shot *s, const float *vp2f, const float *rhof, const float *vp2b,
+                  const float *rhob, const float *coef, const float *wavelet, int mode,
+                  float *gather, int mute, int nw, int tlength, R *g1, R *illum, R *ps_out,
+                  R *p_out)
+{
+    return SFX(orc_shot_ex)(s, vp2f, rhof, vp2b, rhob, coef, wavelet, mode, gather, mute, nw, tlength, g1, illum,
+                            ps_out, p_out, 0, NULL, NULL, NULL, NULL);
 }
