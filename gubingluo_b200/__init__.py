@@ -40,7 +40,7 @@ class Survey(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("strip_precision", C.c_int), ("gather_precision", C.c_int),
                 ("accum_fp64", C.c_int), ("batch", C.c_int), ("use_graph", C.c_int),
-                ("verbose", C.c_int)]
+                ("verbose", C.c_int), ("extra_images", C.c_int)]
 
 
 class Geometry(C.Structure):
@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
     L.rtm_session_image_ptrs.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
     L.rtm_session_get_images.argtypes = [vp, vp, vp, vp, vp]
     L.rtm_session_get_images_f64.argtypes = [vp, vp, vp, vp]
+    L.rtm_session_get_images_extra.argtypes = [vp] * 8
     L.rtm_session_reset_images.argtypes = [vp]
     L.rtm_session_nrec.argtypes = [vp, C.c_int]
     L.rtm_session_stream.argtypes = [vp]
@@ -188,6 +189,7 @@ class RunOptions:
     batch: int = 0
     use_graph: bool = False
     verbose: bool = False
+    extra_images: int = 0   # 1: image3/4/5 and imagetrue, indexing corrected; 2: the reference's
 
     def c(self) -> Options:
         o = Options()
@@ -198,6 +200,7 @@ class RunOptions:
         o.batch = self.batch
         o.use_graph = int(self.use_graph)
         o.verbose = int(self.verbose)
+        o.extra_images = int(self.extra_images)
         return o
 
 
@@ -270,6 +273,15 @@ class Session:
         _check(lib().rtm_session_get_images_f64(self.h, *[_ptr(a) for a in out]))
         return dict(zip(("image1", "image2s", "illum"), out))
 
+    EXTRA_IMAGES = ("image3s", "image4s", "image5s", "image3m", "image4m", "image5m", "imagetrue")
+
+    def images_extra(self):
+        """The other imaging conditions' stacked images (options.extra_images != 0)."""
+        n = (self.survey.nz, self.survey.nx)
+        out = [np.zeros(n, np.float32) for _ in self.EXTRA_IMAGES]
+        _check(lib().rtm_session_get_images_extra(self.h, *[_ptr(a) for a in out]))
+        return dict(zip(self.EXTRA_IMAGES, out))
+
     def reset_images(self):
         _check(lib().rtm_session_reset_images(self.h))
 
@@ -331,6 +343,8 @@ def migrate(survey: SurveyConfig, options: RunOptions, shots, vp, rho, gathers=N
         out = ss.images()
         if options.accum_fp64:
             out["f64"] = ss.images_f64()
+        if options.extra_images:
+            out.update(ss.images_extra())
         if survey.mode == 0:
             out["gathers"] = [ss.gather(k) for k in range(len(ss.shots))]
         out["stats"] = stats

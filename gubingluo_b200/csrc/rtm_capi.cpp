@@ -63,6 +63,10 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
     o.accum_fp64 = env_int("RTM_B200_ACCUM_FP64", 0);
     o.batch = env_int("RTM_B200_BATCH", 0);
     o.verbose = 1;
+    // image3*/4*/5* and Imagetrue: the reference's other imaging conditions, with vx and vz
+    // read at their own cells (1, the default) or with the reference's indexing (2); 0 leaves
+    // those images zero and saves their cost
+    o.extra_images = env_int("RTM_B200_EXTRA_IMAGES", 1);
     const size_t nimg = (size_t)nx * nz;
     float *zero_imgs[6] = {image3s, image4s, image5s, image3m, image4m, image5m};
     for (float *p : zero_imgs)
@@ -102,7 +106,9 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
         }
     }
     const int B = session_batch_size(ss);
-    std::vector<float> tmp(nimg), zeros(nimg, 0.0f);
+    std::vector<float> tmp(nimg);
+    std::vector<float> xi[7];   // image3s .. image5m, imagetrue (zero unless extra_images)
+    for (auto &v : xi) v.assign(nimg, 0.0f);
     for (size_t k0 = 0; k0 < shots.size(); k0 += B) {
         int n = (int)std::min<size_t>(B, shots.size() - k0);
         auto t0 = std::chrono::steady_clock::now();
@@ -132,13 +138,16 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
             float *outs[4] = {image1, image2s, image2m, illum};
             rtm_session_get_images(ss, outs[0] ? outs[0] : tmp.data(), image2s ? image2s : tmp.data(),
                                    image2m ? image2m : tmp.data(), illum ? illum : tmp.data());
+            if (o.extra_images)
+                rtm_session_get_images_extra(ss, xi[0].data(), xi[1].data(), xi[2].data(), xi[3].data(),
+                                             xi[4].data(), xi[5].data(), xi[6].data());
             struct {
                 const char *name;
                 const float *img;
-            } temps[] = {{"Image2stemp", image2s}, {"Image3stemp", zeros.data()}, {"Image4stemp", zeros.data()},
-                         {"Image5stemp", zeros.data()}, {"Image1temp", image1}, {"Illumtemp", illum},
-                         {"Image2mtemp", image2m}, {"Image3mtemp", zeros.data()}, {"Image4mtemp", zeros.data()},
-                         {"Image5mtemp", zeros.data()}, {"Imagetruetemp", zeros.data()}};
+            } temps[] = {{"Image2stemp", image2s}, {"Image3stemp", xi[0].data()}, {"Image4stemp", xi[1].data()},
+                         {"Image5stemp", xi[2].data()}, {"Image1temp", image1}, {"Illumtemp", illum},
+                         {"Image2mtemp", image2m}, {"Image3mtemp", xi[3].data()}, {"Image4mtemp", xi[4].data()},
+                         {"Image5mtemp", xi[5].data()}, {"Imagetruetemp", xi[6].data()}};
             for (auto &t : temps) {
                 if (!t.img) continue;
                 std::snprintf(path, sizeof(path), "./output/%s.su", t.name);
@@ -147,8 +156,10 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
         }
     }
     rtm_session_get_images(ss, image1, image2s, image2m, illum);   // rtm_model.cu:575-585
+    if (o.extra_images)
+        rtm_session_get_images_extra(ss, image3s, image4s, image5s, image3m, image4m, image5m, xi[6].data());
     std::snprintf(path, sizeof(path), "./output/%dImagetrue.su", idevice);
-    if (write_image_su(path, zeros.data(), nz, nx, dx)) std::printf("The file %s open failed !\n", path);
+    if (write_image_su(path, xi[6].data(), nz, nx, dx)) std::printf("The file %s open failed !\n", path);
     rtm_session_close(ss);
 }
 

@@ -51,6 +51,7 @@ struct Arena {
 
 struct ModelDev {       // one padded model pair on the device
     float *inv_rho = nullptr, *kappa = nullptr;
+    float *vp2 = nullptr;  // v^2, kept only for the other imaging conditions
 };
 
 struct ShotState {
@@ -74,6 +75,8 @@ struct Slot {
     void *strips = nullptr;
     float *strip_scale = nullptr, *strip_stage = nullptr;
     void *g1 = nullptr, *illum = nullptr;
+    void *gx[4] = {nullptr, nullptr, nullptr, nullptr};   // other imaging conditions (g2, g3, g3t, g4)
+    float *ps_pre = nullptr, *p_pre = nullptr;           // pressures before the current backward step
 };
 
 struct KernelTiming {
@@ -96,6 +99,7 @@ struct rtm_session {
     float *wavelet = nullptr, *coef = nullptr;
     float coef_host[100];
     void *img1 = nullptr, *img2s = nullptr, *img2m = nullptr, *illum = nullptr;
+    void *ximg[7] = {};              // image3s, image4s, image5s, image3m, image4m, image5m, imagetrue
     ShotDev *d_shots = nullptr;
     TileRef *d_tiles = nullptr;      // tiles of the velocity kernels (whole padded grid)
     TileRef *d_tiles_p = nullptr;    // tiles of the pressure kernels (whole padded grid)
@@ -196,6 +200,15 @@ static void prep_model(const rtm_survey &s, const float *vp, const float *rho, i
 static int upload_model(rtm_session *ss, const std::vector<float> &vp2, const std::vector<float> &rho, int X, int Z,
                         int pitch, ModelDev &m)
 {
+    if (ss->o.extra_images) {   // v^2 for the Poynting and energy-norm imaging conditions
+        std::vector<float> v((size_t)pitch * Z, 0.0f);
+        for (int z = 0; z < Z; z++)
+            for (int x = 0; x < X; x++) v[(size_t)z * pitch + x] = vp2[(size_t)z * X + x];
+        m.vp2 = (float *)ss->arena.take(sizeof(float) * v.size());
+        if (!m.vp2) return fail(RTM_ERR_NOMEM, "device arena exhausted (models)");
+        CK(cudaMemcpyAsync(m.vp2, v.data(), sizeof(float) * v.size(), cudaMemcpyHostToDevice, ss->stream));
+        CK(cudaStreamSynchronize(ss->stream));
+    }
     std::vector<float> ir((size_t)pitch * Z, 0.0f), ka((size_t)pitch * Z, 0.0f);
     for (int z = 0; z < Z; z++)
         for (int x = 0; x < X; x++) {
@@ -222,6 +235,7 @@ static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, i
         b += (size_t)kRing * strip_len * sizeof(float) + 256;
     }
     b += 2 * ((size_t)pitch * Z * (o.accum_fp64 ? 8 : 4) + 256);   // g1, illum on the padded grid
+    if (o.extra_images) b += 4 * ((size_t)pitch * Z * (o.accum_fp64 ? 8 : 4) + 256) + 2 * field;
     (void)nxi;
     (void)nzi;
     return b;
@@ -283,7 +297,8 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     size_t model_bytes = 0;
     for (auto &w : windows) {
         int X = w.first.second - w.first.first + 1 + 2 * s.npml;
-        model_bytes += (sep_b ? 4 : 2) * ((size_t)round_up(X, 32) * ss->Z * 4 + 256);
+        model_bytes += ((sep_b ? 4 : 2) + (o.extra_images ? (sep_b ? 2 : 1) : 0)) *
+                       ((size_t)round_up(X, 32) * ss->Z * 4 + 256);
     }
     // device memory plan
     size_t free_b = 0, total_b = 0;
@@ -291,7 +306,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     const ShotState &big = *std::max_element(ss->shots.begin(), ss->shots.end(),
                                              [](const ShotState &a, const ShotState &b) { return a.X < b.X; });
     size_t per_slot = slot_bytes(s, o, big.pitch, big.Z, big.strip_len, big.nxi, big.nzi);
-    size_t fixed = model_bytes + shot_bytes_total + 4 * ((size_t)s.nx * s.nz * 8 + 256) + (size_t)s.nt * 4 + 4096 +
+    size_t fixed = model_bytes + shot_bytes_total + (o.extra_images ? 11 : 4) * ((size_t)s.nx * s.nz * 8 + 256) + (size_t)s.nt * 4 + 4096 +
                    (size_t)(64 << 20);
     size_t budget = (size_t)(free_b * 0.92);
     if (fixed + per_slot > budget) return fail(RTM_ERR_NOMEM, "survey does not fit in device memory");
@@ -302,6 +317,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         if (e && *e) ss->bz_vel = std::atoi(e);
         e = std::getenv("RTM_B200_BZ_PRES");
         if (e && *e) ss->bz_pres = std::atoi(e);
+        if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
         for (int bz : {ss->bz_vel, ss->bz_pres})
             if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
     }
@@ -334,6 +350,11 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     CK(cudaMemsetAsync(ss->img2s, 0, isz, ss->stream));
     CK(cudaMemsetAsync(ss->img2m, 0, isz, ss->stream));
     CK(cudaMemsetAsync(ss->illum, 0, isz, ss->stream));
+    if (o.extra_images)
+        for (void *&im : ss->ximg) {
+            if (!(im = ss->arena.take(isz))) return fail(RTM_ERR_NOMEM, "device arena exhausted (images)");
+            CK(cudaMemsetAsync(im, 0, isz, ss->stream));
+        }
 
     // models
     std::map<std::pair<int, int>, std::pair<ModelDev, ModelDev>> mcache;
@@ -413,6 +434,13 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         sl.g1 = ss->arena.take(ib);
         sl.illum = ss->arena.take(ib);
         if (!sl.strips || !sl.g1 || !sl.illum) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
+        if (o.extra_images) {
+            for (void *&g : sl.gx)
+                if (!(g = ss->arena.take(ib))) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
+            sl.ps_pre = (float *)ss->arena.take((size_t)big.pitch * big.Z * 4);
+            sl.p_pre = (float *)ss->arena.take((size_t)big.pitch * big.Z * 4);
+            if (!sl.ps_pre || !sl.p_pre) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
+        }
     }
     // descriptor and tile tables, tensor maps, kernel error flag
     ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
@@ -521,6 +549,9 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         d.gather = s.mode == 0 ? sh.gather_raw : sh.gather32;
         d.gather_scale = nullptr;
         d.g1 = sl.g1; d.illum = sl.illum;
+        for (int k = 0; k < 4; k++) d.gx[k] = sl.gx[k];
+        d.ps_pre = sl.ps_pre; d.p_pre = sl.p_pre;
+        d.vp2_b = sh.mb.vp2;
         // tensor maps of the fields the stencil kernels stage, for this shot's row pitch
         {
             const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA, ph = ss->bz_pres + RTM_STAGE_ZEXTRA;
@@ -555,6 +586,8 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         size_t ib = (size_t)sh.pitch * sh.Z * (o.accum_fp64 ? 8 : 4);
         CK(cudaMemsetAsync(sl.g1, 0, ib, st));
         CK(cudaMemsetAsync(sl.illum, 0, ib, st));
+        if (o.extra_images)
+            for (void *g : sl.gx) CK(cudaMemsetAsync(g, 0, ib, st));
     }
     br.ntiles = (int)tiles.size();
     br.ntiles_p = (int)tiles_p.size();
@@ -659,6 +692,19 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     }
     launch_inject(ss->d_shots, n, br.maxrec, s.nt - 1, s.dt, o.gather_precision, st);
     ss->launches++;
+    // the other imaging conditions compare each step with the pressures before it
+    // (rtm_model.cu:419-420); their kernel keeps ps_pre/p_pre current from then on
+    int max_nxi = 0, max_nzi = 0;
+    if (o.extra_images)
+        for (int j = 0; j < n; j++) {
+            const ShotState &sh = ss->shots[br.k0 + j];
+            const Slot &sl = ss->slots[j];
+            const size_t fb = (size_t)sh.pitch * sh.Z * 4;
+            CK(cudaMemcpyAsync(sl.ps_pre, sl.a.p, fb, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(sl.p_pre, sl.b.p, fb, cudaMemcpyDeviceToDevice, st));
+            max_nxi = std::max(max_nxi, sh.nxi);
+            max_nzi = std::max(max_nzi, sh.nzi);
+        }
     for (int it = s.nt - 2; it >= 0; it--) {
         a.it = it;
         cudaEvent_t e;
@@ -681,6 +727,11 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         launch_pres(RTM_WAVE_RECEIVER, ss->bz_pres, a, br.ntiles_p, 0, st);
         timing_end(ss, e);
         ss->launches += 4;
+        if (o.extra_images) {
+            launch_image_extra(ss->d_shots, n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz, s.dt,
+                               st);
+            ss->launches++;
+        }
     }
     CK(cudaGetLastError());
     std::vector<char> fin(finalize_shot_size() * n);
@@ -688,12 +739,16 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         ShotState &sh = ss->shots[br.k0 + j];
         int nwin = 50;   // rtm_model.cu:70, :464-465
         while (2 * nwin >= sh.nxi) nwin -= 3;
-        fill_finalize_shot(fin.data() + j * finalize_shot_size(), ss->slots[j].g1, ss->slots[j].illum, sh.g.nx1,
-                           sh.nxi, nwin, sh.pitch, s.npml);
+        fill_finalize_shot(fin.data() + j * finalize_shot_size(), ss->slots[j].g1, ss->slots[j].illum,
+                           o.extra_images ? ss->slots[j].gx : nullptr, sh.g.nx1, sh.nxi, nwin, sh.pitch, s.npml);
     }
     CK(cudaMemcpyAsync(ss->d_fin, fin.data(), fin.size(), cudaMemcpyHostToDevice, st));
     launch_finalize(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->img1, ss->img2s, ss->img2m, ss->illum, st);
     ss->launches++;
+    if (o.extra_images) {
+        launch_finalize_extra(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->ximg, st);
+        ss->launches++;
+    }
     CK(cudaGetLastError());
     return RTM_OK;
 }
@@ -915,6 +970,21 @@ int rtm_session_get_images_f64(rtm_session *ss, double *image1, double *image2s,
     return RTM_OK;
 }
 
+int rtm_session_get_images_extra(rtm_session *ss, float *image3s, float *image4s, float *image5s, float *image3m,
+                                 float *image4m, float *image5m, float *imagetrue)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    if (!ss->o.extra_images) return fail(RTM_ERR_ARG, "the session was opened without extra_images");
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    float *out[7] = {image3s, image4s, image5s, image3m, image4m, image5m, imagetrue};
+    for (int k = 0; k < 7; k++) {
+        int rc = copy_image(ss, ss->ximg[k], out[k]);
+        if (rc) return rc;
+    }
+    return RTM_OK;
+}
+
 int rtm_session_reset_images(rtm_session *ss)
 {
     if (!ss) return fail(RTM_ERR_ARG, "null session");
@@ -923,6 +993,8 @@ int rtm_session_reset_images(rtm_session *ss)
     CK(cudaMemsetAsync(ss->img2s, 0, isz, ss->stream));
     CK(cudaMemsetAsync(ss->img2m, 0, isz, ss->stream));
     CK(cudaMemsetAsync(ss->illum, 0, isz, ss->stream));
+    if (ss->o.extra_images)
+        for (void *im : ss->ximg) CK(cudaMemsetAsync(im, 0, isz, ss->stream));
     CK(cudaStreamSynchronize(ss->stream));
     return RTM_OK;
 }

@@ -7,6 +7,7 @@
 #include "rtm_types.h"
 
 #define R RTM_RADIUS
+#define RTM_PI 3.1415926535897932   // the reference's pi (common.h:11)
 
 namespace {
 
@@ -242,13 +243,24 @@ __global__ void k_gather_pack(const float *g, void *out, float *scale, int nt, i
 // order.  Images are fp32 (reference) or fp64.
 struct FinalizeShot {
     const void *g1, *illum;   // [Z][pitch]: interior cell (iz, lx) at (iz+npml)*pitch + lx+npml
+    const void *gx[4];        // the other imaging conditions' g2, g3, g3t, g4 (null when off)
     int nx1, nxi, nwin, pitch, npml;
 };
+
+// Taper weight of interior column lx (cuda_taper_calculate, kernel.cu:1591-1604).
+__device__ __forceinline__ float taper_at(int lx, int nwin, int nxl)
+{
+    const float alpha = 0.06f;
+    float tp = 1.0f;
+    if (lx < nwin) tp = expf(-alpha * alpha * (nwin - lx) * (nwin - lx));
+    if (lx >= nxl - nwin && lx < nxl) tp = expf(-alpha * alpha * (lx - nxl + nwin + 1) * (lx - nxl + nwin + 1));
+    if (lx >= nwin && lx < nxl - nwin) tp = 1.0f;
+    return tp;
+}
 
 __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, int fp64, void *image1,
                            void *image2s, void *image2m, void *illum_total)
 {
-    const float alpha = 0.06f;
     const long n = (long)nx * nz;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const int iz = (int)(i / nx), ix = (int)(i - (long)iz * nx);
@@ -256,11 +268,7 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
             const FinalizeShot f = fs[s];
             const int lx = ix - f.nx1;
             if (lx < 0 || lx >= f.nxi) continue;
-            const int nwin = f.nwin, nxl = f.nxi;
-            float tp = 1.0f;
-            if (lx < nwin) tp = expf(-alpha * alpha * (nwin - lx) * (nwin - lx));
-            if (lx >= nxl - nwin && lx < nxl) tp = expf(-alpha * alpha * (lx - nxl + nwin + 1) * (lx - nxl + nwin + 1));
-            if (lx >= nwin && lx < nxl - nwin) tp = 1.0f;
+            const float tp = taper_at(lx, f.nwin, f.nxi);
             const size_t ip = (size_t)(iz + f.npml) * f.pitch + lx + f.npml;
             if (fp64) {
                 double g = ((const double *)f.g1)[ip] * (double)tp;
@@ -282,19 +290,110 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
     }
 }
 
-// Laplacian filter of a stacked image (reference laplacefd1d, image_function.cpp:44-79):
-// integer dx, dz; second differences formed in double; border zeroed.
-__global__ void k_laplace(const float *in, float *out, int nx, int nz, int dx, int dz)
+// The other images of a batch (rtm_model.cu:466-487): taper g2, g3, g4 and g3t like g1, then
+// image3s/4s/5s += g2/g3/g4 / (illum + 1e-6) with the shot's tapered illumination (the
+// division in double, as cuda_applyics promotes it), image3m/4m/5m += g2/g3/g4, imagetrue +=
+// g3t.  img = {image3s, image4s, image5s, image3m, image4m, image5m, imagetrue}.
+struct ExtraImages {
+    void *img[7];
+};
+template <typename T>
+__global__ void k_finalize_extra(const FinalizeShot *fs, int nshots, int nx, int nz, ExtraImages out)
 {
     const long n = (long)nx * nz;
+    T *im[7];
+    for (int k = 0; k < 7; k++) im[k] = (T *)out.img[k];
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const int iz = (int)(i / nx), ix = (int)(i - (long)iz * nx);
-        if (ix == 0 || iz == 0 || ix == nx - 1 || iz == nz - 1) { out[i] = 0.0f; continue; }
-        const float *r = &in[i];
-        float t1 = (r[1] + r[-1] - 2.0 * r[0]) / (dx * dx);
-        float t2 = (r[nx] + r[-nx] - 2.0 * r[0]) / (dz * dz);
-        out[i] = t1 + t2;
+        for (int s = 0; s < nshots; s++) {
+            const FinalizeShot f = fs[s];
+            const int lx = ix - f.nx1;
+            if (lx < 0 || lx >= f.nxi) continue;
+            const T tp = (T)taper_at(lx, f.nwin, f.nxi);
+            const size_t ip = (size_t)(iz + f.npml) * f.pitch + lx + f.npml;
+            const T il = ((const T *)f.illum)[ip] * tp;
+            const T g[4] = {((const T *)f.gx[0])[ip] * tp, ((const T *)f.gx[1])[ip] * tp,
+                            ((const T *)f.gx[2])[ip] * tp, ((const T *)f.gx[3])[ip] * tp};
+            const int gi[3] = {0, 1, 3};   // g2 -> image3, g3 -> image4, g4 -> image5
+            for (int k = 0; k < 3; k++) {
+                im[k][i] = (T)(im[k][i] + g[gi[k]] / (il + 1.0e-6));
+                im[3 + k][i] += g[gi[k]];
+            }
+            im[6][i] += g[2];
+        }
     }
+}
+
+// The reference's other imaging conditions for one backward step (kernel.cu:1417-1522;
+// rtm_model.cu:450-455), run after the receiver update on the interior of every shot of a
+// batch, one thread per cell, grid (ceil(nxi/32), ceil(nzi/8), nshots):
+//   g2  += the up-down, down-up, left-right and right-left products of the decomposed
+//          pressures (the reference keeps four arrays and adds them at the end);
+//   g3  += ps p cos(theta), theta from the angle between the source and receiver Poynting
+//          vectors (the reference bins it by whole degrees in 61 arrays and adds the bins at
+//          the end; only the sum is used);
+//   g3t += ps p 16 pi v / sin(theta);
+//   g4  += -(ps - ps_pre)(p - p_pre)/(dt^2 v^2) + grad ps . grad p (centred differences).
+// PAR = 1 reads vx as the reference does, at the pressure cell's flat index z*X + x on its
+// (X-1)-wide vx arrays, and takes the receiver vz in the source Poynting term; PAR = 0 reads
+// vx and vz at the cell itself.  Operand types follow the reference's expressions (float
+// values, double literals).  Each cell's pressures then become the "before" values of the
+// next (earlier) step.
+template <int PAR, typename ACC>
+__global__ void k_image_extra(const ShotDev *shots, float dx, float dz, float dt)
+{
+    const ShotDev &S = shots[blockIdx.z];
+    const int ix = blockIdx.x * 32 + threadIdx.x, iz = blockIdx.y * 8 + threadIdx.y;
+    if (ix >= S.nxi || iz >= S.nzi) return;
+    const int X = S.X, pitch = S.pitch, npml = S.npml;
+    const int z = iz + npml, x = ix + npml;
+    const size_t id = (size_t)z * pitch + x;
+    size_t ivx = id;
+    if (PAR) {
+        const long f = (long)z * X + x;
+        ivx = (size_t)(f / (X - 1)) * pitch + (size_t)(f % (X - 1));
+    }
+    const float ps = S.a.p[id], p = S.b.p[id];
+    const float vxs = S.a.vx[ivx], vx = S.b.vx[ivx], vzs = S.a.vz[id], vz = S.b.vz[id];
+    const float v2 = S.vp2_b[id];
+    ACC *g2 = (ACC *)S.gx[0], *g3 = (ACC *)S.gx[1], *g3t = (ACC *)S.gx[2], *g4 = (ACC *)S.gx[3];
+    // decomposition (kernel.cu:1417-1451)
+    {
+        const float vectxs = -ps * vxs, vectzs = -ps * vzs, vectxr = -p * vx, vectzr = -p * vz;
+        const float psu = vectzs < 0 ? ps : 0.0f, psd = vectzs > 0 ? ps : 0.0f;
+        const float psl = vectxs < 0 ? ps : 0.0f, psr = vectxs > 0 ? ps : 0.0f;
+        const float pu = vectzr < 0 ? p : 0.0f, pd = vectzr > 0 ? p : 0.0f;
+        const float pl = vectxr < 0 ? p : 0.0f, pr = vectxr > 0 ? p : 0.0f;
+        g2[id] += (ACC)(psu * pd + psd * pu + psl * pr + psr * pl);
+    }
+    // Poynting angle (kernel.cu:1452-1485)
+    {
+        const float ksx = ps * vxs, ksz = ps * (PAR ? vz : vzs), krx = p * vx, krz = p * vz;
+        const float q = (ksx * ksx + ksz * ksz) * (krx * krx + krz * krz);
+        const double den = sqrtf(q) > 0 ? (double)sqrtf(q) : 1.0e-6;
+        float wt = (float)((double)(ksx * krx + ksz * krz) / den);
+        if (wt >= -1.0 && wt <= 1.0) {
+            wt = (float)(0.5 * (double)acosf(wt));
+            wt = (float)(RTM_PI / 2.0 - (double)wt);
+            if (wt > 0 && wt <= RTM_PI / 3.0) {
+                const float c = ps * p * cosf(wt);
+                const double t = (double)(ps * p) * 16.0 * RTM_PI * (double)sqrtf(v2) / (double)sinf(wt);
+                g3[id] += (ACC)c;
+                g3t[id] = (ACC)((double)g3t[id] + t);
+            }
+        }
+    }
+    // energy norm (kernel.cu:1486-1522)
+    {
+        const float *ap = S.a.p, *bp = S.b.p;
+        const float psx = (float)(0.5 * (double)(ap[id + 1] - ap[id - 1]) / dx);
+        const float psz = (float)(0.5 * (double)(ap[id + pitch] - ap[id - pitch]) / dz);
+        const float px = (float)(0.5 * (double)(bp[id + 1] - bp[id - 1]) / dx);
+        const float pz = (float)(0.5 * (double)(bp[id + pitch] - bp[id - pitch]) / dz);
+        g4[id] += (ACC)(-(ps - S.ps_pre[id]) * (p - S.p_pre[id]) / (dt * dt * v2) + psx * px + psz * pz);
+    }
+    S.ps_pre[id] = ps;
+    S.p_pre[id] = p;
 }
 
 // =====================================================================================
@@ -361,12 +460,27 @@ void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void 
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_finalize<<<blocks, 256, 0, s>>>((const FinalizeShot *)fs, nshots, nx, nz, fp64, image1, image2s, image2m, illum);
 }
-void launch_laplace(const float *in, float *out, int nx, int nz, int dx, int dz, cudaStream_t s)
+void launch_image_extra(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, int parity, int fp64,
+                        float dx, float dz, float dt, cudaStream_t s)
+{
+    dim3 grid((max_nxi + 31) / 32, (max_nzi + 7) / 8, nshots), block(32, 8);
+    if (parity) {
+        if (fp64) k_image_extra<1, double><<<grid, block, 0, s>>>(shots, dx, dz, dt);
+        else k_image_extra<1, float><<<grid, block, 0, s>>>(shots, dx, dz, dt);
+    } else {
+        if (fp64) k_image_extra<0, double><<<grid, block, 0, s>>>(shots, dx, dz, dt);
+        else k_image_extra<0, float><<<grid, block, 0, s>>>(shots, dx, dz, dt);
+    }
+}
+void launch_finalize_extra(const void *fs, int nshots, int nx, int nz, int fp64, void *const img[7], cudaStream_t s)
 {
     long n = (long)nx * nz;
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_laplace<<<blocks, 256, 0, s>>>(in, out, nx, nz, dx, dz);
+    ExtraImages out;
+    for (int k = 0; k < 7; k++) out.img[k] = img[k];
+    if (fp64) k_finalize_extra<double><<<blocks, 256, 0, s>>>((const FinalizeShot *)fs, nshots, nx, nz, out);
+    else k_finalize_extra<float><<<blocks, 256, 0, s>>>((const FinalizeShot *)fs, nshots, nx, nz, out);
 }
 void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float dt, int gather_prec, cudaStream_t s)
 {
@@ -374,12 +488,13 @@ void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float d
     k_inject<<<grid, 128, 0, s>>>(shots, it, dt, gather_prec);
 }
 size_t finalize_shot_size() { return sizeof(FinalizeShot); }
-void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin, int pitch,
-                        int npml)
+void fill_finalize_shot(void *dst, const void *g1, const void *illum, const void *const *gx, int nx1, int nxi,
+                        int nwin, int pitch, int npml)
 {
     FinalizeShot f;
     f.g1 = g1;
     f.illum = illum;
+    for (int k = 0; k < 4; k++) f.gx[k] = gx ? gx[k] : nullptr;
     f.nx1 = nx1;
     f.nxi = nxi;
     f.nwin = nwin;

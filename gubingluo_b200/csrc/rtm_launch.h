@@ -20,8 +20,10 @@ void launch_strip_pack(const ShotDev *shots, int nshots, int it0, int ring0, int
 void launch_gather_pack(const float *g, void *out, float *scale, int nt, int nrec, int prec, cudaStream_t s);
 void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void *image1, void *image2s, void *image2m,
                      void *illum, cudaStream_t s);
-void launch_laplace(const float *in, float *out, int nx, int nz, int dx, int dz, cudaStream_t s);
 void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float dt, int gather_prec, cudaStream_t s);
 size_t finalize_shot_size();
-void fill_finalize_shot(void *dst, const void *g1, const void *illum, int nx1, int nxi, int nwin, int pitch,
-                        int npml);
+void fill_finalize_shot(void *dst, const void *g1, const void *illum, const void *const *gx, int nx1, int nxi,
+                        int nwin, int pitch, int npml);
+void launch_image_extra(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, int parity, int fp64,
+                        float dx, float dz, float dt, cudaStream_t s);
+void launch_finalize_extra(const void *fs, int nshots, int nx, int nz, int fp64, void *const img[7], cudaStream_t s);

@@ -76,6 +76,13 @@ struct ShotDev {
     float *gather_scale;                // [nt]
     void *g1, *illum;                   // [Z][pitch] float or double accumulators (interior cells used)
     const void *tmaps;                  // RTM_TMAP_COUNT TMA tensor maps (128 B each) of this shot's slot
+    // the other imaging conditions (when enabled): accumulators g2 (decomposition), g3
+    // (Poynting angle), g3t (true amplitude), g4 (energy norm), [Z][pitch] float or double;
+    // the source and receiver pressures before the current backward step; v^2 of the
+    // backward model
+    void *gx[4];
+    float *ps_pre, *p_pre;
+    const float *vp2_b;
 };
 
 // TMA tensor maps of one slot: the staged fields of the two wavefields with the box each

@@ -69,8 +69,14 @@ typedef struct rtm_options {
     int gather_precision;    /* RTM_PREC_*: storage of the receiver gathers */
     int accum_fp64;          /* 1: image/illumination accumulation and division in fp64 */
     int batch;               /* shots per launch; 0 = as many as fit in device memory */
-    int use_graph;           /* capture each pass's time loop in a CUDA graph */
+    int use_graph;           /* reserved, ignored */
     int verbose;             /* print per-batch progress like the reference */
+    int extra_images;        /* the reference's other imaging conditions (kernel.cu:1417-1555):
+                                0 off; 1 wavefield decomposition, Poynting-angle and energy-norm
+                                images with vx and vz read at their own cells; 2 the same with the
+                                reference's indexing (vx at the pressure cell's flat index on its
+                                (X-1)-wide arrays, receiver vz in the source Poynting term), for
+                                parity with its image3/4/5 outputs */
 } rtm_options;
 
 /* Geometry of one shot for the survey's layout (padded coordinates include the PML). */
@@ -93,9 +99,11 @@ typedef struct rtm_stats {
 /* ---- drop-in entry point (same symbol, signature and file side effects as the reference) ----
  * Writes ./seisReal/{ishot}seisreal.su in mode 0, reads it in mode 1, writes
  * the ./output/ temp images after shots with (ishot-1)%50 == 0 and ./output/{idevice}Imagetrue.su,
- * and overwrites the ten image arrays (nx*nz each).  The image3, image4 and image5 arrays and the Poynting image
- * are the reference's extra imaging conditions, outside this library's scope: they are
- * returned as zeros.  Errors are printed and recorded in rtm_last_error(). */
+ * and overwrites the ten image arrays (nx*nz each).  image3*, image4*, image5* and Imagetrue
+ * come from the reference's other imaging conditions (see rtm_options.extra_images): the
+ * environment variable RTM_B200_EXTRA_IMAGES selects 1 (the default: vx and vz read at their
+ * own cells), 2 (the reference's indexing) or 0 (left zero).  Errors are printed and
+ * recorded in rtm_last_error(). */
 void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int medium_flag,
                int flag_layout, int sgyflag, int endianflag, int ismth, int nx, int nz, int nt,
                float dx, float dz, float dt, int npml, float direct, float direct0, float tsnap,
@@ -138,6 +146,13 @@ int rtm_session_get_gather(rtm_session *ss, int k, float *gather);
 int rtm_session_get_images(rtm_session *ss, float *image1, float *image2s, float *image2m,
                            float *illum);
 int rtm_session_get_images_f64(rtm_session *ss, double *image1, double *image2s, double *illum);
+/* With options.extra_images != 0: the other imaging conditions' stacked images (nz*nx each,
+ * any pointer may be NULL), replacing the reference's image3/4/5 and Imagetrue
+ * (rtm_model.cu:466-487): wavefield decomposition (image3s, normalised by each shot's
+ * illumination; image3m), Poynting-angle weighting (image4s, image4m), energy norm (image5s,
+ * image5m) and the Poynting true-amplitude image (imagetrue). */
+int rtm_session_get_images_extra(rtm_session *ss, float *image3s, float *image4s, float *image5s,
+                                 float *image3m, float *image4m, float *image5m, float *imagetrue);
 /* Zero the stacked images. */
 int rtm_session_reset_images(rtm_session *ss);
 /* Number of traces of shot k. */
