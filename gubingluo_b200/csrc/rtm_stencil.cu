@@ -454,11 +454,11 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 // 2: receiver (backward model): overwrite the receiver row with dt*gather[it], then image
 // g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p strips of step it restored,
 // source subtracted).
-// Register budgets (measured): 6 blocks per SM for the reconstruction, 5 for the receiver
-// pass (4 with fp64 accumulators, which would spill at 5); the forward pass is left to the
-// compiler, which was faster than any bound tried.
+// Register budgets (measured): 6 blocks per SM (80 registers, no spills) for the forward
+// pass and the reconstruction, 5 for the receiver pass (4 with fp64 accumulators, which
+// would spill at 5).  A bound of 5 on the forward pass was slower than no bound, 6 faster.
 template <int BZ, int MODE, typename ACC>
-__global__ void __launch_bounds__(BX, MODE == 3 ? 6 : (MODE == 0 ? 0 : (sizeof(ACC) == 8 ? 4 : 5))) k_pres(const StepArgs a, int record)
+__global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6) k_pres(const StepArgs a, int record)
 {
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QN - 1;   // vz rows z0-10 .. z0+BZ+QN-12, columns x0 .. x0+BX-1
