@@ -125,6 +125,16 @@ def lib() -> C.CDLL:
     L.rtm_migrate.argtypes = [S, O, C.POINTER(C.c_int), C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                               C.POINTER(Stats)]
     L.rtm_model.restype = None
+    L.rtm_real.restype = None
+    L.rtm_session_open_geometry.argtypes = [C.POINTER(vp), S, O, C.POINTER(C.c_int), G, C.c_int, vp, vp, vp,
+                                            vp, vp]
+    L.rtm_session_set_gather_raw.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_float, C.c_int]
+    L.rtm_scan_shotgather.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int), vp, C.c_int]
+    L.rtm_real_geometry.argtypes = [S, C.c_int, C.c_int, C.c_int, C.c_float, G, C.POINTER(C.c_int)]
+    L.rtm_read_shot_traces.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_int,
+                                       vp]
+    L.rtm_interp_gather.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                                    C.c_int]
     _lib = L
     return L
 
@@ -217,18 +227,31 @@ def coef_table() -> np.ndarray:
 
 
 class Session:
-    """Device-resident migration of a list of shots (``rtm_session_*``)."""
+    """Device-resident migration of a list of shots (``rtm_session_*``).  ``geometries``
+    (one ``Geometry`` per shot, e.g. from ``real_geometry``) replaces the survey's layout."""
 
     def __init__(self, survey: SurveyConfig, options: RunOptions, shots, vp, rho, vp_mig=None,
-                 rho_mig=None, diffcoef=None):
+                 rho_mig=None, diffcoef=None, geometries=None):
         self.survey, self.options = survey, options
         self.shots = np.ascontiguousarray(shots, dtype=np.int32)
         self._keep = [f32(vp), f32(rho)] + [None if a is None else f32(a) for a in (vp_mig, rho_mig, diffcoef)]
         h = C.c_void_p()
-        _check(lib().rtm_session_open(C.byref(h), C.byref(survey.c()), C.byref(options.c()),
-                                      self.shots.ctypes.data_as(C.POINTER(C.c_int)), len(self.shots),
-                                      *[_ptr(a) for a in self._keep]))
+        ids = self.shots.ctypes.data_as(C.POINTER(C.c_int))
+        if geometries is None:
+            _check(lib().rtm_session_open(C.byref(h), C.byref(survey.c()), C.byref(options.c()), ids,
+                                          len(self.shots), *[_ptr(a) for a in self._keep]))
+        else:
+            if len(geometries) != len(self.shots):
+                raise ValueError("one geometry per shot")
+            self._geoms = (Geometry * len(geometries))(*geometries)
+            _check(lib().rtm_session_open_geometry(C.byref(h), C.byref(survey.c()), C.byref(options.c()), ids,
+                                                   self._geoms, len(self.shots), *[_ptr(a) for a in self._keep]))
         self.h = h
+
+    def set_gather_raw(self, k: int, seisobs, dt0: float, mirror: int = 0):
+        """Recorded traces [nt0][nx0] of shot k, resampled on the device to [nt][nrec_k]."""
+        g = f32(seisobs)
+        _check(lib().rtm_session_set_gather_raw(self.h, k, _ptr(g), g.shape[1], g.shape[0], dt0, mirror))
 
     def nrec(self, k: int) -> int:
         return lib().rtm_session_nrec(self.h, k)
@@ -347,5 +370,66 @@ def migrate(survey: SurveyConfig, options: RunOptions, shots, vp, rho, gathers=N
             out.update(ss.images_extra())
         if survey.mode == 0:
             out["gathers"] = [ss.gather(k) for k in range(len(ss.shots))]
+        out["stats"] = stats
+    return out
+
+
+# ---- real-data path ----
+def scan_shotgather(path: str, sgyflag: int = 0, max_shots: int = 100000):
+    """scanshotgather: (profile [4][nshots] with rows sx, traces, first trace, offset;
+    endianflag)."""
+    prof = np.zeros((4, max_shots), np.int32)
+    endian = C.c_int(0)
+    n = lib().rtm_scan_shotgather(path.encode(), sgyflag, C.byref(endian), _ptr(prof), max_shots)
+    _check(min(n, 0))
+    return np.ascontiguousarray(prof[:, :n]), endian.value
+
+
+def real_geometry(survey: SurveyConfig, sx: int, offset: int, ntrace: int, dx0: float):
+    """Geometry of one recorded shot and the number of data-grid columns (ncols0)."""
+    g = Geometry()
+    nc = C.c_int(0)
+    _check(lib().rtm_real_geometry(C.byref(survey.c()), sx, offset, ntrace, dx0, C.byref(g), C.byref(nc)))
+    return g, nc.value
+
+
+def read_shot_traces(path: str, sgyflag: int, endianflag: int, nt0: int, itrace_all: int, ntrace: int,
+                     ncols: int) -> np.ndarray:
+    out = np.zeros((nt0, ncols), np.float32)
+    _check(lib().rtm_read_shot_traces(path.encode(), sgyflag, endianflag, nt0, itrace_all, ntrace, ncols,
+                                      _ptr(out)))
+    return out
+
+
+def interp_gather(seisobs, nx: int, nt: int, dt: float, dt0: float, mirror: int = 0, device: int = 0):
+    """Interpseis2d on the GPU: [nt0][nx0] -> [nt][nx]."""
+    obs = f32(seisobs)
+    out = np.zeros((nt, nx), np.float32)
+    _check(lib().rtm_interp_gather(_ptr(obs), obs.shape[1], obs.shape[0], _ptr(out), nx, nt, dt, dt0, mirror,
+                                   device))
+    return out
+
+
+def migrate_real(survey: SurveyConfig, options: RunOptions, path: str, profile, shots, vp, rho, nt0: int,
+                 dt0: float, dx0: float, sgyflag: int = 0, endianflag: int = 0, mirror: int = 0):
+    """The real-data driver through a session: recorded shots ``shots`` (1-based numbers into
+    ``profile``) of the file at ``path``, resampled, muted in the migration model and
+    migrated.  ``survey.mode`` must be 1; ``survey.mute`` 2 mutes as the reference does."""
+    prof = np.asarray(profile)
+    geoms, cols = [], []
+    for ishot in shots:
+        sx, ntrace, _, off = (int(prof[r][ishot - 1]) for r in range(4))
+        g, nc = real_geometry(survey, sx, off, ntrace, dx0)
+        geoms.append(g)
+        cols.append(nc)
+    with Session(survey, options, shots, vp, rho, geometries=geoms) as ss:
+        for k, ishot in enumerate(shots):
+            obs = read_shot_traces(path, sgyflag, endianflag, nt0, int(prof[2][ishot - 1]),
+                                   int(prof[1][ishot - 1]), cols[k])
+            ss.set_gather_raw(k, obs, dt0, mirror)
+        stats = ss.run()
+        out = ss.images()
+        if options.extra_images:
+            out.update(ss.images_extra())
         out["stats"] = stats
     return out

@@ -114,6 +114,7 @@ struct rtm_session {
     int launches = 0;
     int last_batch_n = 0;
     std::vector<int> last_batch_shots;
+    rtm::InterpPlan interp;          // real-data path: workspace of the gather interpolation
 };
 
 namespace rtm {
@@ -174,6 +175,23 @@ static int check_survey(const rtm_survey &s)
     if (s.npml < RTM_RADIUS) return fail(RTM_ERR_ARG, "npml must be >= 10 (the stencil radius)");
     if (s.mode != 0 && s.mode != 1) return fail(RTM_ERR_ARG, "mode must be 0 or 1");
     if (s.receiver_depth < 0 || s.receiver_depth >= s.nz) return fail(RTM_ERR_ARG, "receiver_depth out of range");
+    if (s.mute < 0 || s.mute > 2) return fail(RTM_ERR_ARG, "mute must be 0, 1 or 2");
+    return RTM_OK;
+}
+
+// A caller-supplied shot geometry (the real-data path) must describe a window inside the
+// model and nodes inside its padded grid.
+static int check_geometry(const rtm_survey &s, const rtm_geometry &g, int ishot)
+{
+    const std::string who = "shot " + std::to_string(ishot) + ": ";
+    if (g.nx1 < 0 || g.nx2 > s.nx - 1 || g.nx2 - g.nx1 + 1 != g.nxlength || g.nxlength < 2)
+        return fail(RTM_ERR_ARG, who + "window outside the model");
+    if (g.nxpad != g.nxlength + 2 * s.npml || g.nzpad != s.nz + 2 * s.npml)
+        return fail(RTM_ERR_ARG, who + "padded grid does not match the window");
+    if (g.nsx < 0 || g.nsx >= g.nxpad || g.nsz < 0 || g.nsz >= g.nzpad)
+        return fail(RTM_ERR_ARG, who + "source outside its grid");
+    if (g.nrec < 1 || g.rx0 < 0 || g.rx0 + g.nrec > g.nxpad || g.rz < 0 || g.rz >= g.nzpad)
+        return fail(RTM_ERR_ARG, who + "receivers outside the grid");
     return RTM_OK;
 }
 
@@ -242,7 +260,8 @@ static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, i
 }
 
 static int open_session(rtm_session *ss, const float *vp, const float *rho, const float *vp_mig,
-                        const float *rho_mig, const float *diffcoef, const int *shot_ids, int nshots)
+                        const float *rho_mig, const float *diffcoef, const int *shot_ids, int nshots,
+                        const rtm_geometry *geoms = nullptr)
 {
     const rtm_survey &s = ss->s;
     const rtm_options &o = ss->o;
@@ -260,7 +279,12 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     for (int k = 0; k < nshots; k++) {
         ShotState &sh = ss->shots[k];
         sh.ishot = shot_ids[k];
-        rc = shot_geometry(s, sh.ishot, sh.g);
+        if (geoms) {
+            sh.g = geoms[k];
+            rc = check_geometry(s, sh.g, sh.ishot);
+        } else {
+            rc = shot_geometry(s, sh.ishot, sh.g);
+        }
         if (rc) return rc;
         sh.X = sh.g.nxpad;
         sh.Z = sh.g.nzpad;
@@ -359,6 +383,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     // models
     std::map<std::pair<int, int>, std::pair<ModelDev, ModelDev>> mcache;
     std::map<std::pair<int, int>, std::pair<float, std::vector<float>>> vp2cache;
+    std::map<std::pair<int, int>, std::vector<float>> vb2cache;   // mute 2: v^2 of the migration model
     for (auto &w : windows) {
         std::vector<float> vp2, rp;
         const int nx1 = w.first.first, nx2 = w.first.second;
@@ -375,6 +400,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             prep_model(s, vp_mig ? vp_mig : vp, rho_mig ? rho_mig : (vp_mig ? rho : rho), nx1, nx2, true, vb2, rb);
             rc = upload_model(ss, vb2, rb, X, ss->Z, pitch, mb);
             if (rc) return rc;
+            if (s.mute == 2) vb2cache[w.first] = std::move(vb2);
         }
         mcache[w.first] = {mf, mb};
         vp2cache[w.first] = {sqrtf(m), std::move(vp2)};
@@ -385,7 +411,9 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         sh.mf = mcache[key].first;
         sh.mb = mcache[key].second;
         sh.vpmax = vp2cache[key].first;
-        const std::vector<float> &v2 = vp2cache[key].second;
+        // the direct-wave mute reads v^2 of the modelling model (rtm_model.cu mutes before
+        // smoothing) or, with mute 2, of the migration model (rtm_real.cu:397-403 mutes after)
+        const std::vector<float> &v2 = (s.mute == 2 && vb2cache.count(key)) ? vb2cache[key] : vp2cache[key].second;
         PmlOffsets po = pml_offsets(sh.X, sh.Z);
         sh.pml = (float *)ss->arena.take((size_t)po.total * 4);
         sh.src = (float *)ss->arena.take((size_t)sh.sbnx * sh.sbnz * 4);
@@ -815,6 +843,44 @@ int rtm_session_open(rtm_session **out, const rtm_survey *s, const rtm_options *
     return RTM_OK;
 }
 
+int rtm_session_open_geometry(rtm_session **out, const rtm_survey *s, const rtm_options *o, const int *shots,
+                              const rtm_geometry *geoms, int nshots, const float *vp, const float *rho,
+                              const float *vp_mig, const float *rho_mig, const float *diffcoef)
+{
+    clear_error();
+    if (!out || !s || !o || !shots || !geoms || !vp || !rho) return fail(RTM_ERR_ARG, "null argument");
+    *out = nullptr;
+    rtm_session *ss = new rtm_session();
+    ss->s = *s;
+    ss->o = *o;
+    int rc = open_session(ss, vp, rho, vp_mig, rho_mig, diffcoef, shots, nshots, geoms);
+    if (rc) {
+        rtm_session_close(ss);
+        return rc;
+    }
+    *out = ss;
+    return RTM_OK;
+}
+
+int rtm_session_set_gather_raw(rtm_session *ss, int k, const float *seisobs, int nx0, int nt0, float dt0,
+                               int mirror)
+{
+    if (!ss || k < 0 || k >= (int)ss->shots.size() || !seisobs) return fail(RTM_ERR_ARG, "bad gather argument");
+    if (mirror != 0 && mirror != 1) return fail(RTM_ERR_ARG, "mirror must be 0 or 1");
+    if (ss->s.mode != 1) return fail(RTM_ERR_ARG, "recorded gathers need a mode-1 session");
+    ShotState &sh = ss->shots[k];
+    CK(cudaSetDevice(ss->dev));
+    int nl = 0;
+    int rc = interp_gather_device(ss->interp, seisobs, nx0, nt0, sh.gather32, sh.g.nrec, ss->s.nt, ss->s.dt, dt0,
+                                  mirror, ss->stream, &nl);
+    if (rc) return rc;
+    ss->launches += nl;
+    rc = finish_gather(ss, sh);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
 int rtm_session_set_gather(rtm_session *ss, int k, const float *gather)
 {
     if (!ss || k < 0 || k >= (int)ss->shots.size() || !gather) return fail(RTM_ERR_ARG, "bad gather argument");
@@ -1039,6 +1105,7 @@ void rtm_session_close(rtm_session *ss)
             cudaEventDestroy(e.first);
             cudaEventDestroy(e.second);
         }
+    ss->interp.release();
     if (ss->arena.base) cudaFree(ss->arena.base);
     if (ss->stream) cudaStreamDestroy(ss->stream);
     delete ss;

@@ -1,7 +1,8 @@
 // rtm_gpu_main.cpp — drop-in replacement of the reference's rtm_gpu program
 // (gubingluo RTM_GPU_velstr.cpp:37-317): reads ./input/cmd.in and the parameter file it
 // names, reads and regrids the velocity (and density) model, prints the same parameter
-// banner, migrates through rtm_model() and writes ./output/{idevice}*.su.
+// banner, migrates through rtm_model() (modelled data) or rtm_real() (a recorded multi-shot
+// file, dataflag 1) and writes ./output/{idevice}*.su.
 // Run with "--help" for the parameter-file layout (the reference's README promises a
 // selfdoc that its program does not print).
 #include <cstdio>
@@ -23,9 +24,12 @@ static void selfdoc()
         "  2 full array, 3 unilateral right, 4 unilateral left) | mode (0 model the data,\n"
         "  1 data in ./seisReal/) | dataflag | sgyflag | endianflag | rhoflag | vp_file |\n"
         "  [shotgather_file if dataflag] | [rho_file if rhoflag]\n"
+        "dataflag 1 migrates the multi-shot SU/SEG-Y file ./seisReal/<shotgather_file>: its shot\n"
+        "  table is scanned once into ./shotprofileId.dat (reused when present).\n"
         "Writes ./output/{idevice}{Illum,Image1,Image2s,...,Image5m}.su.\n"
         "Environment: RTM_B200_STRIPS / RTM_B200_GATHERS = fp32|fp16|bf16,\n"
-        "  RTM_B200_ACCUM_FP64=1, RTM_B200_BATCH=<shots per launch>, RTM_B200_RECEIVER_DEPTH=<cells>.\n");
+        "  RTM_B200_ACCUM_FP64=1, RTM_B200_BATCH=<shots per launch>, RTM_B200_RECEIVER_DEPTH=<cells>,\n"
+        "  RTM_B200_EXTRA_IMAGES=0|1|2, RTM_B200_FK_MIRROR=0|1.\n");
 }
 
 int main(int argc, char **argv)
@@ -44,10 +48,6 @@ int main(int argc, char **argv)
     if (P.spx0 < 0 || P.spz0 < 0 || P.spx0 + (P.nshot - 1) * P.dspx > (nx0 - 1) * P.dx0 ||
         P.spx0 + (P.nshot - 1) * P.dspx < 0) {
         std::printf("the shot position out of the model !\nplease check the parameter !\n");
-        return 1;
-    }
-    if (P.dataflag) {
-        std::printf("real SEG-Y data (dataflag=1) is not supported by this build\n");
         return 1;
     }
     std::vector<float> vp0((size_t)nx0 * nz0);
@@ -112,11 +112,54 @@ int main(int argc, char **argv)
     std::vector<float> wavelet(nt, 0.0f);
     const size_t n = (size_t)nx * nz;
     std::vector<std::vector<float>> img(10, std::vector<float>(n, 0.0f));
-    rtm_model(P.idevice, P.nshot, P.startshot, P.dshot, P.mode, P.medium_flag, P.flag_layout, P.sgyflag,
-              P.endianflag, P.ismth, nx, nz, nt, dx, dz, dt, P.npml, P.direct, P.direct0, P.tsnap, P.fdom, P.spx0,
-              P.spz0, P.dspx, P.offset, P.offsetmax, P.amp, P.alp, vp.data(), rho.data(), coef, wavelet.data(),
-              img[0].data(), img[1].data(), img[2].data(), img[3].data(), img[4].data(), img[5].data(),
-              img[6].data(), img[7].data(), img[8].data(), img[9].data());
+    if (!P.dataflag) {
+        rtm_model(P.idevice, P.nshot, P.startshot, P.dshot, P.mode, P.medium_flag, P.flag_layout, P.sgyflag,
+                  P.endianflag, P.ismth, nx, nz, nt, dx, dz, dt, P.npml, P.direct, P.direct0, P.tsnap, P.fdom,
+                  P.spx0, P.spz0, P.dspx, P.offset, P.offsetmax, P.amp, P.alp, vp.data(), rho.data(), coef,
+                  wavelet.data(), img[0].data(), img[1].data(), img[2].data(), img[3].data(), img[4].data(),
+                  img[5].data(), img[6].data(), img[7].data(), img[8].data(), img[9].data());
+    } else {
+        // :226-252: the shot table of the recorded file, cached in ./shotprofileId.dat (one
+        // "sx ntrace first-trace offset" line per shot); a fresh scan also sets the byte order
+        if (P.nshotall < 1) {
+            std::printf("nshotall must be >= 1 for real data\n");
+            return 1;
+        }
+        std::vector<int> prof((size_t)4 * P.nshotall, 0);
+        int *rows[4] = {&prof[0], &prof[P.nshotall], &prof[2 * (size_t)P.nshotall], &prof[3 * (size_t)P.nshotall]};
+        FILE *cache = std::fopen("shotprofileId.dat", "r");
+        if (!cache) {
+            std::snprintf(path, sizeof(path), "./seisReal/%s", P.shotgather_file);
+            int found = rtm_scan_shotgather(path, P.sgyflag, &P.endianflag, prof.data(), P.nshotall);
+            if (found < 0) {
+                std::printf("rtm_gpu: %s\n", rtm_last_error());
+                return 1;
+            }
+            std::printf("nt %d\n", P.nt0);
+            std::printf("shots found: %d\n", found);
+            cache = std::fopen("shotprofileId.dat", "w");
+            if (cache) {
+                for (int i = 0; i < P.nshotall; i++)
+                    std::fprintf(cache, "%d %d %d %d\n", rows[0][i], rows[1][i], rows[2][i], rows[3][i]);
+                std::fclose(cache);
+            }
+        } else {
+            for (int i = 0; i < P.nshotall; i++)
+                if (std::fscanf(cache, "%d %d %d %d", &rows[0][i], &rows[1][i], &rows[2][i], &rows[3][i]) != 4) {
+                    std::printf("shotprofileId.dat holds fewer than %d shots\n", P.nshotall);
+                    std::fclose(cache);
+                    return 1;
+                }
+            std::fclose(cache);
+        }
+        char fname[256];
+        std::snprintf(fname, sizeof(fname), "%s", P.shotgather_file);
+        rtm_real(P.idevice, P.nshot, P.startshot, P.dshot, P.medium_flag, P.flag_layout, P.sgyflag, P.endianflag,
+                 P.ismth, nx, nz, nt, dx, dz, dt, nx0, nz0, P.nt0, P.dx0, P.dz0, P.dt0, P.npml, lx, lz, P.tsnap,
+                 P.fdom, P.spz0, P.amp, P.alp, P.direct, P.direct0, vp.data(), rho.data(), coef, wavelet.data(),
+                 fname, rows, img[0].data(), img[1].data(), img[2].data(), img[3].data(), img[4].data(),
+                 img[5].data(), img[6].data(), img[7].data(), img[8].data(), img[9].data());
+    }
     if (rtm_last_error()[0]) {
         std::printf("rtm_gpu: %s\n", rtm_last_error());
         return 1;

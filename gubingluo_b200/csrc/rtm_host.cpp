@@ -505,6 +505,186 @@ int read_gather_su(const char *path, int sgyflag, float *gather, int *nt_out, in
 
 // Parameter file (RTM_GPU_velstr.cpp:60-120): ./input/cmd.in names the parameter file on
 // its second line; the parameter file alternates one comment line and one value line.
+// ---- real-data path: multi-shot SU / SEG-Y files ----------------------------------------
+// scanshotgather (RTM_GPU_velstr.cpp:363-454).  Byte order from the first trace header: read
+// as little-endian, swapped when its ns or dt is <= 0 (and refused when neither order gives
+// positive values).  Every trace is assumed to hold the first header's ns samples.  One pass
+// over the headers; a shot starts wherever sx changes.  profile is [4][max_shots]: rows sx,
+// trace count, number of the shot's first trace in the file (from 1), offset of that trace.
+// The scan stops at the first incomplete trace or at a header with ns or dt <= 0.  Two
+// outcomes of the reference are not kept: for a byte-swapped file its end-of-file read swaps
+// the last header's keys back, which opens a trailing shot of zero traces (written one entry
+// past the shots, beyond a table sized to the shot count); and its trace count includes the
+// trace whose header ended the scan.
+int scan_shotgather(const char *path, int sgyflag, int *endianflag, int *profile, int max_shots, int *nshots)
+{
+    if (!path || !profile || max_shots < 1) return fail(RTM_ERR_ARG, "scan_shotgather: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(RTM_ERR_IO, std::string("cannot open shot gather file ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const long long size = std::ftell(f);
+    const long long start = sgyflag ? 3600 : 0;
+    unsigned char h[240];
+    std::fseek(f, (long)start, SEEK_SET);
+    if (size < start + 240 || std::fread(h, 1, 240, f) != 240) {
+        std::fclose(f);
+        return fail(RTM_ERR_IO, std::string("shot gather file too short: ") + path);
+    }
+    short ns, dt;
+    std::memcpy(&ns, h + 114, 2);
+    std::memcpy(&dt, h + 116, 2);
+    int endian = 0;
+    if (dt <= 0 || ns <= 0) {
+        swap2(&ns);
+        swap2(&dt);
+        if (dt <= 0 || ns <= 0) {
+            std::fclose(f);
+            return fail(RTM_ERR_IO, std::string("no byte order gives positive ns and dt in ") + path);
+        }
+        endian = 1;
+    }
+    auto key4 = [&](int off) {
+        int v;
+        std::memcpy(&v, h + off, 4);
+        if (endian) swap4(&v);
+        return v;
+    };
+    auto key2 = [&](int off) {
+        short v;
+        std::memcpy(&v, h + off, 2);
+        if (endian) swap2(&v);
+        return v;
+    };
+    const long long tb = 240 + (long long)ns * 4;
+    int n = 0;
+    for (long long k = 0; start + (k + 1) * tb <= size; k++) {
+        std::fseek(f, (long)(start + k * tb), SEEK_SET);
+        if (std::fread(h, 1, 240, f) != 240) break;
+        if (key2(114) <= 0 || key2(116) <= 0) break;
+        const int sx = key4(72);
+        if (n == 0 || profile[n - 1] != sx) {
+            if (n == max_shots) {
+                std::fclose(f);
+                return fail(RTM_ERR_ARG, std::string("more than ") + std::to_string(max_shots) + " shots in " + path);
+            }
+            profile[n] = sx;
+            profile[max_shots + n] = 0;
+            profile[2 * max_shots + n] = (int)(k + 1);
+            profile[3 * max_shots + n] = key4(36);
+            n++;
+        }
+        profile[max_shots + n - 1]++;
+    }
+    std::fclose(f);
+    if (endianflag) *endianflag = endian;
+    if (nshots) *nshots = n;
+    return RTM_OK;
+}
+
+// Shot window and source/receiver nodes of one recorded shot (rtm_real.cu:134-157): the
+// receivers lie to the right of the source from `offset` on, every dx0 (the data spacing),
+// so the spread ends at offsetmax = offset + (ntrace-1)*dx0; the window spans source to last
+// receiver on the model grid (dx).  ncols0 = the spread's width on the data grid, the number
+// of columns the recorded traces are read into before interpolation.  Refused where the
+// reference reads outside the model: a window starting left of x = 0 or ending beyond nx-1.
+int real_geometry(const rtm_survey &s, int sx, int offset, int ntrace, float dx0, rtm_geometry &g, int *ncols0)
+{
+    std::memset(&g, 0, sizeof(g));
+    if (ntrace < 1 || !(dx0 > 0.0f)) return fail(RTM_ERR_ARG, "real_geometry: ntrace and dx0 must be positive");
+    const float dx = s.dx, dz = s.dz;
+    const float offsetmax = (float)(offset + (ntrace - 1) * dx0);
+    const float off = (float)offset;
+    float spx = (float)sx;
+    float spz = s.spz0;
+    const int noffset0 = (int)(off / dx0);
+    const int nx10 = (int)(spx / dx0);
+    const int nx20 = (int)((spx + offsetmax) / dx0);
+    g.noffset = (int)(off / dx);
+    g.nx1 = (int)(spx / dx);
+    g.nx2 = (int)((spx + offsetmax) / dx);
+    g.nxlength = g.nx2 - g.nx1 + 1;
+    if (sx < 0 || g.nx1 < 0 || g.nx2 > s.nx - 1)
+        return fail(RTM_ERR_ARG, "shot at sx = " + std::to_string(sx) + " spreads beyond the model (columns " +
+                                     std::to_string(g.nx1) + ".." + std::to_string(g.nx2) + " of " +
+                                     std::to_string(s.nx) + ")");
+    spx = spx - g.nx1 * dx;
+    spx = spx + s.npml * dx;
+    spz = spz + s.npml * dz;
+    g.nxpad = g.nxlength + 2 * s.npml;
+    g.nzpad = s.nz + 2 * s.npml;
+    g.nsx = (int)(spx / dx);
+    g.nsz = (int)(spz / dz);
+    g.rz = s.npml + s.receiver_depth;
+    g.rx0 = s.npml + g.noffset;
+    g.nrec = g.nxlength - g.noffset;
+    g.iTraceAll = 1;
+    g.iTrace = 1;
+    g.Offset = offset;
+    g.sx = sx;
+    g.gx = sx + offset;
+    g.Nt = (unsigned short)s.nt;
+    g.Dt = (unsigned short)(s.dt * 1000000);
+    g.Dx = dx;
+    g.Ntrace = g.nrec;
+    const int nc0 = nx20 - nx10 + 1 - noffset0;
+    if (ncols0) *ncols0 = nc0;
+    if (g.nxlength < 2 || g.nrec < 1 || nc0 < 1)
+        return fail(RTM_ERR_ARG, "shot at sx = " + std::to_string(sx) + " has no receivers on the grid");
+    if (g.nsx < 0 || g.nsx >= g.nxpad || g.nsz < 0 || g.nsz >= g.nzpad)
+        return fail(RTM_ERR_ARG, "shot at sx = " + std::to_string(sx) + ": source outside its grid");
+    if (g.rz >= g.nzpad - s.npml) return fail(RTM_ERR_ARG, "receiver depth below the model");
+    return RTM_OK;
+}
+
+// The trace-reading loop of rtm_real.cu:379-394: ntrace traces from trace number itrace_all
+// on (240-byte header skipped, nt0 floats, byte-swapped when endianflag) into column ix of
+// seisobs [nt0][ncols].  Columns from ntrace on are zero (the reference leaves them
+// unwritten); traces beyond ncols are not stored (the reference writes past its array).
+// Refused: a file too short for the traces, or a first header whose ns is not nt0.
+int read_shot_traces(const char *path, int sgyflag, int endianflag, int nt0, long long itrace_all, int ntrace,
+                     int ncols, float *seisobs)
+{
+    if (!path || !seisobs || nt0 < 1 || ncols < 1 || ntrace < 1 || itrace_all < 1)
+        return fail(RTM_ERR_ARG, "read_shot_traces: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(RTM_ERR_IO, std::string("cannot open shot gather file ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const long long size = std::ftell(f);
+    const long long tb = 240 + (long long)nt0 * 4;
+    const long long first = (itrace_all - 1) * tb + 3600LL * (sgyflag ? 1 : 0);
+    if (first + ntrace * tb > size) {
+        std::fclose(f);
+        return fail(RTM_ERR_IO, std::string("shot gather file ends before trace ") +
+                                    std::to_string(itrace_all + ntrace - 1) + ": " + path);
+    }
+    std::memset(seisobs, 0, sizeof(float) * (size_t)nt0 * ncols);
+    std::vector<float> tr(nt0);
+    unsigned char h[240];
+    int rc = RTM_OK;
+    for (int ix = 0; ix < ntrace && ix < ncols && !rc; ix++) {
+        std::fseek(f, (long)(first + ix * tb), SEEK_SET);
+        if (std::fread(h, 1, 240, f) != 240 || std::fread(tr.data(), sizeof(float), nt0, f) != (size_t)nt0) {
+            rc = fail(RTM_ERR_IO, std::string("cannot read trace of ") + path);
+            break;
+        }
+        if (ix == 0) {
+            short ns;
+            std::memcpy(&ns, h + 114, 2);
+            if (endianflag) swap2(&ns);
+            if (ns != nt0)
+                rc = fail(RTM_ERR_IO, "trace " + std::to_string(itrace_all) + " of " + path + " holds " +
+                                          std::to_string(ns) + " samples, not nt0 = " + std::to_string(nt0));
+        }
+        for (int it = 0; it < nt0; it++) {
+            float v = tr[it];
+            if (endianflag) swap4(&v);
+            seisobs[(size_t)it * ncols + ix] = v;
+        }
+    }
+    std::fclose(f);
+    return rc;
+}
+
 int read_params(const char *input_dir, rtm_params &p)
 {
     std::memset(&p, 0, sizeof(p));

@@ -4,6 +4,9 @@
 
 #include "rtm_b200.h"
 
+struct CUstream_st;
+typedef CUstream_st *cudaStream_t_fwd;   // cudaStream_t without the runtime header
+
 namespace rtm {
 
 int fail(int code, const std::string &msg);
@@ -28,5 +31,36 @@ int write_gather_su(const char *path, const float *gather, const rtm_geometry &g
                     int endianflag);
 int read_gather_su(const char *path, int sgyflag, float *gather, int *nt, int *ntr, rtm_geometry *keys);
 int read_params(const char *input_dir, rtm_params &p);
+
+// ---- real-data path --------------------------------------------------------------------
+int scan_shotgather(const char *path, int sgyflag, int *endianflag, int *profile, int max_shots, int *nshots);
+int real_geometry(const rtm_survey &s, int sx, int offset, int ntrace, float dx0, rtm_geometry &g, int *ncols0);
+int read_shot_traces(const char *path, int sgyflag, int endianflag, int nt0, long long itrace_all, int ntrace,
+                     int ncols, float *seisobs);
+
+// Shape of one gather interpolation [nt0][nx0] -> [nt][nx] (reference Interpseis2d).
+struct InterpShape {
+    int nx0, nt0, nx, nt;
+    int fk, sinc;          // x by F-K (nx > nx0), t by sinc (nt > nt0)
+    int lx, Nx, Nt, nf;    // F-K: fold, padded sizes, positive frequencies
+};
+int interp_shape(int nx0, int nt0, int nx, int nt, InterpShape &sh);
+
+// Device workspace and cuFFT plans of one shape; kept by the caller and reused while the
+// shape repeats (shots of a survey usually share it).
+struct InterpPlan {
+    InterpShape shape{};
+    void *work = nullptr;                 // one allocation holding everything below
+    float *d_in = nullptr, *d_tmp = nullptr;
+    void *K = nullptr, *S = nullptr, *Z = nullptr, *G1 = nullptr, *G = nullptr;   // double2 arrays
+    unsigned *zmax = nullptr;
+    int p_k = 0, p_s = 0, p_x = 0, p_t = 0;   // cufftHandle values, valid when `plans`
+    bool plans = false;
+    void release();
+};
+// Uploads host_in [nt0][nx0] and writes the interpolated gather to d_out [nt][nx] on stream
+// st; mirror 0 = the reference's negative-frequency indexing, 1 = the Hermitian partner.
+int interp_gather_device(InterpPlan &p, const float *host_in, int nx0, int nt0, float *d_out, int nx, int nt,
+                         float dt, float dt0, int mirror, cudaStream_t_fwd st, int *launches);
 
 }  // namespace rtm

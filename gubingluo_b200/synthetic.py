@@ -137,3 +137,41 @@ def config(n: int, nshots: int | None = None, nt: int | None = None):
     s.dt = float(np.float32(s.dt))
     meta = dict(config=n, smooth_m=smooth_m)
     return s, shots, v, vm, rho, meta
+
+
+def write_shot_file(path: str, shots, nt0: int, dt0: float, dx0: float, sgyflag: int = 0,
+                    big_endian: bool = False, first_trace: int = 1) -> None:
+    """Writes a multi-shot SU (sgyflag 0) or SEG-Y (sgyflag 1: a zeroed 3600-byte volume
+    header first) file of the layout the real-data driver reads (rtm_real.cu:379-394,
+    sgyhead.h:92-103): per trace a 240-byte header, then nt0 IEEE floats.  Header keys
+    written (byte offset): tracl 0, tracf 12, offset 36, sx 72, gx 80 (int32), ns 114, dt 116
+    (int16, microseconds), d2 188 (float), ntr 208 (int32); the rest zero.  ``shots`` is a list
+    of (sx, offset, gather[nt0][ntrace]) with receivers offset, offset+dx0, ... to the right
+    of the source, as that driver assumes."""
+    e = ">" if big_endian else "<"
+    hdr = np.dtype([("tracl", e + "i4"), ("p0", "V8"), ("tracf", e + "i4"), ("p1", "V20"), ("offset", e + "i4"),
+                    ("p2", "V32"), ("sx", e + "i4"), ("p3", "V4"), ("gx", e + "i4"), ("p4", "V30"),
+                    ("ns", e + "i2"), ("dt", e + "i2"), ("p5", "V70"), ("d2", e + "f4"), ("p6", "V16"),
+                    ("ntr", e + "i4"), ("p7", "V28")])
+    assert hdr.itemsize == 240
+    with open(path, "wb") as f:
+        if sgyflag:
+            f.write(bytes(3600))
+        itr = first_trace
+        for sx, offset, g in shots:
+            g = np.asarray(g, np.float32)
+            assert g.shape[0] == nt0
+            for ix in range(g.shape[1]):
+                h = np.zeros(1, hdr)
+                h["tracl"] = itr
+                h["tracf"] = ix + 1
+                h["offset"] = int(offset + ix * dx0)
+                h["sx"] = int(sx)
+                h["gx"] = int(sx + offset + ix * dx0)
+                h["ns"] = nt0
+                h["dt"] = int(round(dt0 * 1e6))
+                h["d2"] = dx0
+                h["ntr"] = g.shape[1]
+                f.write(h.tobytes())
+                f.write(np.ascontiguousarray(g[:, ix]).astype(e + "f4").tobytes())
+                itr += 1

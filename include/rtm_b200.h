@@ -59,7 +59,9 @@ typedef struct rtm_survey {
     int ismth;               /* >0: smooth v^2 and rho by a Gaussian of half-width ismth after the
                                 source pass, as the reference does (rtm_model.cu:402-408) */
     float direct, direct0;   /* direct-wave mute: nw = direct/(fdom*dt), tlength = direct0/dt */
-    int mute;                /* apply the direct-wave mute (the reference always does) */
+    int mute;                /* direct-wave mute: 0 none, 1 with the modelling model's velocities
+                                (rtm_model.cu mutes before smoothing), 2 with the migration
+                                model's (rtm_real.cu:397-403 mutes after smoothing) */
     int receiver_depth;      /* receiver row below z = 0 in cells (reference: 0) */
 } rtm_survey;
 
@@ -112,6 +114,29 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
                float *image1, float *image2s, float *image3s, float *image4s, float *image5s,
                float *image2m, float *image3m, float *image4m, float *image5m, float *illum);
 
+/* Drop-in for the reference's real-data driver (definition rtm_real.cu:17-22; the caller's
+ * prototype RTM_GPU_velstr.cpp:30-35 declares `int nw, int tlength` where the definition has
+ * `float direct, float direct0`: this symbol takes the definition's list).  For shots
+ * startshot, startshot+dshot, ... <= nshot: geometry from shotprofileId[0..3][ishot-1] (sx,
+ * trace count, first trace, offset; rtm_scan_shotgather), traces read from
+ * ./seisReal/<filename_shotgather> (nt0 samples at dt0, receivers every dx0), resampled to
+ * dx and dt (F-K in x, windowed sinc in t: rtm_interp_gather), muted in the migration model
+ * and migrated on the device in batches.  vp0/rho0: the nz*nx model on the dx grid.  nx0,
+ * nz0, dz0, lx, lz, tsnap, flag_layout and wavelet are accepted and not used, as in the
+ * reference.  Writes the ./output/ temp images after shots with (ishot-1)%50 == 0 and
+ * ./output/{idevice}Imagetrue.su, and overwrites the ten image arrays.  Environment: as for
+ * rtm_model, plus RTM_B200_FK_MIRROR = 0 (default: the reference's negative-frequency
+ * indexing in the F-K step) or 1 (the Hermitian partner).  Errors are printed and recorded
+ * in rtm_last_error(). */
+void rtm_real(int idevice, int nshot, int startshot, int dshot, int medium_flag, int flag_layout,
+              int sgyflag, int endianflag, int ismth, int nx, int nz, int nt, float dx, float dz,
+              float dt, int nx0, int nz0, int nt0, float dx0, float dz0, float dt0, int npml, int lx,
+              int lz, float tsnap, float fdom, float spz0, float amp, float alp, float direct,
+              float direct0, float *vp0, float *rho0, float *diffcoef, float *wavelet,
+              char filename_shotgather[40], int **shotprofileId, float *image1, float *image2s,
+              float *image3s, float *image4s, float *image5s, float *image2m, float *image3m,
+              float *image4m, float *image5m, float *illum);
+
 /* Last error message of this thread ("" when none). */
 const char *rtm_last_error(void);
 
@@ -127,8 +152,20 @@ typedef struct rtm_session rtm_session;
 int rtm_session_open(rtm_session **out, const rtm_survey *s, const rtm_options *o, const int *shots,
                      int nshots, const float *vp, const float *rho, const float *vp_mig,
                      const float *rho_mig, const float *diffcoef);
+/* As rtm_session_open, with every shot's geometry given (geoms[k] for shot shots[k], e.g. from
+ * rtm_real_geometry) instead of computed from the survey's layout; layout, spx0, dspx, offset
+ * and offsetmax of the survey are then unused. */
+int rtm_session_open_geometry(rtm_session **out, const rtm_survey *s, const rtm_options *o,
+                              const int *shots, const rtm_geometry *geoms, int nshots,
+                              const float *vp, const float *rho, const float *vp_mig,
+                              const float *rho_mig, const float *diffcoef);
 /* Mode 1: upload shot k's gather gathers[k] ([nt][nrec_k]), mute and pack it on the device. */
 int rtm_session_set_gather(rtm_session *ss, int k, const float *gather);
+/* Mode 1, recorded data: upload shot k's traces seisobs [nt0][nx0] (dt0, data spacing),
+ * resample them on the device to [nt][nrec_k] (rtm_interp_gather; mirror as there), then
+ * mute and pack as rtm_session_set_gather does. */
+int rtm_session_set_gather_raw(rtm_session *ss, int k, const float *seisobs, int nx0, int nt0,
+                               float dt0, int mirror);
 /* Migrate every shot of the session; images accumulate on the device.  Inputs must be
  * resident (rtm_session_set_gather for mode 1). */
 int rtm_session_run(rtm_session *ss, rtm_stats *stats);
@@ -205,6 +242,33 @@ void rtm_laplace_image(float *image, int nx, int nz, int dx, int dz);
  * Returns RTM_OK or an RTM_ERR_* code (message in rtm_last_error()). */
 int rtm_laplace_image_noalloc(float *image, int nx, int nz, int dx, int dz);
 void rtm_scale_image(const float *illum, float *image, int n);
+
+/* ---- real-data path ---- */
+/* scanshotgather (RTM_GPU_velstr.cpp:363-454) on a multi-shot SU (sgyflag 0) or SEG-Y (1)
+ * file: byte order from the first header's ns/dt (*endianflag 1 = big-endian), then one row
+ * per shot, a shot starting wherever sx changes: profile is [4][max_shots] with rows sx,
+ * trace count, first trace number (from 1) and offset of the first trace (the rows of the
+ * reference's shotprofileId).  Returns the number of shots (>= 0) or an RTM_ERR_* code. */
+int rtm_scan_shotgather(const char *path, int sgyflag, int *endianflag, int *profile, int max_shots);
+/* Geometry of one recorded shot (rtm_real.cu:134-157): receivers from `offset` to the right
+ * of the source every dx0.  *ncols0 = traces on the data grid (the width nx0 that
+ * rtm_interp_gather and rtm_session_set_gather_raw take).  Uses nx, nz, dx, dz, npml, spz0,
+ * nt, dt and receiver_depth of s. */
+int rtm_real_geometry(const rtm_survey *s, int sx, int offset, int ntrace, float dx0,
+                      rtm_geometry *g, int *ncols0);
+/* ntrace traces of nt0 samples from trace number itrace_all on (rtm_real.cu:379-394) into
+ * seisobs [nt0][ncols]; columns from ntrace on are zero. */
+int rtm_read_shot_traces(const char *path, int sgyflag, int endianflag, int nt0,
+                         long long itrace_all, int ntrace, int ncols, float *seisobs);
+/* Interpseis2d (Interp_function.cpp:245-264) on the GPU: seisobs [nt0][nx0] -> seiscal
+ * [nt][nx].  nx > nx0: F-K interpolation by lx = (nx-1)/(nx0-1) (nx <= lx*nx0 required);
+ * nt > nt0: 21-tap Kaiser-windowed sinc; neither: the first nt samples of the first nx
+ * traces.  mirror 0 builds the negative frequencies of the F-K step with the reference's
+ * indexing (one row off the Hermitian partner; for odd nt0 the first such row reads as zero
+ * where the reference reads past its array), 1 from the Hermitian partner.  Host buffers;
+ * synchronous on device `device`. */
+int rtm_interp_gather(const float *seisobs, int nx0, int nt0, float *seiscal, int nx, int nt,
+                      float dt, float dt0, int mirror, int device);
 
 /* ---- files ---- */
 typedef struct rtm_params {

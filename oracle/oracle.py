@@ -80,6 +80,9 @@ def lib():
         L.orc_pml_profiles.argtypes = [_vp] * 4 + [C.c_float] * 3 + [C.c_int] * 3
         L.orc_norder.argtypes = [_vp] * 3 + [C.c_int] * 2
         L.orc_source.argtypes = [_vp] + [C.c_int] * 4 + [C.c_float] * 4
+        L.orc_interp_gather.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        C.c_int]
+        L.orc_fk_interp.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_mute.argtypes = [_vp, _vp] + [C.c_int] * 9 + [C.c_float] * 3
         L.orc_taper.argtypes = [_vp, C.c_int, C.c_int, C.c_float]
         L.orc_taper_nwin.argtypes = [C.c_int]
@@ -202,6 +205,57 @@ def shot(shot: OrcShot, vp2f, rhof, vp2b=None, rhob=None, mode=1, gather=None, m
     return dict(g1=g1, illum=il, gather=gather, ps=ps, p=pr, g2=ex[0], g3=ex[1], g3t=ex[2], g4=ex[3])
 
 
+def _migrate_shot(s, g, vp, rho, vp_mig, rho_mig, mode, gather, mute, nw, tlength, precision, keep_fields,
+                  extra, images, fields, out_gathers):
+    """One shot of the reference's shot loop for geometry ``g``: model window + padding
+    (+ PML smoothing), migration model (+ smoothing), the shot, then the per-shot stacking
+    into ``images`` (rtm_model.cu:150-488, rtm_real.cu:196-468)."""
+    nx, nz = s["nx"], s["nz"]
+    vp2f = pad_model(vp, g.nx1, g.nx2, s["npml"], True, s.get("medium_flag", 0))
+    rhof = pad_model(rho, g.nx1, g.nx2, s["npml"], False, s.get("medium_flag", 0))
+    if vp_mig is not None or s.get("ismth", 0) > 0:
+        vb = vp_mig if vp_mig is not None else vp
+        rb = rho_mig if rho_mig is not None else rho
+        vp2b = pad_model(vb, g.nx1, g.nx2, s["npml"], True, s.get("medium_flag", 0))
+        rhob = pad_model(rb, g.nx1, g.nx2, s["npml"], False, s.get("medium_flag", 0))
+        if s.get("ismth", 0) > 0:
+            vp2b = velsmooth(vp2b, s["ismth"])
+            rhob = velsmooth(rhob, s["ismth"])
+    else:
+        vp2b, rhob = vp2f, rhof
+    vpmax = float(np.sqrt(np.float32(vp2f.max()), dtype=np.float32))
+    rz = s["npml"] + s.get("receiver_depth", 0)
+    sh = shot_struct(g.nxpad, g.nzpad, s["npml"], s["nt"], s["dx"], s["dz"], s["dt"], g.nsx, g.nsz,
+                     s["amp"], s["alp"], s["fdom"], rz, g.rx0, g.nrec, vpmax)
+    r = shot(sh, vp2f, rhof, vp2b, rhob, mode=mode, gather=gather, mute=mute, nw=nw, tlength=tlength,
+             precision=precision, want_fields=keep_fields, extra=extra)
+    out_gathers.append(r["gather"])
+    if keep_fields:
+        fields.append((r["ps"], r["p"]))
+    fin = lib().orc_finalize_f32 if precision == "f32" else lib().orc_finalize_f64
+    fin(_p(r["g1"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1, _p(images["image1"]), _p(images["image2s"]),
+        _p(images["illum"]))
+    if extra:   # after fin, which tapered r["illum"] in place
+        fx = lib().orc_finalize_extra_f32 if precision == "f32" else lib().orc_finalize_extra_f64
+        fx(_p(r["g2"]), _p(r["g3"]), _p(r["g4"]), _p(r["g3t"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1,
+           *[_p(images[k]) for k in XNAMES])
+
+
+XNAMES = ("image3s", "image4s", "image5s", "image3m", "image4m", "image5m", "imagetrue")
+
+
+def _new_images(nz, nx, precision, extra):
+    acc = np.float32 if precision == "f32" else np.float64
+    names = ("image1", "image2s", "illum") + (XNAMES if extra else ())
+    return {k: np.zeros((nz, nx), acc) for k in names}
+
+
+def _mute_lengths(s):
+    nw = int(np.float32(s["direct"]) / (np.float32(s["fdom"]) * np.float32(s["dt"])))
+    tlength = int(np.float32(s["direct0"]) / np.float32(s["dt"]))
+    return nw, tlength
+
+
 def rtm_model(survey: dict, shots, vp, rho, vp_mig=None, rho_mig=None, gathers=None,
               precision="f32", keep_fields=False, extra=0):
     """Restatement of the reference's rtm_model shot loop for one layout (mode 0 models each
@@ -211,50 +265,107 @@ def rtm_model(survey: dict, shots, vp, rho, vp_mig=None, rho_mig=None, gathers=N
     also image3s, image4s, image5s, image3m, image4m, image5m and imagetrue."""
     s = survey
     nx, nz = s["nx"], s["nz"]
-    acc = np.float32 if precision == "f32" else np.float64
-    image1 = np.zeros((nz, nx), acc)
-    image2s = np.zeros((nz, nx), acc)
-    illum = np.zeros((nz, nx), acc)
-    xnames = ("image3s", "image4s", "image5s", "image3m", "image4m", "image5m", "imagetrue")
-    ximg = {k: np.zeros((nz, nx), acc) for k in xnames} if extra else {}
+    images = _new_images(nz, nx, precision, extra)
     out_gathers, fields = [], []
-    nw = int(np.float32(s["direct"]) / (np.float32(s["fdom"]) * np.float32(s["dt"])))
-    tlength = int(np.float32(s["direct0"]) / np.float32(s["dt"]))
+    nw, tlength = _mute_lengths(s)
     for k, ishot in enumerate(shots):
         g = geometry(s["layout"], ishot, nx, nz, s["nt"], s["dx"], s["dz"], s["dt"], s["npml"],
                      s["spx0"], s["spz0"], s["dspx"], s.get("offset", 0.0), s.get("offsetmax", 0.0))
-        vp2f = pad_model(vp, g.nx1, g.nx2, s["npml"], True, s.get("medium_flag", 0))
-        rhof = pad_model(rho, g.nx1, g.nx2, s["npml"], False, s.get("medium_flag", 0))
-        if vp_mig is not None or s.get("ismth", 0) > 0:
-            vb = vp_mig if vp_mig is not None else vp
-            rb = rho_mig if rho_mig is not None else rho
-            vp2b = pad_model(vb, g.nx1, g.nx2, s["npml"], True, s.get("medium_flag", 0))
-            rhob = pad_model(rb, g.nx1, g.nx2, s["npml"], False, s.get("medium_flag", 0))
-            if s.get("ismth", 0) > 0:
-                vp2b = velsmooth(vp2b, s["ismth"])
-                rhob = velsmooth(rhob, s["ismth"])
-        else:
-            vp2b, rhob = vp2f, rhof
-        vpmax = float(np.sqrt(np.float32(vp2f.max()), dtype=np.float32))
-        rz = s["npml"] + s.get("receiver_depth", 0)
-        sh = shot_struct(g.nxpad, g.nzpad, s["npml"], s["nt"], s["dx"], s["dz"], s["dt"], g.nsx, g.nsz,
-                         s["amp"], s["alp"], s["fdom"], rz, g.rx0, g.nrec, vpmax)
-        r = globals()["shot"](sh, vp2f, rhof, vp2b, rhob, mode=s["mode"],
-                              gather=None if s["mode"] == 0 else gathers[k], mute=s.get("mute", 1),
-                              nw=nw, tlength=tlength, precision=precision, want_fields=keep_fields,
-                              extra=extra)
-        out_gathers.append(r["gather"])
-        if keep_fields:
-            fields.append((r["ps"], r["p"]))
-        fin = lib().orc_finalize_f32 if precision == "f32" else lib().orc_finalize_f64
-        img2m = np.zeros_like(image1)
-        fin(_p(r["g1"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1, _p(image1), _p(image2s), _p(illum))
-        if extra:   # after fin, which tapered r["illum"] in place
-            fx = lib().orc_finalize_extra_f32 if precision == "f32" else lib().orc_finalize_extra_f64
-            fx(_p(r["g2"]), _p(r["g3"]), _p(r["g4"]), _p(r["g3t"]), _p(r["illum"]), g.nxlength, nz, nx, g.nx1,
-               *[_p(ximg[k]) for k in xnames])
-    return dict(image1=image1, image2s=image2s, image2m=image1.copy(), illum=illum,
-                gathers=out_gathers, fields=fields, **ximg)
+        _migrate_shot(s, g, vp, rho, vp_mig, rho_mig, s["mode"], None if s["mode"] == 0 else gathers[k],
+                      s.get("mute", 1), nw, tlength, precision, keep_fields, extra, images, fields, out_gathers)
+    return dict(image2m=images["image1"].copy(), gathers=out_gathers, fields=fields, **images)
+
+
+# ---- the real-data path (rtm_real.cu) ----
+class RealGeom:
+    """Shot window of one recorded shot; the attributes of OrcGeom that the shot loop uses."""
+
+
+def real_geometry(s: dict, sx: int, offset: int, ntrace: int, dx0: float):
+    """rtm_real.cu:134-157 in the reference's float arithmetic: the spread runs from the
+    source to offsetmax = offset + (ntrace-1)*dx0 on its right.  Returns (geometry, ncols0),
+    ncols0 = the spread's width on the data grid."""
+    f = np.float32
+    dx, dz, npml = f(s["dx"]), f(s["dz"]), s["npml"]
+    dx0 = f(dx0)
+    offsetmax = f(f(offset) + f(ntrace - 1) * dx0)
+    off, spx = f(offset), f(sx)
+    noffset0 = int(off / dx0)
+    nx10 = int(spx / dx0)
+    nx20 = int(f(spx + offsetmax) / dx0)
+    g = RealGeom()
+    g.noffset = int(off / dx)
+    g.nx1 = int(spx / dx)
+    g.nx2 = int(f(spx + offsetmax) / dx)
+    g.nxlength = g.nx2 - g.nx1 + 1
+    spx = f(spx - f(g.nx1) * dx)
+    spx = f(spx + f(npml) * dx)
+    spz = f(f(s["spz0"]) + f(npml) * dz)
+    g.nxpad = g.nxlength + 2 * npml
+    g.nzpad = s["nz"] + 2 * npml
+    g.nsx = int(spx / dx)
+    g.nsz = int(spz / dz)
+    g.rx0 = npml + g.noffset
+    g.nrec = g.nxlength - g.noffset
+    return g, nx20 - nx10 + 1 - noffset0
+
+
+def read_traces(path, sgyflag, endianflag, nt0, itrace_all, ntrace, ncols):
+    """The trace loop of rtm_real.cu:379-394 with numpy: [nt0][ncols], unread columns zero."""
+    dt = np.dtype(">f4" if endianflag else "<f4")
+    tb = 240 + 4 * nt0
+    raw = np.fromfile(path, dtype=np.uint8)
+    out = np.zeros((nt0, ncols), np.float32)
+    first = (itrace_all - 1) * tb + 3600 * (1 if sgyflag else 0)
+    for ix in range(min(ntrace, ncols)):
+        o = first + ix * tb + 240
+        out[:, ix] = np.frombuffer(raw[o:o + 4 * nt0].tobytes(), dt)
+    return out
+
+
+def interp_gather(seisobs, nx, nt, dt, dt0, mirror=0):
+    """Interpseis2d (orc_interp.c): seisobs [nt0][nx0] -> [nt][nx]."""
+    obs = f32(seisobs)
+    nt0, nx0 = obs.shape
+    out = np.zeros((nt, nx), np.float32)
+    rc = lib().orc_interp_gather(_p(obs), nx0, nt0, _p(out), nx, nt, dt, dt0, mirror)
+    if rc:
+        raise ValueError(f"orc_interp_gather failed ({rc})")
+    return out
+
+
+def fk_interp(seisin, nx, lx, mirror=0):
+    """GeneralFKinterp (orc_interp.c): seisin [nt0][nx0] -> [nt0][nx]."""
+    a = f32(seisin)
+    nt0, nx0 = a.shape
+    out = np.zeros((nt0, nx), np.float32)
+    rc = lib().orc_fk_interp(_p(a), _p(out), nx, nx0, nt0, lx, mirror)
+    if rc:
+        raise ValueError(f"orc_fk_interp failed ({rc})")
+    return out
+
+
+def rtm_real(survey: dict, path: str, profile, shots, vp, rho, nt0, dt0, dx0, sgyflag=0, endianflag=0,
+             precision="f32", extra=0, mirror=0):
+    """Restatement of the reference's rtm_real shot loop (rtm_real.cu:130-468): per shot
+    (1-based numbers into ``profile`` = [sx, ntrace, first trace, offset] rows) the geometry,
+    the recorded traces, Interpseis2d onto the model grid, the direct-wave mute in the
+    migration model (the reference mutes after smoothing) and the migration.  ``survey``
+    keys as for rtm_model (layout, spx0, dspx, offset, offsetmax unused)."""
+    s = dict(survey)
+    nx, nz = s["nx"], s["nz"]
+    images = _new_images(nz, nx, precision, extra)
+    out_gathers, fields = [], []
+    nw, tlength = _mute_lengths(s)
+    prof = np.asarray(profile)
+    for ishot in shots:
+        sx, ntrace, itr, off = (int(prof[r][ishot - 1]) for r in range(4))
+        g, ncols0 = real_geometry(s, sx, off, ntrace, dx0)
+        obs = read_traces(path, sgyflag, endianflag, nt0, itr, ntrace, ncols0)
+        gather = interp_gather(obs, g.nrec, s["nt"], s["dt"], dt0, mirror)
+        _migrate_shot(s, g, vp, rho, None, None, 1, gather, 2 if s.get("mute", 1) else 0, nw, tlength, precision,
+                      False, extra, images, fields, out_gathers)
+    return dict(image2m=images["image1"].copy(), gathers=out_gathers, **images)
 
 
 # ---- the reference's own host code (compiled from its sources) ----

@@ -12,6 +12,8 @@
 //   ref_harness units <dir>      unit kernels + 300 forward / 20 backward steps
 //   ref_harness rtm <dir>        three rtm_model() runs (layouts 1 and 2, modes 0 and 1)
 //   ref_harness time <dir> <case> per-shot timing of rtm_model() at a larger parity size
+//   ref_harness real <dir>       scanshotgather() + rtm_real() on a synthetic 3-shot SEG-Y
+//                                file (called with rtm_real.cu's own argument list)
 #include <cuda_runtime.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -28,7 +30,12 @@ static cudaError_t harness_malloc(void **p, size_t n) { return cudaMalloc(p, n +
 #include "kernel.cu"
 #define cudaMalloc(ptr, n) harness_malloc((void **)(ptr), (n))
 #include "rtm_model.cu"
+#include "rtm_real.cu"
 #undef cudaMalloc
+
+// scanshotgather is defined in the reference's RTM_GPU_velstr.cpp (compiled with its main
+// renamed).
+void scanshotgather(char filename_shotgather[40], int **shotprofileId, int sgyflag, int *endianflag);
 
 static std::string g_dir;
 
@@ -355,10 +362,108 @@ static int run_time(const std::string root, const std::string which)
     return 0;
 }
 
+// ---------------------------------------------------------------------------------------
+// Real-data path.  Model grid dx = 10 m (nx 192, nz 64, nt 600 at 1 ms); data grid dx0 = 20 m,
+// nt0 = 300 at 2 ms, so every shot goes through the F-K (x2) and sinc (x2) interpolation.
+// Shots at sx = 0, 400, 800 m, 46 receivers from 50 m offset every 20 m: nxlength = 96,
+// noffset = 5, 91 migrated traces, 46 data traces; nxlength, nz, nxpad, nzpad are multiples
+// of 32.  Data: three hyperbolic 20 Hz Ricker events.
+static const int kRealShots = 3, kRealTraces = 46, kRealNt0 = 300;
+static const float kRealDx0 = 20.f, kRealDt0 = 2e-3f, kRealOffset = 50.f;
+
+static void put_i32(unsigned char *h, int off, int v) { std::memcpy(h + off, &v, 4); }
+static void put_i16(unsigned char *h, int off, short v) { std::memcpy(h + off, &v, 2); }
+
+static int write_real_file(const std::string &path)
+{
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) return 4;
+    std::vector<unsigned char> vol(3600, 0);
+    std::fwrite(vol.data(), 1, 3600, f);
+    const float t0s[3] = {0.12f, 0.28f, 0.45f}, amps[3] = {1.0f, -0.6f, 0.4f};
+    std::vector<float> tr(kRealNt0);
+    int itr = 1;
+    for (int s = 0; s < kRealShots; s++) {
+        const int sx = 400 * s;
+        for (int j = 0; j < kRealTraces; j++) {
+            const float h = kRealOffset + j * kRealDx0;
+            unsigned char hd[240];
+            std::memset(hd, 0, sizeof(hd));
+            put_i32(hd, 0, itr++);
+            put_i32(hd, 12, j + 1);
+            put_i32(hd, 36, (int)h);
+            put_i32(hd, 72, sx);
+            put_i32(hd, 80, sx + (int)h);
+            put_i16(hd, 114, (short)kRealNt0);
+            put_i16(hd, 116, (short)2000);
+            float d2 = kRealDx0;
+            std::memcpy(hd + 188, &d2, 4);
+            put_i32(hd, 208, kRealTraces);
+            std::fwrite(hd, 1, 240, f);
+            for (int it = 0; it < kRealNt0; it++) {
+                double t = it * (double)kRealDt0, v = 0.0;
+                for (int e = 0; e < 3; e++) {
+                    double te = std::sqrt((double)t0s[e] * t0s[e] + (h / 2000.0) * (h / 2000.0));
+                    double a = M_PI * 20.0 * (t - te);
+                    v += amps[e] * (1.0 - 2.0 * a * a) * std::exp(-a * a);
+                }
+                tr[it] = (float)v;
+            }
+            std::fwrite(tr.data(), sizeof(float), kRealNt0, f);
+        }
+    }
+    std::fclose(f);
+    return 0;
+}
+
+static int run_real(const std::string root)
+{
+    std::string dir = root + "/real";
+    mkdir_p(dir);
+    mkdir_p(dir + "/seisReal");
+    mkdir_p(dir + "/output");
+    int rc = write_real_file(dir + "/seisReal/real.sgy");
+    if (rc) return rc;
+    const int nx = 192, nz = 64, nt = 600, npml = 32;
+    const float dx = 10.f, dt = 1e-3f;
+    std::vector<float> vp(nx * nz), rho(nx * nz), diffcoef(100), wavelet(nt);
+    make_model(nx, nz, dx, vp.data(), rho.data(), 0);
+    coef_table(diffcoef.data());
+    Ricker(wavelet.data(), 20.f, nt, dt, 1);
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd))) return 5;
+    if (chdir(dir.c_str()) != 0) return 5;
+    g_dir = ".";
+    dump_host("vp0", vp.data(), vp.size());
+    dump_host("rho0", rho.data(), rho.size());
+    const int nshotall = kRealShots + 2;   // room for a trailing entry
+    std::vector<int> prof(4 * nshotall, -7);
+    int *rows[4] = {&prof[0], &prof[nshotall], &prof[2 * nshotall], &prof[3 * nshotall]};
+    char fname[40] = "real.sgy";
+    int endianflag = -1;
+    scanshotgather(fname, rows, 1, &endianflag);
+    dump_host("profile", prof.data(), prof.size());
+    dump_host("endianflag", &endianflag, 1);
+    std::vector<std::vector<float>> img(10, std::vector<float>(nx * nz, 0.0f));
+    rtm_real(0, kRealShots, 1, 1, /*medium_flag*/ 1, /*flag_layout*/ 3, /*sgyflag*/ 1, endianflag, /*ismth*/ 2,
+             nx, nz, nt, dx, dx, dt, nx / 2, nz / 2, kRealNt0, kRealDx0, kRealDx0, kRealDt0, npml, 2, 2,
+             /*tsnap*/ 1.0f, /*fdom*/ 20.f, /*spz0*/ 20.f, /*amp*/ 1.f, /*alp*/ 0.1f, /*direct*/ 1.5f,
+             /*direct0*/ 0.05f, vp.data(), rho.data(), diffcoef.data(), wavelet.data(), fname, rows,
+             img[0].data(), img[1].data(), img[2].data(), img[3].data(), img[4].data(), img[5].data(),
+             img[6].data(), img[7].data(), img[8].data(), img[9].data());
+    ck("rtm_real");
+    const char *names[10] = {"image1", "image2s", "image3s", "image4s", "image5s",
+                             "image2m", "image3m", "image4m", "image5m", "illum"};
+    for (int i = 0; i < 10; i++) dump_host(names[i], img[i].data(), img[i].size());
+    if (chdir(cwd) != 0) return 5;
+    std::printf("real done\n");
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s units|rtm|time <outdir> [case]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s units|rtm|time|real <outdir> [case]\n", argv[0]);
         return 1;
     }
     std::string mode = argv[1];
@@ -368,5 +473,6 @@ int main(int argc, char **argv)
     if (mode == "units") return run_units();
     if (mode == "rtm") return run_rtm(g_dir);
     if (mode == "time") return run_time(g_dir, argc > 3 ? argv[3] : "cfg1");
+    if (mode == "real") return run_real(g_dir);
     return 1;
 }

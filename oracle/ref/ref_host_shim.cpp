@@ -14,6 +14,8 @@ void get_constant(float *vp, float fdom, float dx0, float dz0, int nx0, int nz0,
 void get_parameter(char buff[40], int sgyflag, int *ntrace, short int *nsample, short int *dt,
                    int *endianflag);
 
+void scanshotgather(char filename_shotgather[40], int **shotprofileId, int sgyflag, int *endianflag);
+
 // RTM_GPU_velstr.cpp is compiled (with its main renamed) only for get_constant; it refers to
 // the GPU entry points, which this host-only library never calls.
 extern "C" void rtm_model() { std::abort(); }
@@ -67,5 +69,51 @@ void ref_get_parameter(char *path, int sgyflag, int *ntrace, int *nsample, int *
     short ns = 0, d = 0;
     get_parameter(path, sgyflag, ntrace, &ns, &d, endian);
     *nsample = ns; *dt = d;
+}
+// scanshotgather (RTM_GPU_velstr.cpp:363-454) on ./seisReal/<name> under the working
+// directory.  profile is [4][max_shots] (the rows of shotprofileId); the caller pre-fills it.
+void ref_scanshotgather(char *name, int sgyflag, int *endianflag, int *profile, int max_shots)
+{
+    int *rows[4] = {profile, profile + max_shots, profile + 2 * max_shots, profile + 3 * max_shots};
+    scanshotgather(name, rows, sgyflag, endianflag);
+}
+// Interpseis2d (Interp_function.cpp:245-264): seisobs [nt0][nx0] -> seiscal [nt][nx].  The
+// output rows are zeroed first, so a branch that writes nothing leaves zeros.
+void ref_Interpseis2d(float *seiscal, const float *seisobs, int nx, int nx0, int nt, int nt0, float dt, float dt0)
+{
+    float **out = Creat2dArray(nt, nx), **in = Creat2dArray(nt0, nx0);
+    for (int i = 0; i < nt0; i++)
+        for (int j = 0; j < nx0; j++) in[i][j] = seisobs[(size_t)i * nx0 + j];
+    for (int i = 0; i < nt; i++)
+        for (int j = 0; j < nx; j++) out[i][j] = 0.0f;
+    Interpseis2d(out, in, nx, nx0, nt, nt0, dt, dt0);
+    for (int i = 0; i < nt; i++)
+        for (int j = 0; j < nx; j++) seiscal[(size_t)i * nx + j] = out[i][j];
+    free2dArray(out, nt, nx);
+    free2dArray(in, nt0, nx0);
+}
+// GeneralFKinterp (Interp_function.cpp:127-244): seisin [nt0][nx0] -> seisout [nt0][nx].
+void ref_GeneralFKinterp(const float *seisin, float *seisout, int nx, int nx0, int nt0, int lx)
+{
+    float **out = Creat2dArray(nt0, nx), **in = Creat2dArray(nt0, nx0);
+    for (int i = 0; i < nt0; i++)
+        for (int j = 0; j < nx0; j++) in[i][j] = seisin[(size_t)i * nx0 + j];
+    GeneralFKinterp(in, out, nx, nx0, nt0, lx);
+    for (int i = 0; i < nt0; i++)
+        for (int j = 0; j < nx; j++) seisout[(size_t)i * nx + j] = out[i][j];
+    free2dArray(out, nt0, nx);
+    free2dArray(in, nt0, nx0);
+}
+// Sincinterp (Interp_function.cpp:61-115): seisin [nt0][nx] -> seisout [nt][nx].
+void ref_Sincinterp(const float *seisin, float *seisout, int nx, int nt, int nt0, float dt, float dt0)
+{
+    float **out = Creat2dArray(nt, nx), **in = Creat2dArray(nt0, nx);
+    for (int i = 0; i < nt0; i++)
+        for (int j = 0; j < nx; j++) in[i][j] = seisin[(size_t)i * nx + j];
+    Sincinterp(in, out, nx, nt, nt0, dt, dt0);
+    for (int i = 0; i < nt; i++)
+        for (int j = 0; j < nx; j++) seisout[(size_t)i * nx + j] = out[i][j];
+    free2dArray(out, nt, nx);
+    free2dArray(in, nt0, nx);
 }
 }

@@ -88,7 +88,9 @@ void orc_get_constant(const float *vp, float fdom, float dx0, float dz0, int nx0
 /* ---- per-shot RTM (the hot path) ----
  * mode 0: model the gather in vp2f/rhof (written, unmuted, to `gather`), then migrate it.
  * mode 1: `gather` (nt*nrec) is the recorded data, migrated as given.
- * mute != 0 applies the direct-wave mute of kernel.cu:96-121 to the migrated copy.
+ * mute != 0 applies the direct-wave mute of kernel.cu:96-121 to the migrated copy, with the
+ * velocities of vp2f (mute 1, rtm_model.cu: before smoothing) or of vp2b (mute 2, the
+ * real-data driver rtm_real.cu:397-403, which mutes after smoothing).
  * vp2b/rhob: model of the backward pass (differs from the forward one only when the
  * reference smooths after the source pass, rtm_model.cu:402-408).
  * g1/illum: nz*nxlen interior images (untapered).  ps_out/p_out (optional, Z*X): the
@@ -149,6 +151,14 @@ void orc_finalize_extra_f64(double *g2, double *g3, double *g4, double *g3t, con
 
 /* Threads used by the OpenMP loops (1 when built without OpenMP). */
 int orc_num_threads(void);
+
+/* Seismic interpolation of the real-data path (orc_interp.c; Interp_function.cpp). */
+void orc_kaiser(float *w, int n, double beta);
+void orc_sinc_interp(const float *seisin, int ld_in, float *seisout, int nx, int nt, int nt0, float dt,
+                     float dt0);
+int orc_fk_interp(const float *seisin, float *seisout, int nx, int nx0, int nt0, int lx, int mirror);
+int orc_interp_gather(const float *seisobs, int nx0, int nt0, float *seiscal, int nx, int nt, float dt,
+                      float dt0, int mirror);
 
 #ifdef __cplusplus
 }

@@ -492,7 +492,8 @@ int SFX(orc_shot_ex)(const orc_shot *s, const float *vp2f, const float *rhof, co
     if (mute) {
         float dx2 = s->dx * s->dx, dz2 = s->dz * s->dz;
         float rdt = (float)(1.0 / s->dt);  /* rtm_model.cu:75 */
-        orc_mute(mig, vp2f, X, s->nsx, s->nsz, nt, s->rz, s->rx0, s->nrec, nw, tlength, dx2, dz2, rdt);
+        orc_mute(mig, mute == 2 ? vp2b : vp2f, X, s->nsx, s->nsz, nt, s->rz, s->rx0, s->nrec, nw, tlength, dx2, dz2,
+                 rdt);
     }
     for (i = 0; i < (size_t)nt * s->nrec; i++) rec[i] = (R)mig[i];
 
