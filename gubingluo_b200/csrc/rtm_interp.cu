@@ -64,24 +64,47 @@ __device__ __forceinline__ float sinc_f(float x)
 // Sincinterp: out [nt][nx] from in [nt0][ld_in].  Window start it0 - 10 around
 // it0 = (int)((it+1)*dt/dt0), sinc centred on it*dt, taps cut at the ends as the reference
 // does (at the start the window shifts with the cut, at the end it keeps its first taps).
-__global__ void k_sinc(const float *__restrict__ in, int ld_in, float *__restrict__ out, int nx, int nt, int nt0,
-                       float dt, float dt0, Kaiser21 kw)
+// The sinc values and window taps depend on the output sample's time only: each block of
+// kSincRows rows x 32 traces evaluates them once per row into shared memory (the reference
+// evaluates them per trace), then every thread forms (trace * sinc) * window tap by tap.
+constexpr int kSincRows = 8;
+__global__ void __launch_bounds__(32 * kSincRows) k_sinc(const float *__restrict__ in, int ld_in, float *__restrict__ out,
+                                                         int nx, int nt, int nt0, float dt, float dt0, Kaiser21 kw)
 {
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    const int it = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= nx || it >= nt) return;
+    __shared__ float s_sinc[kSincRows][kTaps], s_win[kSincRows][kTaps];
+    __shared__ int s_start[kSincRows], s_len[kSincRows];
     const int halfnw = 10;
-    const int it0 = (int)__fdiv_rn(__fmul_rn((float)(it + 1), dt), dt0);
-    const int itstart = max(0, it0 - halfnw), itend = min(nt0 - 1, it0 + halfnw);
-    const int lenit = itend - itstart + 1;
-    const int inwstart = itstart <= halfnw ? kTaps - lenit : 0;
-    const float t = __fmul_rn((float)it, dt);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid < kSincRows * kTaps) {
+        const int r = tid / kTaps, ik = tid % kTaps;
+        const int it = blockIdx.y * kSincRows + r;
+        if (it < nt) {
+            const int it0 = (int)__fdiv_rn(__fmul_rn((float)(it + 1), dt), dt0);
+            const int itstart = max(0, it0 - halfnw), itend = min(nt0 - 1, it0 + halfnw);
+            const int lenit = itend - itstart + 1;
+            const int inwstart = itstart <= halfnw ? kTaps - lenit : 0;
+            if (ik == 0) {
+                s_start[r] = itstart;
+                s_len[r] = lenit;
+            }
+            if (ik < lenit) {
+                const float t = __fmul_rn((float)it, dt);
+                const float tn = __fmul_rn((float)(ik + itstart), dt0);
+                s_sinc[r][ik] = sinc_f(__fdiv_rn(__fsub_rn(t, tn), dt0));
+                s_win[r][ik] = kw.w[ik + inwstart];
+            }
+        }
+    }
+    __syncthreads();
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = threadIdx.y;
+    const int it = blockIdx.y * kSincRows + r;
+    if (ix >= nx || it >= nt) return;
+    const int itstart = s_start[r], lenit = s_len[r];
     float sum = 0.0f;
     for (int ik = 0; ik < lenit; ik++) {
-        const float tn = __fmul_rn((float)(ik + itstart), dt0);
         const float a = in[(size_t)(ik + itstart) * ld_in + ix];
-        const float b = sinc_f(__fdiv_rn(__fsub_rn(t, tn), dt0));
-        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(a, b), kw.w[ik + inwstart]));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(a, s_sinc[r][ik]), s_win[r][ik]));
     }
     out[(size_t)it * nx + ix] = sum;
 }
@@ -338,7 +361,7 @@ static int interp_run(InterpPlan &p, float *out, float dt, float dt0, int mirror
         ld = sh.nx;
     }
     if (sh.sinc) {
-        dim3 blk(32, 8), grd((sh.nx + 31) / 32, (sh.nt + 7) / 8);
+        dim3 blk(32, kSincRows), grd((sh.nx + 31) / 32, (sh.nt + kSincRows - 1) / kSincRows);
         k_sinc<<<grd, blk, 0, st>>>(src, ld, out, sh.nx, sh.nt, sh.nt0, dt, dt0, kaiser_window());
         if (launches) *launches += 1;
     } else if (!sh.fk) {
