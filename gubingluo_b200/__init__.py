@@ -20,7 +20,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librtm_b200.so")
 
-RTM_OK, RTM_ERR_ARG, RTM_ERR_CUDA, RTM_ERR_IO, RTM_ERR_NOMEM = 0, -1, -2, -3, -4
+RTM_OK, RTM_ERR_ARG, RTM_ERR_CUDA, RTM_ERR_IO, RTM_ERR_NOMEM, RTM_ERR_NUMERIC = 0, -1, -2, -3, -4, -5
 PREC = {"fp32": 0, "fp16": 1, "bf16": 2}
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -40,7 +40,7 @@ class Survey(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("strip_precision", C.c_int), ("gather_precision", C.c_int),
                 ("accum_fp64", C.c_int), ("batch", C.c_int), ("use_graph", C.c_int),
-                ("verbose", C.c_int), ("extra_images", C.c_int)]
+                ("verbose", C.c_int), ("extra_images", C.c_int), ("tsnap", C.c_float)]
 
 
 class Geometry(C.Structure):
@@ -126,6 +126,11 @@ def lib() -> C.CDLL:
                               C.POINTER(Stats)]
     L.rtm_model.restype = None
     L.rtm_real.restype = None
+    L.rtm_session_save_checkpoint.argtypes = [vp, C.c_char_p, C.c_int]
+    L.rtm_session_load_checkpoint.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int)]
+    L.rtm_checkpoint_info.argtypes = [C.c_char_p] + [C.POINTER(C.c_int)] * 5 + [C.POINTER(C.c_ulonglong)]
+    L.rtm_session_config_hash.argtypes = [vp]
+    L.rtm_session_config_hash.restype = C.c_ulonglong
     L.rtm_session_open_geometry.argtypes = [C.POINTER(vp), S, O, C.POINTER(C.c_int), G, C.c_int, vp, vp, vp,
                                             vp, vp]
     L.rtm_session_set_gather_raw.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_float, C.c_int]
@@ -200,6 +205,7 @@ class RunOptions:
     use_graph: bool = False
     verbose: bool = False
     extra_images: int = 0   # 1: image3/4/5 and imagetrue, indexing corrected; 2: the reference's
+    tsnap: float = 0.0      # with verbose: print max |p| per shot every tsnap seconds
 
     def c(self) -> Options:
         o = Options()
@@ -211,6 +217,7 @@ class RunOptions:
         o.use_graph = int(self.use_graph)
         o.verbose = int(self.verbose)
         o.extra_images = int(self.extra_images)
+        o.tsnap = float(self.tsnap)
         return o
 
 
@@ -247,6 +254,20 @@ class Session:
             _check(lib().rtm_session_open_geometry(C.byref(h), C.byref(survey.c()), C.byref(options.c()), ids,
                                                    self._geoms, len(self.shots), *[_ptr(a) for a in self._keep]))
         self.h = h
+
+    def save_checkpoint(self, path: str, shots_done: int):
+        """Stacked images after ``shots_done`` shots, for ``load_checkpoint``."""
+        _check(lib().rtm_session_save_checkpoint(self.h, path.encode(), shots_done))
+
+    def load_checkpoint(self, path: str) -> int:
+        """Restores the images of a checkpoint of the same configuration; returns the number of
+        shots it had stacked (continue with ``run_range`` from there)."""
+        done = C.c_int(0)
+        _check(lib().rtm_session_load_checkpoint(self.h, path.encode(), C.byref(done)))
+        return done.value
+
+    def config_hash(self) -> int:
+        return lib().rtm_session_config_hash(self.h)
 
     def set_gather_raw(self, k: int, seisobs, dt0: float, mirror: int = 0):
         """Recorded traces [nt0][nx0] of shot k, resampled on the device to [nt][nrec_k]."""
@@ -372,6 +393,14 @@ def migrate(survey: SurveyConfig, options: RunOptions, shots, vp, rho, gathers=N
             out["gathers"] = [ss.gather(k) for k in range(len(ss.shots))]
         out["stats"] = stats
     return out
+
+
+def checkpoint_info(path: str) -> dict:
+    """Header of a checkpoint file (no device work)."""
+    v = [C.c_int(0) for _ in range(5)]
+    h = C.c_ulonglong(0)
+    _check(lib().rtm_checkpoint_info(path.encode(), *[C.byref(x) for x in v], C.byref(h)))
+    return dict(zip(("nx", "nz", "nshots", "shots_done", "elem_bytes"), [x.value for x in v]), config_hash=h.value)
 
 
 # ---- real-data path ----

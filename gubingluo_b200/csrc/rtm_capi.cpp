@@ -53,15 +53,48 @@ static void drive(const char *who, rtm_session *ss, const rtm_survey &s, const r
     std::vector<float> tmp(nimg);
     std::vector<float> xi[7];   // image3s .. image5m, imagetrue (zero unless extra_images)
     for (auto &v : xi) v.assign(nimg, 0.0f);
-    for (size_t k0 = 0; k0 < shots.size(); k0 += B) {
+    // checkpoint after every batch (RTM_B200_CHECKPOINT=<path>); resume from it
+    // (RTM_B200_RESUME=1) when it exists and matches this run
+    const char *ckpt = std::getenv("RTM_B200_CHECKPOINT");
+    if (ckpt && !*ckpt) ckpt = nullptr;
+    size_t start = 0;
+    if (ckpt && env_int("RTM_B200_RESUME", 0)) {
+        FILE *probe = std::fopen(ckpt, "rb");
+        if (!probe) {
+            std::printf("%s: no checkpoint at %s, starting from the first shot\n", who, ckpt);
+        } else {
+            std::fclose(probe);
+            int done = 0;
+            if (rtm_session_load_checkpoint(ss, ckpt, &done)) {
+                std::printf("%s: %s\n", who, rtm_last_error());
+                return;
+            }
+            start = (size_t)done;
+            std::printf("%s: resuming after %d of %zu shots from %s\n", who, done, shots.size(), ckpt);
+        }
+    }
+    // one JSON line per batch (RTM_B200_LOG=<path>)
+    FILE *log = nullptr;
+    if (const char *lp = std::getenv("RTM_B200_LOG"))
+        if (*lp) log = std::fopen(lp, "a");
+    for (size_t k0 = start; k0 < shots.size(); k0 += B) {
         int n = (int)std::min<size_t>(B, shots.size() - k0);
         auto t0 = std::chrono::steady_clock::now();
         rc = session_run_range(ss, (int)k0, n);
         if (rc) {
             std::printf("%s: %s\n", who, rtm_last_error());
+            if (log) std::fclose(log);
             return;   // the caller closes the session
         }
         double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (ckpt && rtm_session_save_checkpoint(ss, ckpt, (int)(k0 + n)))
+            std::printf("%s: %s\n", who, rtm_last_error());
+        if (log) {
+            std::fprintf(log, "{\"entry\": \"%s\", \"first_shot\": %d, \"last_shot\": %d, \"shots\": %d, "
+                              "\"seconds\": %.6f, \"shots_per_s\": %.6f, \"shots_done\": %zu, \"shots_total\": %zu}\n",
+                         who, shots[k0], shots[k0 + n - 1], n, sec, n / sec, k0 + n, shots.size());
+            std::fflush(log);
+        }
         bool temp_dump = false;
         for (int j = 0; j < n; j++) {
             const int ishot = shots[k0 + j];
@@ -98,6 +131,7 @@ static void drive(const char *who, rtm_session *ss, const rtm_survey &s, const r
             }
         }
     }
+    if (log) std::fclose(log);
     rtm_session_get_images(ss, image1, image2s, image2m, illum);   // rtm_model.cu:575-585
     if (o.extra_images)
         rtm_session_get_images_extra(ss, image3s, image4s, image5s, image3m, image4m, image5m, xi[6].data());
@@ -114,7 +148,6 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
                float *image1, float *image2s, float *image3s, float *image4s, float *image5s, float *image2m,
                float *image3m, float *image4m, float *image5m, float *illum)
 {
-    (void)tsnap;
     (void)wavelet;   // the reference regenerates the wavelet on the device (rtm_model.cu:86-88)
     clear_error();
     rtm_survey s;
@@ -133,6 +166,7 @@ void rtm_model(int idevice, int nshot, int startshot, int dshot, int mode, int m
     o.accum_fp64 = env_int("RTM_B200_ACCUM_FP64", 0);
     o.batch = env_int("RTM_B200_BATCH", 0);
     o.verbose = 1;
+    o.tsnap = tsnap;
     // image3*/4*/5* and Imagetrue: the reference's other imaging conditions, with vx and vz
     // read at their own cells (1, the default) or with the reference's indexing (2); 0 leaves
     // those images zero and saves their cost
@@ -189,7 +223,7 @@ void rtm_real(int idevice, int nshot, int startshot, int dshot, int medium_flag,
               float *illum)
 {
     // accepted and unused, as in the reference (rtm_real.cu:17-581)
-    (void)flag_layout; (void)nx0; (void)nz0; (void)dz0; (void)lx; (void)lz; (void)tsnap; (void)wavelet;
+    (void)flag_layout; (void)nx0; (void)nz0; (void)dz0; (void)lx; (void)lz; (void)wavelet;
     clear_error();
     rtm_survey s;
     std::memset(&s, 0, sizeof(s));
@@ -208,6 +242,7 @@ void rtm_real(int idevice, int nshot, int startshot, int dshot, int medium_flag,
     o.batch = env_int("RTM_B200_BATCH", 0);
     o.verbose = 1;
     o.extra_images = env_int("RTM_B200_EXTRA_IMAGES", 1);
+    o.tsnap = tsnap;
     const int mirror = env_int("RTM_B200_FK_MIRROR", 0);
     const size_t nimg = (size_t)nx * nz;
     float *zero_imgs[6] = {image3s, image4s, image5s, image3m, image4m, image5m};

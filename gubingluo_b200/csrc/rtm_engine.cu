@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
@@ -115,6 +116,10 @@ struct rtm_session {
     int last_batch_n = 0;
     std::vector<int> last_batch_shots;
     rtm::InterpPlan interp;          // real-data path: workspace of the gather interpolation
+    int *d_nonfinite = nullptr;      // lowest batch index of a shot whose image went non-finite
+    unsigned *d_absmax = nullptr;    // progress snapshots: [2 passes][snaps][B] max |p| bits
+    int nsnap = 0;                   // snapshots per pass (0: none)
+    unsigned long long config_hash = 0;   // survey, image-relevant options, shots, models
 };
 
 namespace rtm {
@@ -165,6 +170,29 @@ static int check_kernel_flag(rtm_session *ss)
         CK(cudaMemset(ss->d_err, 0, sizeof(int)));
         return fail(RTM_ERR_CUDA, "a stencil kernel gave up waiting for its tile (TMA copy did not complete)");
     }
+    return RTM_OK;
+}
+
+// FNV-1a, 64 bit.
+static unsigned long long fnv1a(const void *data, size_t n, unsigned long long h = 1469598103934665603ULL)
+{
+    const unsigned char *p = (const unsigned char *)data;
+    for (size_t i = 0; i < n; i++) {
+        h ^= p[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+// After a batch: a shot whose image holds NaN or infinity stops the run with a status.
+static int check_nonfinite(rtm_session *ss, int k0, int n)
+{
+    int bad = n;
+    CK(cudaMemcpy(&bad, ss->d_nonfinite, sizeof(int), cudaMemcpyDeviceToHost));
+    if (bad >= 0 && bad < n)
+        return fail(RTM_ERR_NUMERIC, "shot " + std::to_string(ss->shots[k0 + bad].ishot) +
+                                         ": the image holds NaN or infinite values (the wavefield diverged: time step "
+                                         "above the stability limit, or invalid model values)");
     return RTM_OK;
 }
 
@@ -474,7 +502,16 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
     ss->d_tmaps = ss->arena.take((size_t)B * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
     ss->d_err = (int *)ss->arena.take(sizeof(int));
-    if (!ss->d_tmaps || !ss->d_err) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
+    ss->d_nonfinite = (int *)ss->arena.take(sizeof(int));
+    if (!ss->d_tmaps || !ss->d_err || !ss->d_nonfinite) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
+    if (o.verbose && o.tsnap > 0.0f) {
+        const int ntsnap = (int)(o.tsnap / s.dt);   // rtm_model.cu:21
+        if (ntsnap >= 1) {
+            ss->nsnap = (s.nt + ntsnap - 1) / ntsnap;
+            ss->d_absmax = (unsigned *)ss->arena.take(sizeof(unsigned) * 2 * ss->nsnap * B);
+            if (!ss->d_absmax) return fail(RTM_ERR_NOMEM, "device arena exhausted (snapshots)");
+        }
+    }
     CK(cudaMemsetAsync(ss->d_err, 0, sizeof(int), ss->stream));
     const int bz_min = std::min(ss->bz_vel, ss->bz_pres);
     int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + bz_min - 1) / bz_min);
@@ -487,6 +524,24 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_tiles_r || !ss->d_tiles_pr || !ss->d_fin)
         return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     CK(cudaStreamSynchronize(ss->stream));
+    // what a checkpoint must agree on: the survey, the options that change the images, the
+    // shots and their geometry, the models and the coefficients
+    {
+        const size_t nm = (size_t)s.nx * s.nz;
+        unsigned long long h = fnv1a(&s, sizeof(s));
+        const int oi[4] = {o.strip_precision, o.gather_precision, o.accum_fp64, o.extra_images};
+        h = fnv1a(oi, sizeof(oi), h);
+        for (const ShotState &sh : ss->shots) {
+            h = fnv1a(&sh.ishot, sizeof(int), h);
+            h = fnv1a(&sh.g, sizeof(sh.g), h);
+        }
+        h = fnv1a(vp, nm * sizeof(float), h);
+        h = fnv1a(rho, nm * sizeof(float), h);
+        if (vp_mig) h = fnv1a(vp_mig, nm * sizeof(float), h);
+        if (rho_mig) h = fnv1a(rho_mig, nm * sizeof(float), h);
+        h = fnv1a(ss->coef_host, sizeof(ss->coef_host), h);
+        ss->config_hash = h;
+    }
     return RTM_OK;
 }
 
@@ -647,6 +702,32 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     return RTM_OK;
 }
 
+// Progress lines of the reference (rtm_model.cu:324-326, 415-417), one per shot of the batch
+// and snapshot, from the device reductions of the pass just queued.
+static int print_snapshots(rtm_session *ss, const BatchRun &br, int side, const char *label, int nsteps, int ntsnap)
+{
+    const int B = ss->B;
+    std::vector<unsigned> h((size_t)ss->nsnap * B);
+    CK(cudaMemcpyAsync(h.data(), ss->d_absmax + (size_t)side * ss->nsnap * B, sizeof(unsigned) * h.size(),
+                       cudaMemcpyDeviceToHost, ss->stream));
+    CK(cudaStreamSynchronize(ss->stream));
+    std::vector<int> its;
+    if (side == 0)
+        for (int it = 0; it < nsteps; it += ntsnap) its.push_back(it);
+    else
+        for (int it = ss->s.nt - 2; it >= 0; it--)
+            if (it % ntsnap == 0) its.push_back(it);
+    for (int it : its)
+        for (int j = 0; j < br.n; j++) {
+            float v;
+            unsigned bits = h[(size_t)(it / ntsnap) * B + j];
+            std::memcpy(&v, &bits, 4);
+            std::printf("%s-the current shot: %d\ttime: %f s; wavefield: %.5e\n", label, ss->shots[br.k0 + j].ishot,
+                        it * ss->s.dt, v);
+        }
+    return RTM_OK;
+}
+
 // Source pass (rtm_model.cu:322-346): nsteps forward steps with the source added; strips
 // saved after every step when `save` (one small copy kernel, so the stencil kernels carry no
 // strip logic); the gather recorded when `record` (mode 0 fuses the reference's separate
@@ -657,10 +738,17 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
     const rtm_options &o = ss->o;
     cudaStream_t st = ss->stream;
     StepArgs &a = br.a;
+    const int ntsnap = ss->nsnap ? (int)(o.tsnap / ss->s.dt) : 0;
+    if (ntsnap) CK(cudaMemsetAsync(ss->d_absmax, 0, sizeof(unsigned) * ss->nsnap * ss->B, st));
+    nvtxRangePushA(record && !save ? "rtm: modelling pass" : "rtm: source pass");
     for (int it = 0; it < nsteps; it++) {
         a.it = it;
         a.ring = it % kRing;
         const int mode = RTM_WAVE_FWD;
+        if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:324-326: |p| before the step
+            launch_absmax(ss->d_shots, br.n, 0, ss->d_absmax + (size_t)(it / ntsnap) * ss->B, st);
+            ss->launches++;
+        }
         cudaEvent_t e;
         timing_begin(ss, "vel_fwd", it, &e);
         a.tiles = ss->d_tiles;
@@ -680,7 +768,9 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
             ss->launches++;
         }
     }
+    nvtxRangePop();
     CK(cudaGetLastError());
+    if (ntsnap) return print_snapshots(ss, br, 0, save ? "source" : "forward", nsteps, ntsnap);
     return RTM_OK;
 }
 
@@ -733,9 +823,17 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             max_nxi = std::max(max_nxi, sh.nxi);
             max_nzi = std::max(max_nzi, sh.nzi);
         }
+    const int ntsnap = ss->nsnap ? (int)(o.tsnap / s.dt) : 0;
+    unsigned *snap_b = ntsnap ? ss->d_absmax + (size_t)ss->nsnap * ss->B : nullptr;
+    if (ntsnap) CK(cudaMemsetAsync(snap_b, 0, sizeof(unsigned) * ss->nsnap * ss->B, st));
+    nvtxRangePushA("rtm: backward pass");
     for (int it = s.nt - 2; it >= 0; it--) {
         a.it = it;
         cudaEvent_t e;
+        if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:415-417: receiver |p| before the step
+            launch_absmax(ss->d_shots, n, 1, snap_b + (size_t)(it / ntsnap) * ss->B, st);
+            ss->launches++;
+        }
         // reconstruction of the source wavefield, then the receiver wavefield and imaging
         // (which reads the reconstructed pressure of the same step)
         timing_begin(ss, "vel_recon", it, &e);
@@ -761,7 +859,13 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             ss->launches++;
         }
     }
+    nvtxRangePop();
     CK(cudaGetLastError());
+    if (ntsnap) {
+        int rc = print_snapshots(ss, br, 1, "backward", s.nt, ntsnap);
+        if (rc) return rc;
+    }
+    nvtxRangePushA("rtm: stacking");
     std::vector<char> fin(finalize_shot_size() * n);
     for (int j = 0; j < n; j++) {
         ShotState &sh = ss->shots[br.k0 + j];
@@ -771,12 +875,15 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
                            o.extra_images ? ss->slots[j].gx : nullptr, sh.g.nx1, sh.nxi, nwin, sh.pitch, s.npml);
     }
     CK(cudaMemcpyAsync(ss->d_fin, fin.data(), fin.size(), cudaMemcpyHostToDevice, st));
-    launch_finalize(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->img1, ss->img2s, ss->img2m, ss->illum, st);
+    CK(cudaMemsetAsync(ss->d_nonfinite, 0x7f, sizeof(int), st));   // 0x7f7f7f7f: none
+    launch_finalize(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->img1, ss->img2s, ss->img2m, ss->illum,
+                    ss->d_nonfinite, st);
     ss->launches++;
     if (o.extra_images) {
         launch_finalize_extra(ss->d_fin, n, s.nx, s.nz, o.accum_fp64, ss->ximg, st);
         ss->launches++;
     }
+    nvtxRangePop();
     CK(cudaGetLastError());
     return RTM_OK;
 }
@@ -786,10 +893,13 @@ static int run_batch(rtm_session *ss, int k0, int n)
     BatchRun br;
     int rc = batch_setup(ss, k0, n, br);
     if (rc) return rc;
-    if ((rc = batch_forward(ss, br, ss->s.nt, true, ss->s.mode == 0))) return rc;
-    if ((rc = batch_backward(ss, br))) return rc;
+    nvtxRangePushA("rtm: batch");
+    if (!(rc = batch_forward(ss, br, ss->s.nt, true, ss->s.mode == 0))) rc = batch_backward(ss, br);
+    nvtxRangePop();
+    if (rc) return rc;
     CK(cudaStreamSynchronize(ss->stream));
-    return check_kernel_flag(ss);
+    if ((rc = check_kernel_flag(ss))) return rc;
+    return check_nonfinite(ss, k0, n);
 }
 
 int session_batch_size(rtm_session *ss) { return ss ? ss->B : 0; }
@@ -1050,6 +1160,141 @@ int rtm_session_get_images_extra(rtm_session *ss, float *image3s, float *image4s
     }
     return RTM_OK;
 }
+
+// ---- checkpoints ----------------------------------------------------------------------
+// File: the header below, then the session's stacked images as accumulated (image1, image2s,
+// image2m, illum, then with extra_images image3s..5s, image3m..5m, imagetrue), each nx*nz
+// elements of elem_bytes (4 or 8).  Written to "<path>.tmp" and renamed over <path>.
+struct CheckpointHeader {
+    char magic[8];                 // "RTMB200C"
+    unsigned version;              // 1
+    unsigned elem_bytes;
+    unsigned long long config_hash;
+    int nx, nz, nshots, shots_done, nimages, batch;
+};
+
+static int checkpoint_images(rtm_session *ss, void **img)
+{
+    int k = 0;
+    img[k++] = ss->img1;
+    img[k++] = ss->img2s;
+    img[k++] = ss->img2m;
+    img[k++] = ss->illum;
+    if (ss->o.extra_images)
+        for (void *x : ss->ximg) img[k++] = x;
+    return k;
+}
+
+int rtm_session_save_checkpoint(rtm_session *ss, const char *path, int shots_done)
+{
+    if (!ss || !path) return fail(RTM_ERR_ARG, "null argument");
+    if (shots_done < 0 || shots_done > (int)ss->shots.size()) return fail(RTM_ERR_ARG, "shots_done out of range");
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    void *img[11];
+    CheckpointHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, "RTMB200C", 8);
+    h.version = 1;
+    h.elem_bytes = ss->o.accum_fp64 ? 8 : 4;
+    h.config_hash = ss->config_hash;
+    h.nx = ss->s.nx;
+    h.nz = ss->s.nz;
+    h.nshots = (int)ss->shots.size();
+    h.shots_done = shots_done;
+    h.nimages = checkpoint_images(ss, img);
+    h.batch = ss->B;
+    const size_t bytes = (size_t)h.nx * h.nz * h.elem_bytes;
+    std::vector<char> buf(bytes);
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE *f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return fail(RTM_ERR_IO, "cannot create " + tmp);
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+    for (int k = 0; k < h.nimages && ok; k++) {
+        if (cudaMemcpy(buf.data(), img[k], bytes, cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
+        ok = ok && std::fwrite(buf.data(), 1, bytes, f) == bytes;
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok || std::rename(tmp.c_str(), path) != 0) {
+        std::remove(tmp.c_str());
+        return fail(RTM_ERR_IO, std::string("cannot write checkpoint ") + path);
+    }
+    return RTM_OK;
+}
+
+// Reads and checks a checkpoint header (no device work).
+static int read_checkpoint_header(const char *path, CheckpointHeader &h, FILE **keep)
+{
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(RTM_ERR_IO, std::string("cannot open checkpoint ") + path);
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, "RTMB200C", 8) != 0 || h.version != 1 ||
+        (h.elem_bytes != 4 && h.elem_bytes != 8) || h.nx < 1 || h.nz < 1 || h.nimages < 4 || h.nimages > 11 ||
+        h.shots_done < 0 || h.shots_done > h.nshots) {
+        std::fclose(f);
+        return fail(RTM_ERR_IO, std::string("not a checkpoint of this library: ") + path);
+    }
+    std::fseek(f, 0, SEEK_END);
+    const long long want = (long long)sizeof(h) + (long long)h.nimages * h.nx * h.nz * h.elem_bytes;
+    if (std::ftell(f) != want) {
+        std::fclose(f);
+        return fail(RTM_ERR_IO, std::string("truncated checkpoint: ") + path);
+    }
+    if (keep) {
+        std::fseek(f, (long)sizeof(h), SEEK_SET);
+        *keep = f;
+    } else {
+        std::fclose(f);
+    }
+    return RTM_OK;
+}
+
+int rtm_session_load_checkpoint(rtm_session *ss, const char *path, int *shots_done)
+{
+    if (!ss || !path) return fail(RTM_ERR_ARG, "null argument");
+    CheckpointHeader h;
+    FILE *f = nullptr;
+    int rc = read_checkpoint_header(path, h, &f);
+    if (rc) return rc;
+    void *img[11];
+    const int nimg = checkpoint_images(ss, img);
+    if (h.config_hash != ss->config_hash || h.nx != ss->s.nx || h.nz != ss->s.nz ||
+        h.nshots != (int)ss->shots.size() || h.nimages != nimg || h.elem_bytes != (ss->o.accum_fp64 ? 8u : 4u)) {
+        std::fclose(f);
+        return fail(RTM_ERR_ARG, std::string("checkpoint ") + path +
+                                     " was written by a run with another survey, model, shot list or image options");
+    }
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    const size_t bytes = (size_t)h.nx * h.nz * h.elem_bytes;
+    std::vector<char> buf(bytes);
+    for (int k = 0; k < nimg && !rc; k++) {
+        if (std::fread(buf.data(), 1, bytes, f) != bytes) rc = fail(RTM_ERR_IO, std::string("cannot read ") + path);
+        else if (cudaMemcpy(img[k], buf.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(RTM_ERR_CUDA, "checkpoint upload failed");
+    }
+    std::fclose(f);
+    if (!rc && shots_done) *shots_done = h.shots_done;
+    return rc;
+}
+
+int rtm_checkpoint_info(const char *path, int *nx, int *nz, int *nshots, int *shots_done, int *elem_bytes,
+                        unsigned long long *config_hash)
+{
+    clear_error();
+    if (!path) return fail(RTM_ERR_ARG, "null path");
+    CheckpointHeader h;
+    int rc = read_checkpoint_header(path, h, nullptr);
+    if (rc) return rc;
+    if (nx) *nx = h.nx;
+    if (nz) *nz = h.nz;
+    if (nshots) *nshots = h.nshots;
+    if (shots_done) *shots_done = h.shots_done;
+    if (elem_bytes) *elem_bytes = (int)h.elem_bytes;
+    if (config_hash) *config_hash = h.config_hash;
+    return RTM_OK;
+}
+
+unsigned long long rtm_session_config_hash(rtm_session *ss) { return ss ? ss->config_hash : 0ULL; }
 
 int rtm_session_reset_images(rtm_session *ss)
 {

@@ -29,14 +29,26 @@ static void selfdoc()
         "Writes ./output/{idevice}{Illum,Image1,Image2s,...,Image5m}.su.\n"
         "Environment: RTM_B200_STRIPS / RTM_B200_GATHERS = fp32|fp16|bf16,\n"
         "  RTM_B200_ACCUM_FP64=1, RTM_B200_BATCH=<shots per launch>, RTM_B200_RECEIVER_DEPTH=<cells>,\n"
-        "  RTM_B200_EXTRA_IMAGES=0|1|2, RTM_B200_FK_MIRROR=0|1.\n");
+        "  RTM_B200_EXTRA_IMAGES=0|1|2, RTM_B200_FK_MIRROR=0|1, RTM_B200_LOG=<JSON-lines file>.\n"
+        "Options: --checkpoint <file> saves the stacked images after every batch;\n"
+        "  --resume continues from that file when it matches the run (same parameters and models).\n");
 }
 
 int main(int argc, char **argv)
 {
-    if (argc > 1 && (!std::strcmp(argv[1], "--help") || !std::strcmp(argv[1], "-h"))) {
-        selfdoc();
-        return 0;
+    for (int i = 1; i < argc; i++) {
+        if (!std::strcmp(argv[i], "--help") || !std::strcmp(argv[i], "-h")) {
+            selfdoc();
+            return 0;
+        } else if (!std::strcmp(argv[i], "--checkpoint") && i + 1 < argc) {
+            setenv("RTM_B200_CHECKPOINT", argv[++i], 1);
+        } else if (!std::strcmp(argv[i], "--resume")) {
+            setenv("RTM_B200_RESUME", "1", 1);
+        } else {
+            std::printf("unknown argument %s\n", argv[i]);
+            selfdoc();
+            return 1;
+        }
     }
     rtm_params P;
     if (rtm_read_params("./input", &P) != RTM_OK) {

@@ -4,6 +4,8 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "rtm_types.h"
 
 #define R RTM_RADIUS
@@ -258,10 +260,13 @@ __device__ __forceinline__ float taper_at(int lx, int nwin, int nxl)
     return tp;
 }
 
+// nonfinite: lowest batch index of a shot whose g1 or illumination holds a NaN or infinity
+// (a diverging run: unstable time step or invalid model values); left as set when none.
 __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, int fp64, void *image1,
-                           void *image2s, void *image2m, void *illum_total)
+                           void *image2s, void *image2m, void *illum_total, int *nonfinite)
 {
     const long n = (long)nx * nz;
+    int bad = nshots;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const int iz = (int)(i / nx), ix = (int)(i - (long)iz * nx);
         for (int s = 0; s < nshots; s++) {
@@ -273,6 +278,7 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
             if (fp64) {
                 double g = ((const double *)f.g1)[ip] * (double)tp;
                 double il = ((const double *)f.illum)[ip] * (double)tp;
+                if (!isfinite(g) || !isfinite(il)) bad = min(bad, s);
                 ((double *)image2s)[i] += g / (il + 1.0e-6);
                 ((double *)image1)[i] += g;
                 ((double *)image2m)[i] += g;
@@ -280,6 +286,7 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
             } else {
                 float g = ((const float *)f.g1)[ip] * tp;
                 float il = ((const float *)f.illum)[ip] * tp;
+                if (!isfinite(g) || !isfinite(il)) bad = min(bad, s);
                 float *i2s = (float *)image2s;
                 i2s[i] = i2s[i] + g / (il + 1.0e-6);
                 ((float *)image1)[i] += g;
@@ -288,6 +295,33 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
             }
         }
     }
+    if (bad < nshots) atomicMin(nonfinite, bad);
+}
+
+// Largest |p| of each shot's wavefield (a: source side, b: receiver side) over its padded
+// grid, for the progress snapshots the reference prints every tsnap (rtm_model.cu:271-273,
+// 324-326, 415-417); a NaN or infinity reads as +infinity.  out[s] holds the float's bits
+// (non-negative floats order like their bit patterns) and must start at 0.
+__global__ void k_absmax(const ShotDev *shots, int side, unsigned *out)
+{
+    const ShotDev &sh = shots[blockIdx.y];
+    const float *p = side ? sh.b.p : sh.a.p;
+    const long n = (long)sh.Z * sh.pitch;
+    float m = 0.0f;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const long iz = i / sh.pitch, ix = i - iz * sh.pitch;
+        if (ix >= sh.X) continue;
+        const float v = p[i];
+        m = fmaxf(m, isfinite(v) ? fabsf(v) : INFINITY);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, __float_as_uint(m));
+}
+
+void launch_absmax(const ShotDev *shots, int nshots, int side, unsigned *out, cudaStream_t s)
+{
+    dim3 grid(std::max(1, 148 * 4 / std::max(1, nshots)), nshots);
+    k_absmax<<<grid, 256, 0, s>>>(shots, side, out);
 }
 
 // The other images of a batch (rtm_model.cu:466-487): taper g2, g3, g4 and g3t like g1, then
@@ -453,12 +487,13 @@ void launch_gather_pack(const float *g, void *out, float *scale, int nt, int nre
     k_gather_pack<<<nt, 256, 0, s>>>(g, out, scale, nt, nrec, prec);
 }
 void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void *image1, void *image2s, void *image2m,
-                     void *illum, cudaStream_t s)
+                     void *illum, int *nonfinite, cudaStream_t s)
 {
     long n = (long)nx * nz;
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_finalize<<<blocks, 256, 0, s>>>((const FinalizeShot *)fs, nshots, nx, nz, fp64, image1, image2s, image2m, illum);
+    k_finalize<<<blocks, 256, 0, s>>>((const FinalizeShot *)fs, nshots, nx, nz, fp64, image1, image2s, image2m, illum,
+                                      nonfinite);
 }
 void launch_image_extra(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, int parity, int fp64,
                         float dx, float dz, float dt, cudaStream_t s)

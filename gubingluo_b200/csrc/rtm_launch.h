@@ -19,7 +19,10 @@ void launch_strip_save(const ShotDev *shots, int nshots, int max_strip_len, int 
 void launch_strip_pack(const ShotDev *shots, int nshots, int it0, int ring0, int nsteps, int prec, cudaStream_t s);
 void launch_gather_pack(const float *g, void *out, float *scale, int nt, int nrec, int prec, cudaStream_t s);
 void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void *image1, void *image2s, void *image2m,
-                     void *illum, cudaStream_t s);
+                     void *illum, int *nonfinite, cudaStream_t s);
+// out[s] (zeroed by the caller) <- bits of max |p| over shot s's padded grid, side 0: source
+// wavefield, 1: receiver wavefield; non-finite values count as +infinity.
+void launch_absmax(const ShotDev *shots, int nshots, int side, unsigned *out, cudaStream_t s);
 void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float dt, int gather_prec, cudaStream_t s);
 size_t finalize_shot_size();
 void fill_finalize_shot(void *dst, const void *g1, const void *illum, const void *const *gx, int nx1, int nxi,

@@ -38,6 +38,7 @@ extern "C" {
 #define RTM_ERR_CUDA -2     /* CUDA runtime error (device, launch, memory) */
 #define RTM_ERR_IO -3       /* file missing, unreadable or malformed */
 #define RTM_ERR_NOMEM -4    /* host or device allocation failed */
+#define RTM_ERR_NUMERIC -5  /* a shot's image went NaN or infinite (the wavefield diverged) */
 
 /* ---- storage precisions ---- */
 #define RTM_PREC_FP32 0
@@ -79,6 +80,9 @@ typedef struct rtm_options {
                                 reference's indexing (vx at the pressure cell's flat index on its
                                 (X-1)-wide arrays, receiver vz in the source Poynting term), for
                                 parity with its image3/4/5 outputs */
+    float tsnap;             /* with verbose: print max |p| of every shot every tsnap seconds, as
+                                the reference does (rtm_model.cu:271-273, 324-326, 415-417),
+                                from an on-device reduction; 0 = none */
 } rtm_options;
 
 /* Geometry of one shot for the survey's layout (padded coordinates include the PML). */
@@ -192,6 +196,20 @@ int rtm_session_get_images_extra(rtm_session *ss, float *image3s, float *image4s
                                  float *image3m, float *image4m, float *image5m, float *imagetrue);
 /* Zero the stacked images. */
 int rtm_session_reset_images(rtm_session *ss);
+/* Checkpoints (no counterpart in the reference, which only dumps partial images every 50
+ * shots, rtm_model.cu:490-538, and resumes by hand from a new startshot without them).  Save
+ * writes the stacked images as accumulated (fp32 or fp64; 4 images, 11 with extra_images)
+ * with the count of shots already stacked, atomically (<path>.tmp renamed over <path>).
+ * Load restores them into a session of the same configuration (hash of the survey, the
+ * image options, the shots and their geometry, the models and the coefficients; refused
+ * otherwise) and returns the count; running the remaining shots then gives the images of an
+ * uninterrupted run bit for bit (shots are stacked in shot order whatever the batching). */
+int rtm_session_save_checkpoint(rtm_session *ss, const char *path, int shots_done);
+int rtm_session_load_checkpoint(rtm_session *ss, const char *path, int *shots_done);
+/* Header of a checkpoint file (no device work); any output may be NULL. */
+int rtm_checkpoint_info(const char *path, int *nx, int *nz, int *nshots, int *shots_done,
+                        int *elem_bytes, unsigned long long *config_hash);
+unsigned long long rtm_session_config_hash(rtm_session *ss);
 /* Number of traces of shot k. */
 int rtm_session_nrec(rtm_session *ss, int k);
 /* cudaStream_t of the session (as void*), for event timing by the caller. */
