@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
     L.rtm_checkpoint_info.argtypes = [C.c_char_p] + [C.POINTER(C.c_int)] * 5 + [C.POINTER(C.c_ulonglong)]
     L.rtm_session_config_hash.argtypes = [vp]
     L.rtm_session_config_hash.restype = C.c_ulonglong
+    L.rtm_session_guard_count.argtypes = [vp]
     L.rtm_session_open_geometry.argtypes = [C.POINTER(vp), S, O, C.POINTER(C.c_int), G, C.c_int, vp, vp, vp,
                                             vp, vp]
     L.rtm_session_set_gather_raw.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_float, C.c_int]
@@ -268,6 +269,10 @@ class Session:
 
     def config_hash(self) -> int:
         return lib().rtm_session_config_hash(self.h)
+
+    def guard_count(self) -> int:
+        """Guard bands of the checking mode (RTM_B200_GUARDS=1 when the session opened)."""
+        return lib().rtm_session_guard_count(self.h)
 
     def set_gather_raw(self, k: int, seisobs, dt0: float, mirror: int = 0):
         """Recorded traces [nt0][nx0] of shot k, resampled on the device to [nt][nrec_k]."""

@@ -38,14 +38,36 @@ static size_t elem_size(int prec) { return prec == RTM_PREC_FP32 ? 4 : 2; }
 static int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // Device allocation arena: one cudaMalloc per session, 256-byte aligned sub-allocations.
+// With guards on (RTM_B200_GUARDS=1, a checking mode) every sub-allocation is followed by at
+// least kGuardBytes filled with kGuardByte on the session stream as it is taken, and
+// check_guards() verifies them after setup and after every batch: a kernel that writes past
+// the end of any buffer is reported with the buffer's label.
+static constexpr size_t kGuardBytes = 256;
+static constexpr int kGuardByte = 0xA5;
 struct Arena {
     char *base = nullptr;
     size_t size = 0, used = 0;
+    bool guard = false;
+    cudaStream_t stream = nullptr;
+    const char *label = "";
+    struct Guard {
+        size_t off, len;
+        const char *label;
+        int index;
+    };
+    std::vector<Guard> guards;
+    int taken = 0;
     void *take(size_t n)
     {
         size_t off = (used + 255) & ~(size_t)255;
-        if (off + n > size) return nullptr;
-        used = off + n;
+        const size_t tail = guard ? ((n + 255) & ~(size_t)255) - n + kGuardBytes : 0;
+        if (off + n + tail > size) return nullptr;
+        used = off + n + tail;
+        if (guard) {
+            guards.push_back({off + n, tail, label, taken});
+            if (cudaMemsetAsync(base + off + n, kGuardByte, tail, stream) != cudaSuccess) return nullptr;
+        }
+        taken++;
         return base + off;
     }
 };
@@ -195,6 +217,25 @@ static int check_nonfinite(rtm_session *ss, int k0, int n)
                                          "above the stability limit, or invalid model values)");
     return RTM_OK;
 }
+
+// Guard bands of the checking mode: every byte must still hold kGuardByte.
+static int check_guards(rtm_session *ss)
+{
+    if (!ss->arena.guard) return RTM_OK;
+    CK(cudaStreamSynchronize(ss->stream));
+    std::vector<unsigned char> h;
+    for (const Arena::Guard &g : ss->arena.guards) {
+        h.resize(g.len);
+        CK(cudaMemcpy(h.data(), ss->arena.base + g.off, g.len, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < g.len; i++)
+            if (h[i] != kGuardByte)
+                return fail(RTM_ERR_CUDA, "device write " + std::to_string(i) + " bytes past the end of allocation #" +
+                                              std::to_string(g.index) + " (" + g.label + ")");
+    }
+    return RTM_OK;
+}
+
+int session_guard_count(rtm_session *ss) { return ss ? (int)ss->arena.guards.size() : 0; }
 
 static int check_survey(const rtm_survey &s)
 {
@@ -376,10 +417,18 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     B = std::max(B, 1);
     ss->B = B;
     size_t arena_bytes = fixed + (size_t)B * per_slot;
+    {
+        const char *g = std::getenv("RTM_B200_GUARDS");
+        ss->arena.guard = g && std::atoi(g) != 0;
+    }
+    if (ss->arena.guard)   // an upper bound of the sub-allocations, each with its guard
+        arena_bytes += (size_t)(16 * nshots + 8 * (int)windows.size() + 32 * B + 64) * (kGuardBytes + 256);
     char *base = nullptr;
     CK(cudaMalloc((void **)&base, arena_bytes));
     ss->arena.base = base;
     ss->arena.size = arena_bytes;
+    ss->arena.stream = ss->stream;
+    ss->arena.label = "wavelet and coefficients";
 
     // wavelet and coefficient table
     ss->wavelet = (float *)ss->arena.take((size_t)s.nt * 4);
@@ -393,6 +442,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     CK(cudaMemcpyAsync(ss->coef, ctab, sizeof(ctab), cudaMemcpyHostToDevice, ss->stream));
     CK(cudaStreamSynchronize(ss->stream));
     // stacked images
+    ss->arena.label = "stacked images";
     const size_t isz = (size_t)s.nx * s.nz * (o.accum_fp64 ? 8 : 4);
     ss->img1 = ss->arena.take(isz);
     ss->img2s = ss->arena.take(isz);
@@ -409,6 +459,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         }
 
     // models
+    ss->arena.label = "models";
     std::map<std::pair<int, int>, std::pair<ModelDev, ModelDev>> mcache;
     std::map<std::pair<int, int>, std::pair<float, std::vector<float>>> vp2cache;
     std::map<std::pair<int, int>, std::vector<float>> vb2cache;   // mute 2: v^2 of the migration model
@@ -434,6 +485,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         vp2cache[w.first] = {sqrtf(m), std::move(vp2)};
     }
     // per-shot device state
+    ss->arena.label = "per-shot state (PML, source, mute row, gathers)";
     for (ShotState &sh : ss->shots) {
         auto key = std::make_pair(sh.g.nx1, sh.g.nx2);
         sh.mf = mcache[key].first;
@@ -473,6 +525,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         CK(cudaStreamSynchronize(ss->stream));
     }
     // batch slots
+    ss->arena.label = "batch slots (wavefields, strips, accumulators)";
     ss->slots.resize(B);
     for (Slot &sl : ss->slots) {
         const size_t fb = (size_t)big.pitch * big.Z * 4;
@@ -499,6 +552,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         }
     }
     // descriptor and tile tables, tensor maps, kernel error flag
+    ss->arena.label = "tables and flags";
     ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
     ss->d_tmaps = ss->arena.take((size_t)B * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
     ss->d_err = (int *)ss->arena.take(sizeof(int));
@@ -542,7 +596,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         h = fnv1a(ss->coef_host, sizeof(ss->coef_host), h);
         ss->config_hash = h;
     }
-    return RTM_OK;
+    return check_guards(ss);
 }
 
 // Mute the fp32 gather of shot k in place (reference kernel.cu:96-173) and pack it to the
@@ -899,6 +953,7 @@ static int run_batch(rtm_session *ss, int k0, int n)
     if (rc) return rc;
     CK(cudaStreamSynchronize(ss->stream));
     if ((rc = check_kernel_flag(ss))) return rc;
+    if ((rc = check_guards(ss))) return rc;
     return check_nonfinite(ss, k0, n);
 }
 
@@ -913,7 +968,8 @@ static int model_range(rtm_session *ss, int k0, int n)
     if (rc) return rc;
     if ((rc = batch_forward(ss, br, ss->s.nt, false, true))) return rc;
     CK(cudaStreamSynchronize(ss->stream));
-    return check_kernel_flag(ss);
+    if ((rc = check_kernel_flag(ss))) return rc;
+    return check_guards(ss);
 }
 
 // Run shots [k0, k0+n) (n <= batch size) as one batch.
@@ -988,7 +1044,8 @@ int rtm_session_set_gather_raw(rtm_session *ss, int k, const float *seisobs, int
     rc = finish_gather(ss, sh);
     if (rc) return rc;
     CK(cudaStreamSynchronize(ss->stream));
-    return RTM_OK;
+    if ((rc = interp_check_guards(ss->interp))) return rc;
+    return check_guards(ss);
 }
 
 int rtm_session_set_gather(rtm_session *ss, int k, const float *gather)
@@ -1295,6 +1352,8 @@ int rtm_checkpoint_info(const char *path, int *nx, int *nz, int *nshots, int *sh
 }
 
 unsigned long long rtm_session_config_hash(rtm_session *ss) { return ss ? ss->config_hash : 0ULL; }
+
+int rtm_session_guard_count(rtm_session *ss) { return session_guard_count(ss); }
 
 int rtm_session_reset_images(rtm_session *ss)
 {

@@ -1,6 +1,8 @@
 // rtm_internal.h — declarations shared by the library's translation units.
 #pragma once
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "rtm_b200.h"
 
@@ -56,8 +58,11 @@ struct InterpPlan {
     unsigned *zmax = nullptr;
     int p_k = 0, p_s = 0, p_x = 0, p_t = 0;   // cufftHandle values, valid when `plans`
     bool plans = false;
+    std::vector<std::pair<size_t, size_t>> guards;   // checking mode: (offset, length) bands
     void release();
 };
+// Checking mode (RTM_B200_GUARDS=1): the guard bands after the workspace's buffers are intact.
+int interp_check_guards(const InterpPlan &p);
 // Uploads host_in [nt0][nx0] and writes the interpolated gather to d_out [nt][nx] on stream
 // st; mirror 0 = the reference's negative-frequency indexing, 1 = the Hermitian partner.
 int interp_gather_device(InterpPlan &p, const float *host_in, int nx0, int nt0, float *d_out, int nx, int nt,

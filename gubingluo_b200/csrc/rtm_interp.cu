@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -241,6 +242,18 @@ void InterpPlan::release()
     *this = InterpPlan();
 }
 
+int interp_check_guards(const InterpPlan &p)
+{
+    std::vector<unsigned char> h;
+    for (const auto &g : p.guards) {
+        h.resize(g.second);
+        CKI(cudaMemcpy(h.data(), (char *)p.work + g.first, g.second, cudaMemcpyDeviceToHost));
+        for (unsigned char c : h)
+            if (c != 0xA5) return fail(RTM_ERR_CUDA, "device write past the end of a resampling buffer");
+    }
+    return RTM_OK;
+}
+
 int interp_shape(int nx0, int nt0, int nx, int nt, InterpShape &sh)
 {
     std::memset(&sh, 0, sizeof(sh));
@@ -276,9 +289,15 @@ static int plan_for(InterpPlan &p, const InterpShape &sh, cudaStream_t st)
     p.release();
     p.shape = sh;
     size_t off = 0;
+    const char *gv = std::getenv("RTM_B200_GUARDS");
+    const bool guard = gv && std::atoi(gv) != 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
         off += (bytes + 255) & ~(size_t)255;
+        if (guard) {
+            p.guards.push_back({o + bytes, off + 256 - (o + bytes)});
+            off += 256;
+        }
         return o;
     };
     const size_t o_in = take(sizeof(float) * (size_t)sh.nt0 * sh.nx0);
@@ -294,6 +313,7 @@ static int plan_for(InterpPlan &p, const InterpShape &sh, cudaStream_t st)
     }
     CKI(cudaMalloc(&p.work, off));
     char *b = (char *)p.work;
+    for (const auto &g : p.guards) CKI(cudaMemsetAsync(b + g.first, 0xA5, g.second, st));
     p.d_in = (float *)(b + o_in);
     if (sh.fk) {
         p.d_tmp = (float *)(b + o_tmp);
@@ -405,6 +425,7 @@ extern "C" int rtm_interp_gather(const float *seisobs, int nx0, int nt0, float *
     if (cudaMalloc(&d_out, sizeof(float) * (size_t)nt * nx) != cudaSuccess)
         rc = fail(RTM_ERR_NOMEM, "rtm_interp_gather: device allocation failed");
     if (!rc) rc = interp_gather_device(p, seisobs, nx0, nt0, d_out, nx, nt, dt, dt0, mirror, st, nullptr);
+    if (!rc && cudaStreamSynchronize(st) == cudaSuccess) rc = interp_check_guards(p);
     if (!rc) {
         cudaError_t e = cudaMemcpyAsync(seiscal, d_out, sizeof(float) * (size_t)nt * nx, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -210,6 +210,12 @@ int rtm_session_load_checkpoint(rtm_session *ss, const char *path, int *shots_do
 int rtm_checkpoint_info(const char *path, int *nx, int *nz, int *nshots, int *shots_done,
                         int *elem_bytes, unsigned long long *config_hash);
 unsigned long long rtm_session_config_hash(rtm_session *ss);
+/* Checking mode (no counterpart in the reference): with RTM_B200_GUARDS=1 in the environment
+ * when a session opens, every device sub-allocation is followed by a guard band of a known
+ * byte pattern, verified after setup, after every batch and after every resampling; a write
+ * past the end of a buffer fails the call with RTM_ERR_CUDA naming the buffer.  Returns the
+ * number of guard bands of the session (0 when the mode is off). */
+int rtm_session_guard_count(rtm_session *ss);
 /* Number of traces of shot k. */
 int rtm_session_nrec(rtm_session *ss, int k);
 /* cudaStream_t of the session (as void*), for event timing by the caller. */

@@ -211,3 +211,66 @@ with G.Session(s, G.RunOptions(device=0, verbose=True, tsnap=0.1), [1, 2], v, rh
             p, _, _, _ = G.forward(s, G.RunOptions(device=0), ishot, v, rho, it)
             want = float(np.abs(p).max())
             assert abs(vals[(ishot, round(it * 1e-3, 4))] - want) <= 1e-5 * want
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("opt", ["fp32", "fp16_extra_fp64", "bz8_bz64"])
+def test_guard_bands_hold(rtmlib, monkeypatch, opt):
+    """Checking mode (RTM_B200_GUARDS=1): every device buffer is followed by a guard band,
+    verified after setup and after every batch; the general cases (partial tiles, layouts
+    1-4, receivers below z = 0, PML smoothing) in modes 0 and 1 with packed strips and
+    gathers, fp64 images, the other imaging conditions and other tile heights leave every
+    band intact, and give the same images as without the mode."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from test_gpu_parity import GENERAL, _random_model as rmodel, _survey as gsurvey, cfg_from
+    G = rtmlib
+    kw = dict(device=0, batch=2)
+    if opt == "fp16_extra_fp64":
+        kw.update(strip_precision="fp16", gather_precision="fp16", accum_fp64=True, extra_images=1)
+    if opt == "bz8_bz64":
+        monkeypatch.setenv("RTM_B200_BZ_VEL", "8")
+        monkeypatch.setenv("RTM_B200_BZ_PRES", "64")
+    for ci, c in enumerate(GENERAL):
+        v, rho = rmodel(c["nz"], c["nx"], ci)
+        shots = list(range(1, c["nshot"] + 1))
+        monkeypatch.delenv("RTM_B200_GUARDS", raising=False)
+        plain = G.migrate(cfg_from(G, gsurvey(c, 0)), G.RunOptions(**kw), shots, v, rho)
+        monkeypatch.setenv("RTM_B200_GUARDS", "1")
+        for mode in (0, 1):
+            s = cfg_from(G, gsurvey(c, mode))
+            with G.Session(s, G.RunOptions(**kw), shots, v, rho) as ss:
+                assert ss.guard_count() > 20
+                if mode == 1:
+                    for k in range(len(shots)):
+                        ss.set_gather(k, plain["gathers"][k])
+                ss.run()
+                got = ss.images()
+            if mode == 0:
+                for k in ("image1", "image2s", "illum"):
+                    assert np.array_equal(got[k], plain[k]), (ci, k)
+
+
+@pytest.mark.gpu
+def test_guard_bands_hold_on_recorded_data(rtmlib, monkeypatch, tmp_path):
+    """The same checking mode on the recorded-data path: resampling workspace (F-K and sinc)
+    and the session's buffers."""
+    from gubingluo_b200.synthetic import write_shot_file
+    G = rtmlib
+    monkeypatch.setenv("RTM_B200_GUARDS", "1")
+    rng = np.random.default_rng(12)
+    nz, nx = 37, 141
+    v = (1800 + 200 * rng.random((nz, nx))).astype(np.float32)
+    rho = np.full((nz, nx), 2000.0, np.float32)
+    nt0, dt0, dx0 = 151, float(np.float32(2e-3)), 20.0
+    shots = [(0, 20, 25), (240, 40, 30), (600, 0, 19)]
+    write_shot_file(str(tmp_path / "d.su"), [(sx, off, rng.standard_normal((nt0, n)).astype(np.float32))
+                                             for sx, off, n in shots], nt0, dt0, dx0, big_endian=True)
+    prof, endian = G.scan_shotgather(str(tmp_path / "d.su"))
+    s = G.SurveyConfig(nx=nx, nz=nz, nt=301, dx=10.0, dz=10.0, dt=float(np.float32(1e-3)), npml=17, fdom=20.0,
+                       amp=1.0, alp=0.1, spz0=10.0, layout=3, mode=1, mute=2, ismth=1, direct=1.2)
+    for mirror in (0, 1):
+        out = G.migrate_real(s, G.RunOptions(device=0, batch=2), str(tmp_path / "d.su"), prof, [1, 2, 3], v, rho,
+                             nt0, dt0, dx0, endianflag=endian, mirror=mirror)
+        assert np.isfinite(out["image1"]).all() and np.abs(out["image1"]).max() > 0
+    obs = rng.standard_normal((nt0, 24)).astype(np.float32)
+    G.interp_gather(obs, 47, 301, float(np.float32(1e-3)), dt0)   # standalone entry, odd nt0
