@@ -49,6 +49,13 @@ class Geometry(C.Structure):
                                        "Offset", "sx", "gx", "Nt", "Dt", "Ntrace")] + [("Dx", C.c_float)]
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [("survey", Survey), ("options", Options), ("shots", C.POINTER(C.c_int)), ("nshots", C.c_int),
+                ("vp", C.c_void_p), ("rho", C.c_void_p), ("vp_mig", C.c_void_p), ("rho_mig", C.c_void_p),
+                ("gathers_in", C.POINTER(C.c_void_p)), ("gathers_out", C.POINTER(C.c_void_p)),
+                ("image1", C.c_void_p), ("image2s", C.c_void_p), ("image2m", C.c_void_p), ("illum", C.c_void_p)]
+
+
 class Stats(C.Structure):
     _fields_ = [("seconds_total", C.c_double), ("gcell_updates", C.c_double), ("shots", C.c_int),
                 ("batches", C.c_int), ("kernel_launches", C.c_int)]
@@ -126,6 +133,7 @@ def lib() -> C.CDLL:
                               C.POINTER(Stats)]
     L.rtm_model.restype = None
     L.rtm_real.restype = None
+    L.rtm_batch.argtypes = [C.POINTER(BatchDesc), C.POINTER(Stats)]
     L.rtm_session_save_checkpoint.argtypes = [vp, C.c_char_p, C.c_int]
     L.rtm_session_load_checkpoint.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int)]
     L.rtm_checkpoint_info.argtypes = [C.c_char_p] + [C.POINTER(C.c_int)] * 5 + [C.POINTER(C.c_ulonglong)]

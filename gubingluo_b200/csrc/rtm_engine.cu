@@ -1485,4 +1485,12 @@ int rtm_migrate(const rtm_survey *s, const rtm_options *o, const int *shots, int
     return rc;
 }
 
+int rtm_batch(const rtm_batch_desc *d, rtm_stats *stats)
+{
+    clear_error();
+    if (!d) return fail(RTM_ERR_ARG, "null batch descriptor");
+    return rtm_migrate(&d->survey, &d->options, d->shots, d->nshots, d->vp, d->rho, d->vp_mig, d->rho_mig,
+                       d->gathers_in, d->gathers_out, d->image1, d->image2s, d->image2m, d->illum, stats);
+}
+
 }  // extern "C"

@@ -8,7 +8,12 @@
  *
  * Reference interfaces replaced (gubingluo/gubingluo):
  *   rtm_model          <- extern "C" rtm_model   RTM_GPU_velstr.cpp:23-28, rtm_model.cu:12-17
- *   rtm_migrate / rtm_session_*  new: status-returning, file-free form of the same path
+ *   rtm_real           <- extern "C" rtm_real    rtm_real.cu:17-22 (the definition's argument list)
+ *   rtm_migrate / rtm_batch / rtm_session_*  new: status-returning, file-free form of the same path
+ *   rtm_scan_shotgather<- scanshotgather         RTM_GPU_velstr.cpp:363-454
+ *   rtm_real_geometry  <- per-shot geometry      rtm_real.cu:134-157
+ *   rtm_read_shot_traces <- trace reading        rtm_real.cu:379-394
+ *   rtm_interp_gather  <- Interpseis2d           Interp_function.cpp:245-264
  *   rtm_read_params    <- parameter-file reader  RTM_GPU_velstr.cpp:60-120
  *   rtm_get_constant   <- get_constant           RTM_GPU_velstr.cpp:319-362
  *   rtm_shot_geometry  <- per-layout shot window rtm_model.cu:122-154, 626-650, 1122-1158, 1629-1665
@@ -235,6 +240,22 @@ int rtm_migrate(const rtm_survey *s, const rtm_options *o, const int *shots, int
                 const float *vp, const float *rho, const float *vp_mig, const float *rho_mig,
                 const float *const *gathers_in, float *const *gathers_out, float *image1,
                 float *image2s, float *image2m, float *illum, rtm_stats *stats);
+
+/* The batched form as one descriptor (the same call as rtm_migrate): every shot of `shots`
+ * migrated on one device in batches of options.batch (0: as many as fit), images stacked in
+ * shot order and written to the four outputs (nz*nx each, overwritten; any may be NULL). */
+typedef struct rtm_batch_desc {
+    rtm_survey survey;
+    rtm_options options;
+    const int *shots;                 /* 1-based shot numbers */
+    int nshots;
+    const float *vp, *rho;            /* nz*nx modelling (mode 0) / migration model */
+    const float *vp_mig, *rho_mig;    /* nz*nx backward-pass model, NULL for vp/rho */
+    const float *const *gathers_in;   /* mode 1: nshots pointers to [nt][nrec_k] gathers */
+    float *const *gathers_out;        /* mode 0: nshots pointers (NULL entries skipped), or NULL */
+    float *image1, *image2s, *image2m, *illum;
+} rtm_batch_desc;
+int rtm_batch(const rtm_batch_desc *d, rtm_stats *stats);
 
 /* Forward modelling only: nsteps source-pass steps of shot `ishot` from rest, in the model
  * vp/rho (nz*nx, as for sessions).  Outputs (any may be NULL): p [nzpad][nxpad],

@@ -312,3 +312,39 @@ def test_extra_images_leave_the_main_images_unchanged(rtmlib):
     _, _, b = golden_run(rtmlib, "caseB", rtmlib.RunOptions(extra_images=1))
     for k in ("image1", "image2s", "illum"):
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_rtm_batch_refuses_null_without_gpu(rtmlib):
+    assert rtmlib.lib().rtm_batch(None, None) == rtmlib.RTM_ERR_ARG
+
+
+@pytest.mark.gpu
+def test_rtm_batch_descriptor_equals_session(rtmlib):
+    """rtm_batch (one descriptor: survey, options, shots, models, gathers, images) gives the
+    images and gathers of the session API, bit for bit."""
+    G = rtmlib
+    c = GENERAL[2]
+    v, rho = _random_model(c["nz"], c["nx"], 2)
+    shots = list(range(1, c["nshot"] + 1))
+    s = cfg_from(G, _survey(c, 0))
+    opts = G.RunOptions(batch=2)
+    want = G.migrate(s, opts, shots, v, rho)
+    d = G.BatchDesc()
+    d.survey, d.options = s.c(), opts.c()
+    ids = np.ascontiguousarray(shots, np.int32)
+    d.shots, d.nshots = ids.ctypes.data_as(C.POINTER(C.c_int)), len(shots)
+    v32, r32 = np.ascontiguousarray(v, np.float32), np.ascontiguousarray(rho, np.float32)
+    d.vp, d.rho = v32.ctypes.data, r32.ctypes.data
+    gouts = [np.zeros_like(g) for g in want["gathers"]]
+    gp = (C.c_void_p * len(shots))(*[g.ctypes.data for g in gouts])
+    d.gathers_out = C.cast(gp, C.POINTER(C.c_void_p))
+    imgs = {k: np.zeros((c["nz"], c["nx"]), np.float32) for k in ("image1", "image2s", "image2m", "illum")}
+    for k, a in imgs.items():
+        setattr(d, k, a.ctypes.data)
+    st = G.Stats()
+    assert G.lib().rtm_batch(C.byref(d), C.byref(st)) == 0, G.lib().rtm_last_error()
+    assert st.shots == len(shots) and st.batches == 2
+    for k in ("image1", "image2s", "illum"):
+        assert np.array_equal(imgs[k], want[k]), k
+    for a, b in zip(gouts, want["gathers"]):
+        assert np.array_equal(a, b)
