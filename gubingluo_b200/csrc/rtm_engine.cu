@@ -663,6 +663,8 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.n = n;
     br.hd.assign(n, ShotDev{});
     std::vector<TileRef> tiles, tiles_p, tiles_r, tiles_pr;
+    const char *fast_env = std::getenv("RTM_B200_FAST_TILES");   // 0: every tile on the general form
+    const bool fast = !(fast_env && *fast_env && std::atoi(fast_env) == 0);
     std::vector<unsigned char> maps((size_t)n * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
     br.maxrec = 0;
     br.max_strip_len = 0;
@@ -712,7 +714,15 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
                 for (int x0 = xa; x0 < xb; x0 += RTM_BX) v.push_back({j, x0, z0});
         };
         add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
-        add_tiles(tiles_p, ss->bz_pres, 0, sh.X, 0, sh.Z);
+        // pressure tiles: interior tiles (no PML, source or receiver cell) go to their own list
+        for (int z0 = 0; z0 < sh.Z; z0 += ss->bz_pres)
+            for (int x0 = 0; x0 < sh.X; x0 += RTM_BX) {
+                const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
+                const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
+                const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
+                const bool rec = sh.g.rz >= z0 && sh.g.rz < z1 && x0 < sh.g.rx0 + sh.g.nrec && sh.g.rx0 < x1;
+                tiles_p.push_back({j, x0, z0, (fast && inside && !src && !rec) ? 1 : 0});
+            }
         add_tiles(tiles_r, ss->bz_vel, xr0, xr1, zr0, zr1);
         add_tiles(tiles_pr, ss->bz_pres, xr0, xr1, zr0, zr1);
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
@@ -754,6 +764,15 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     ss->last_batch_shots.clear();
     for (int j = 0; j < n; j++) ss->last_batch_shots.push_back(k0 + j);
     return RTM_OK;
+}
+
+// Full-grid pressure update of one step (interior tiles are flagged in the tile list).
+static void launch_pres_tiles(rtm_session *ss, BatchRun &br, int mode, int record)
+{
+    StepArgs &a = br.a;
+    a.tiles = ss->d_tiles_p;
+    launch_pres(mode, ss->bz_pres, a, br.ntiles_p, record, ss->stream);
+    ss->launches++;
 }
 
 // Progress lines of the reference (rtm_model.cu:324-326, 415-417), one per shot of the batch
@@ -809,10 +828,9 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
         launch_vel(mode, ss->bz_vel, a, br.ntiles, st);
         timing_end(ss, e);
         timing_begin(ss, "pres_fwd", it, &e);
-        a.tiles = ss->d_tiles_p;
-        launch_pres(mode, ss->bz_pres, a, br.ntiles_p, record ? 1 : 0, st);
+        launch_pres_tiles(ss, br, mode, record ? 1 : 0);
         timing_end(ss, e);
-        ss->launches += 2;
+        ss->launches += 1;
         if (save) {
             launch_strip_save(ss->d_shots, br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
             ss->launches++;
@@ -903,10 +921,9 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         launch_vel(RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles, st);
         timing_end(ss, e);
         timing_begin(ss, "pres_recv", it, &e);
-        a.tiles = ss->d_tiles_p;
-        launch_pres(RTM_WAVE_RECEIVER, ss->bz_pres, a, br.ntiles_p, 0, st);
+        launch_pres_tiles(ss, br, RTM_WAVE_RECEIVER, 0);
         timing_end(ss, e);
-        ss->launches += 4;
+        ss->launches += 3;
         if (o.extra_images) {
             launch_image_extra(ss->d_shots, n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz, s.dt,
                                st);

@@ -133,6 +133,19 @@ __device__ __forceinline__ int strip_row_tb(int z, int npml, int first, int nxi)
     return -1;
 }
 
+// Interior pressure update p - (dxs + dzs) and the cross-correlation terms, shared by the
+// general and the interior-tile forms of the pressure kernel so that both give the same
+// bits: the sum and the difference are rounded separately (no fused multiply-add), as the
+// reference's host-order arithmetic and the oracle have them.
+__device__ __forceinline__ float p_interior(float p0, float dxs, float dzs) { return __fsub_rn(p0, __fadd_rn(dxs, dzs)); }
+template <typename ACC>
+__device__ __forceinline__ void image_cell(ACC *__restrict__ g1p, ACC *__restrict__ ilp, unsigned id, ACC og1, ACC oil,
+                                           float ps, float pn)
+{
+    g1p[id] = og1 + (ACC)ps * (ACC)pn;
+    ilp[id] = oil + (ACC)ps * (ACC)ps;
+}
+
 // Damped or undamped update f' = (c1*f - d)*ic2; outside the PML c1 = ic2 = 1, which makes
 // this exactly f - d.
 __device__ __forceinline__ float damp(float f, float d, float c1, float ic2) { return (c1 * f - d) * ic2; }
@@ -280,7 +293,7 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
     bool wr = false;
     if (upd) {
         const float dxs = ddx * kk, dzs = ddz * kk;
-        if (zin && !cc.xb) pn = p0 - (dxs + dzs);   // interior, kernel.cu:501-541
+        if (zin && !cc.xb) pn = p_interior(p0, dxs, dzs);   // interior, kernel.cu:501-541
         else {                                      // split-field PML, kernel.cu:714-1185
             const float s1n = damp(s1o, dxs, cc.c1x, cc.ic2x);
             const float s2n = damp(s2o, dzs, c1z, ic2z);
@@ -304,10 +317,7 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
             wr = true;
         }
         if (wr) pp[id] = pn;
-        if (zin && cc.xin) {   // kernel.cu:1401-1416 (accumulators on the padded grid)
-            g1p[id] = og1 + (ACC)ps * (ACC)pn;
-            ilp[id] = oil + (ACC)ps * (ACC)ps;
-        }
+        if (zin && cc.xin) image_cell<ACC>(g1p, ilp, id, og1, oil, ps, pn);   // kernel.cu:1401-1416
     }
 }
 
@@ -457,9 +467,20 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 // Register budgets (measured): 6 blocks per SM (80 registers, no spills) for the forward
 // pass and the reconstruction, 5 for the receiver pass (4 with fp64 accumulators, which
 // would spill at 5).  A bound of 5 on the forward pass was slower than no bound, 6 faster.
+//
+// Interior tiles (TileRef.interior, set by the host for tiles whose every column lies in
+// [npml, X-npml) and every row in [npml, Z-npml), with no source cell and no receiver) take
+// a second body in the same kernel, chosen per block: the interior update alone, with no
+// PML, source or receiver tests and no split-field loads, in the arithmetic of the general
+// body's interior branch.  RTM_INTERIOR_MODES selects the modes that use it (bit 0: forward,
+// bit 2: receiver).
+#ifndef RTM_INTERIOR_MODES
+#define RTM_INTERIOR_MODES 5
+#endif
 template <int BZ, int MODE, typename ACC>
 __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6) k_pres(const StepArgs a, int record)
 {
+    static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QN - 1;   // vz rows z0-10 .. z0+BZ+QN-12, columns x0 .. x0+BX-1
     extern __shared__ __align__(128) float sm[];
@@ -545,6 +566,57 @@ __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6
     float q[QN];                          // q[k] = vz[z-10+k][x] at the current row z
 #pragma unroll
     for (int j = 0; j < QN; j++) q[j] = colz[j * BX];
+
+    if ((RTM_INTERIOR_MODES >> MODE) & 1 && MODE != 3 && t.interior) {
+#pragma unroll 1
+        for (int z = z0; z < z0 + BZ; z += U) {
+            float nkk[U], np0[U], nps[U];
+            ACC ng1[U], nil[U];
+            const bool more = z + 2 * U <= z0 + BZ;
+            if (more) {
+                const unsigned g0 = (unsigned)(z + U) * pitch + x;
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const unsigned id = g0 + u * pitch;
+                    nkk[u] = __ldg(&kappa[id]);
+                    np0[u] = pp[id];
+                    if (MODE == 2) {
+                        nps[u] = __ldg(&psp[id]);
+                        ng1[u] = g1p[id];
+                        nil[u] = ilp[id];
+                    }
+                }
+            }
+            const unsigned id0 = (unsigned)z * pitch + x;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const float *rw = &colx[(z + u - z0) * WW];
+                const float dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i - 1]; },
+                                         [&](int i) { return rw[-i]; });
+                const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                                         [&](int i) { return q[u + 10 - i]; });
+                const float ddx = dx * a.dtx, ddz = dz * a.dtz;
+                const float pn = p_interior(cp0[u], ddx * ckk[u], ddz * ckk[u]);
+                const unsigned id = id0 + u * pitch;
+                pp[id] = pn;
+                if (MODE == 2) image_cell<ACC>(g1p, ilp, id, cg1[u], cil[u], cps[u], pn);
+            }
+            advance<U, BX>(q, colz, z + U - z0, z + U < z0 + BZ);
+            if (more) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    ckk[u] = nkk[u];
+                    cp0[u] = np0[u];
+                    if (MODE == 2) {
+                        cps[u] = nps[u];
+                        cg1[u] = ng1[u];
+                        cil[u] = nil[u];
+                    }
+                }
+            }
+        }
+        return;
+    }
 
     // one-row path for the rows after the last whole group: local orders from the table
     auto one_row = [&](int z) {

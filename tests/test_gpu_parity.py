@@ -348,3 +348,26 @@ def test_rtm_batch_descriptor_equals_session(rtmlib):
         assert np.array_equal(imgs[k], want[k]), k
     for a, b in zip(gouts, want["gathers"]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp64", [False, True])
+def test_interior_tile_form_is_bitwise_identical(rtmlib, monkeypatch, fp64):
+    """The pressure kernel's interior-tile form (tiles with no PML, source or receiver cell)
+    gives the same bits as the general form on every tile (RTM_B200_FAST_TILES=0): gathers
+    and images of the general cases, fp32 and fp64 accumulators, with the other imaging
+    conditions."""
+    G = rtmlib
+    for ci, c in enumerate(GENERAL):
+        v, rho = _random_model(c["nz"], c["nx"], ci)
+        shots = list(range(1, c["nshot"] + 1))
+        s = cfg_from(G, _survey(c, 0))
+        opts = G.RunOptions(accum_fp64=fp64, extra_images=1)
+        monkeypatch.setenv("RTM_B200_FAST_TILES", "0")
+        want = G.migrate(s, opts, shots, v, rho)
+        monkeypatch.delenv("RTM_B200_FAST_TILES")
+        got = G.migrate(s, opts, shots, v, rho)
+        for k in ("image1", "image2s", "illum", "image3s", "image4s", "image5s", "imagetrue"):
+            assert np.array_equal(got[k], want[k]), (ci, k)
+        for a, b in zip(got["gathers"], want["gathers"]):
+            assert np.array_equal(a, b), ci
