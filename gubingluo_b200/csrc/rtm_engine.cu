@@ -709,9 +709,15 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10)
         const int xr0 = (s.npml - RTM_RADIUS) & ~3, xr1 = sh.X - s.npml + RTM_RADIUS;
         const int zr0 = s.npml - RTM_RADIUS, zr1 = sh.Z - s.npml + RTM_RADIUS;
+        // velocity tiles: interior when every column lies in [npml, X-npml-1) and every row in
+        // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies
         auto add_tiles = [&](std::vector<TileRef> &v, int bz, int xa, int xb, int za, int zb) {
             for (int z0 = za; z0 < zb; z0 += bz)
-                for (int x0 = xa; x0 < xb; x0 += RTM_BX) v.push_back({j, x0, z0});
+                for (int x0 = xa; x0 < xb; x0 += RTM_BX) {
+                    const bool inside = x0 >= s.npml && x0 + RTM_BX <= sh.X - s.npml - 1 && z0 >= s.npml &&
+                                        z0 + bz <= sh.Z - s.npml - 1;
+                    v.push_back({j, x0, z0, (fast && inside) ? 1 : 0});
+                }
         };
         add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
         // pressure tiles: interior tiles (no PML, source or receiver cell) go to their own list
@@ -724,7 +730,15 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
                 tiles_p.push_back({j, x0, z0, (fast && inside && !src && !rec) ? 1 : 0});
             }
         add_tiles(tiles_r, ss->bz_vel, xr0, xr1, zr0, zr1);
-        add_tiles(tiles_pr, ss->bz_pres, xr0, xr1, zr0, zr1);
+        // reconstruction pressure tiles: interior when inside the pressure interior with no
+        // source cell
+        for (int z0 = zr0; z0 < zr1; z0 += ss->bz_pres)
+            for (int x0 = xr0; x0 < xr1; x0 += RTM_BX) {
+                const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
+                const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
+                const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
+                tiles_pr.push_back({j, x0, z0, (fast && inside && !src) ? 1 : 0});
+            }
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
         br.max_strip_len = std::max(br.max_strip_len, sh.strip_len);
         size_t fb = (size_t)sh.pitch * sh.Z * 4;

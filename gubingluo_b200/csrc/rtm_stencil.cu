@@ -147,8 +147,16 @@ __device__ __forceinline__ void image_cell(ACC *__restrict__ g1p, ACC *__restric
 }
 
 // Damped or undamped update f' = (c1*f - d)*ic2; outside the PML c1 = ic2 = 1, which makes
-// this exactly f - d.
-__device__ __forceinline__ float damp(float f, float d, float c1, float ic2) { return (c1 * f - d) * ic2; }
+// this exactly f - d.  Each operation is rounded on its own (no fused multiply-add), so the
+// interior-tile bodies below, which write f - d, give the same bits.
+__device__ __forceinline__ float damp(float f, float d, float c1, float ic2)
+{
+    return __fmul_rn(__fsub_rn(__fmul_rn(c1, f), d), ic2);
+}
+// Velocity increment (dt/h) * D * (1/rho), and the reconstruction updates, rounded the same
+// way in every body.
+__device__ __forceinline__ float vel_inc(float d, float dth, float ir) { return __fmul_rn(__fmul_rn(d, dth), ir); }
+__device__ __forceinline__ float p_recon(float p0, float dxs, float dzs) { return __fadd_rn(p0, __fadd_rn(dxs, dzs)); }
 
 // Advance the z window by N rows: q[k] <- q[k+N], then the N new entries from the staged
 // column s (entry k of the advanced window is staged row dz + k, dz = rows advanced since
@@ -210,13 +218,13 @@ __device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, c
         // kernel.cu:318-388 (+=) on the interior; strips of step it+1 elsewhere
         const bool zin = (z >= npml && z < Z - npml);
         const bool zinv = (z >= npml && z <= Z - npml - 2);
-        if (zin && cc.rvx) vxp[id] = ov + dx * dtx * ir;
+        if (zin && cc.rvx) vxp[id] = __fadd_rn(ov, vel_inc(dx, dtx, ir));
         else if (zin && cc.svx >= 0) {   // read_d_vxpml, kernel.cu:1294-1320
             const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 0] : 1.0f;
             vxp[id] = load_strip(S.strips, (size_t)(a.it + 1) * k.strip_len + cc.svx + (size_t)(z - npml) * R,
                                  a.strip_prec, sc);
         }
-        if (zinv && cc.rvz) vzp[id] = ow + dz * dtz * ir;
+        if (zinv && cc.rvz) vzp[id] = __fadd_rn(ow, vel_inc(dz, dtz, ir));
         else if (cc.svz >= 0 && z < Z - 1) {   // read_d_vzpml, kernel.cu:1321-1347
             const int srow = strip_row_tb(z, npml, Z - npml - 1, k.nxi);
             if (srow >= 0) {
@@ -229,9 +237,9 @@ __device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, c
         return;
     }
     // kernel.cu:430-500 (interior) and :542-713 (PML): f' = (c1*f - d)*ic2
-    const float nvx = damp(ov, dx * dtx * ir, cc.c1vx, cc.ic2vx);
+    const float nvx = damp(ov, vel_inc(dx, dtx, ir), cc.c1vx, cc.ic2vx);
     if (cc.hvx) vxp[id] = nvx;
-    const float nvz = damp(ow, dz * dtz * ir, c1z, ic2z);
+    const float nvz = damp(ow, vel_inc(dz, dtz, ir), c1z, ic2z);
     if (z < Z - 1) vzp[id] = nvz;
 }
 
@@ -261,7 +269,7 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
         float pn = p0;
         bool wr = false;
         if (zin && cc.xin) {
-            pn = p0 + (ddx * kk + ddz * kk);
+            pn = p_recon(p0, ddx * kk, ddz * kk);
             wr = true;
         } else {
             const size_t pstrip = 2 * (size_t)R * k.nzi + 2 * (size_t)R * k.nxi;
@@ -332,6 +340,7 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
 template <int BZ, int MODE>
 __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 {
+    static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int WH = BZ + QN - 1;   // staged rows z0-9 .. z0+BZ+QN-11
     extern __shared__ __align__(128) float sw[];
     __shared__ __align__(8) unsigned long long s_bar;
@@ -398,6 +407,45 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
     float q[QN];                        // q[k] = p[z-9+k][x] at the current row z
 #pragma unroll
     for (int j = 0; j < QN; j++) q[j] = col[j * WW];
+
+    // interior tiles (TileRef.interior: every column in [npml, X-npml-1), every row in
+    // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies): the update
+    // alone, in the arithmetic of the general body
+    if (t.interior) {
+#pragma unroll 1
+        for (int z = z0; z < z0 + BZ; z += U) {
+            float nir[U], nov[U], now[U];
+            const bool more = z + 2 * U <= z0 + BZ;
+            if (more) load_group(z + U, nir, nov, now);
+            const unsigned id0 = (unsigned)z * pitch + x;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const float *rw = &col[(z + u - z0 + 9) * WW];
+                const float dx = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i]; },
+                                         [&](int i) { return rw[1 - i]; });
+                const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                                         [&](int i) { return q[u + 10 - i]; });
+                const unsigned id = id0 + u * pitch;
+                if (MODE == 3) {
+                    vxp[id] = __fadd_rn(cov[u], vel_inc(dx, a.dtx, cir[u]));
+                    vzp[id] = __fadd_rn(cow[u], vel_inc(dz, a.dtz, cir[u]));
+                } else {
+                    vxp[id] = __fsub_rn(cov[u], vel_inc(dx, a.dtx, cir[u]));
+                    vzp[id] = __fsub_rn(cow[u], vel_inc(dz, a.dtz, cir[u]));
+                }
+            }
+            advance<U, WW>(q, col, z + U - z0, z + U < z0 + BZ);
+            if (more) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    cir[u] = nir[u];
+                    cov[u] = nov[u];
+                    cow[u] = now[u];
+                }
+            }
+        }
+        return;
+    }
 
     // one-row path for the rows after the last whole group: local orders from the table
     auto one_row = [&](int z) {
@@ -472,11 +520,7 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 // [npml, X-npml) and every row in [npml, Z-npml), with no source cell and no receiver) take
 // a second body in the same kernel, chosen per block: the interior update alone, with no
 // PML, source or receiver tests and no split-field loads, in the arithmetic of the general
-// body's interior branch.  RTM_INTERIOR_MODES selects the modes that use it (bit 0: forward,
-// bit 2: receiver).
-#ifndef RTM_INTERIOR_MODES
-#define RTM_INTERIOR_MODES 5
-#endif
+// body's interior branch (for the reconstruction: tiles of the interior with no source cell).
 template <int BZ, int MODE, typename ACC>
 __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6) k_pres(const StepArgs a, int record)
 {
@@ -567,7 +611,7 @@ __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6
 #pragma unroll
     for (int j = 0; j < QN; j++) q[j] = colz[j * BX];
 
-    if ((RTM_INTERIOR_MODES >> MODE) & 1 && MODE != 3 && t.interior) {
+    if (t.interior) {
 #pragma unroll 1
         for (int z = z0; z < z0 + BZ; z += U) {
             float nkk[U], np0[U], nps[U];
@@ -596,7 +640,8 @@ __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6
                 const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
                                          [&](int i) { return q[u + 10 - i]; });
                 const float ddx = dx * a.dtx, ddz = dz * a.dtz;
-                const float pn = p_interior(cp0[u], ddx * ckk[u], ddz * ckk[u]);
+                const float pn = MODE == 3 ? p_recon(cp0[u], ddx * ckk[u], ddz * ckk[u])
+                                           : p_interior(cp0[u], ddx * ckk[u], ddz * ckk[u]);
                 const unsigned id = id0 + u * pitch;
                 pp[id] = pn;
                 if (MODE == 2) image_cell<ACC>(g1p, ilp, id, cg1[u], cil[u], cps[u], pn);

@@ -98,7 +98,8 @@ enum RtmTmap { RTM_TMAP_A_P = 0, RTM_TMAP_A_VX, RTM_TMAP_A_VZ, RTM_TMAP_B_P, RTM
 struct TileRef {
     int shot;
     int x0, z0;
-    int interior;   // pressure tiles: 1 when the tile holds no PML, source or receiver cell
+    int interior;   // 1: the tile lies in the interior and holds no source, receiver or strip
+                    // cell, so the kernels take their branch-free body (set by the host)
 };
 
 // Kernel-wide constants of one launch.
