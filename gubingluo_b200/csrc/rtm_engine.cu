@@ -693,7 +693,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         d.vp2_b = sh.mb.vp2;
         // tensor maps of the fields the stencil kernels stage, for this shot's row pitch
         {
-            const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA, ph = ss->bz_pres + RTM_STAGE_ZEXTRA;
+            const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA_VEL, ph = ss->bz_pres + RTM_STAGE_ZEXTRA_PRES;
             struct { float *f; int w, h; } m[RTM_TMAP_COUNT] = {
                 {sl.a.p, RTM_STAGE_W, vh}, {sl.a.vx, RTM_STAGE_W, ss->bz_pres}, {sl.a.vz, RTM_BX, ph},
                 {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph}};

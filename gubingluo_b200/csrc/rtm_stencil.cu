@@ -34,9 +34,15 @@ namespace {
 constexpr int BX = RTM_BX;          // threads (= columns) per block
 constexpr int WW = RTM_STAGE_W;     // staged width: columns x0-12 .. x0+BX+11 (16-byte aligned)
 constexpr int R = RTM_RADIUS;
-constexpr int U = RTM_GROUP;        // rows per unrolled group
-constexpr int QN = 2 * R + U - 1;   // z window: the 2R taps of U consecutive rows
-static_assert(QN - 1 == RTM_STAGE_ZEXTRA, "staged rows beyond a tile must cover the z window");
+// Rows per unrolled group (measured: 2 rows make the forward and receiver velocity kernels
+// 2-5% faster than 4, and the reconstruction 24% slower; the pressure kernels are fastest
+// at 4).  The z window of U rows is 2R+U-1 deep; the velocity kernels stage the rows of the
+// deeper window, so every mode reads one box height.
+constexpr int UV = RTM_GROUP_VEL, UVR = RTM_GROUP_VEL_RECON, UP = RTM_GROUP_PRES;
+constexpr int QNV_MAX = 2 * R + (UV > UVR ? UV : UVR) - 1;
+constexpr int QNP = 2 * R + UP - 1;
+static_assert(QNV_MAX - 1 == RTM_STAGE_ZEXTRA_VEL && QNP - 1 == RTM_STAGE_ZEXTRA_PRES,
+              "staged rows beyond a tile must cover the z window");
 static_assert(WW == BX + 24, "staged width");
 constexpr long kWaitLimit = 1L << 22;   // polls of a tile's TMA barrier before giving up
 
@@ -161,7 +167,7 @@ __device__ __forceinline__ float p_recon(float p0, float dxs, float dzs) { retur
 // Advance the z window by N rows: q[k] <- q[k+N], then the N new entries from the staged
 // column s (entry k of the advanced window is staged row dz + k, dz = rows advanced since
 // the tile's first row).  `more` is false after the tile's last row: nothing is read then.
-template <int N, int STRIDE>
+template <int N, int STRIDE, int QN>
 __device__ __forceinline__ void advance(float (&q)[QN], const float *s, int dz, bool more)
 {
 #pragma unroll
@@ -340,8 +346,9 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
 template <int BZ, int MODE>
 __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 {
+    constexpr int U = MODE == 3 ? UVR : UV, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
-    constexpr int WH = BZ + QN - 1;   // staged rows z0-9 .. z0+BZ+QN-11
+    constexpr int WH = BZ + QNV_MAX - 1;   // staged rows z0-9 .. z0+BZ+QNV_MAX-11 (the box height)
     extern __shared__ __align__(128) float sw[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
@@ -524,6 +531,7 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? 5 : 6) k_vel(const StepArgs a)
 template <int BZ, int MODE, typename ACC>
 __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6) k_pres(const StepArgs a, int record)
 {
+    constexpr int U = UP, QN = QNP;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QN - 1;   // vz rows z0-10 .. z0+BZ+QN-12, columns x0 .. x0+BX-1
@@ -744,9 +752,9 @@ __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6
 // =====================================================================================
 // Host launchers.
 template <int BZ>
-static size_t vel_smem() { return (size_t)(BZ + QN - 1) * WW * sizeof(float); }
+static size_t vel_smem() { return (size_t)(BZ + QNV_MAX - 1) * WW * sizeof(float); }
 template <int BZ>
-static size_t pres_smem() { return ((size_t)BZ * WW + (size_t)(BZ + QN - 1) * BX) * sizeof(float); }
+static size_t pres_smem() { return ((size_t)BZ * WW + (size_t)(BZ + QNP - 1) * BX) * sizeof(float); }
 
 template <int BZ, int MODE>
 static void vel_launch(const StepArgs &a, int ntiles, cudaStream_t s)
