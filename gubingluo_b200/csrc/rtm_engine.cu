@@ -128,7 +128,9 @@ struct rtm_session {
     TileRef *d_tiles_p = nullptr;    // tiles of the pressure kernels (whole padded grid)
     TileRef *d_tiles_r = nullptr;    // velocity tiles of the reconstruction region (interior + strips)
     TileRef *d_tiles_pr = nullptr;   // pressure tiles of the reconstruction region
-    int bz_vel = 16, bz_pres = 16;   // rows per tile of the two stencil kernels
+    // rows per tile (measured): 32 for the forward and receiver velocity kernels, 16 for the
+    // velocity reconstruction and the pressure kernels
+    int bz_vel = 32, bz_vel_recon = 16, bz_pres = 16;
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -408,10 +410,12 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     {
         const char *e = std::getenv("RTM_B200_BZ_VEL");
         if (e && *e) ss->bz_vel = std::atoi(e);
+        e = std::getenv("RTM_B200_BZ_VEL_RECON");
+        if (e && *e) ss->bz_vel_recon = std::atoi(e);
         e = std::getenv("RTM_B200_BZ_PRES");
         if (e && *e) ss->bz_pres = std::atoi(e);
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
-        for (int bz : {ss->bz_vel, ss->bz_pres})
+        for (int bz : {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres})
             if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
     }
     B = std::max(B, 1);
@@ -567,7 +571,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         }
     }
     CK(cudaMemsetAsync(ss->d_err, 0, sizeof(int), ss->stream));
-    const int bz_min = std::min(ss->bz_vel, ss->bz_pres);
+    const int bz_min = std::min(std::min(ss->bz_vel, ss->bz_vel_recon), ss->bz_pres);
     int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + bz_min - 1) / bz_min);
     ss->max_tiles = tiles_per_shot * B;
     ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
@@ -694,9 +698,11 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         // tensor maps of the fields the stencil kernels stage, for this shot's row pitch
         {
             const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA_VEL, ph = ss->bz_pres + RTM_STAGE_ZEXTRA_PRES;
+            const int vhr = ss->bz_vel_recon + RTM_STAGE_ZEXTRA_VEL;
             struct { float *f; int w, h; } m[RTM_TMAP_COUNT] = {
                 {sl.a.p, RTM_STAGE_W, vh}, {sl.a.vx, RTM_STAGE_W, ss->bz_pres}, {sl.a.vz, RTM_BX, ph},
-                {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph}};
+                {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph},
+                {sl.a.p, RTM_STAGE_W, vhr}};
             for (int t = 0; t < RTM_TMAP_COUNT; t++) {
                 CUtensorMap cm;
                 int rc = encode_field_map(&cm, m[t].f, sh.pitch, sh.Z, m[t].w, m[t].h);
@@ -729,7 +735,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
                 const bool rec = sh.g.rz >= z0 && sh.g.rz < z1 && x0 < sh.g.rx0 + sh.g.nrec && sh.g.rx0 < x1;
                 tiles_p.push_back({j, x0, z0, (fast && inside && !src && !rec) ? 1 : 0});
             }
-        add_tiles(tiles_r, ss->bz_vel, xr0, xr1, zr0, zr1);
+        add_tiles(tiles_r, ss->bz_vel_recon, xr0, xr1, zr0, zr1);
         // reconstruction pressure tiles: interior when inside the pressure interior with no
         // source cell
         for (int z0 = zr0; z0 < zr1; z0 += ss->bz_pres)
@@ -924,7 +930,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         // (which reads the reconstructed pressure of the same step)
         timing_begin(ss, "vel_recon", it, &e);
         a.tiles = ss->d_tiles_r;
-        launch_vel(RTM_WAVE_RECON, ss->bz_vel, a, br.ntiles_r, st);
+        launch_vel(RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r, st);
         timing_end(ss, e);
         timing_begin(ss, "pres_recon", it, &e);
         a.tiles = ss->d_tiles_pr;

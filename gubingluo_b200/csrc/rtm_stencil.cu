@@ -364,7 +364,8 @@ __global__ void __launch_bounds__(BX, MODE == 3 && BZ == 8 ? 5 : 6) k_vel(const 
     if (threadIdx.x == 0) {   // p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139
         mbar_init(&s_bar);
         mbar_expect(&s_bar, WH * WW * sizeof(float));
-        tma_box(sw, tmap_of(S, MODE == 2 ? RTM_TMAP_B_P : RTM_TMAP_A_P), x0 - 12, z0 - 9, &s_bar);
+        tma_box(sw, tmap_of(S, MODE == 2 ? RTM_TMAP_B_P : (MODE == 3 ? RTM_TMAP_A_P_RECON : RTM_TMAP_A_P)), x0 - 12,
+                z0 - 9, &s_bar);
     }
     for (int i = threadIdx.x; i < 100; i += BX) s_tab[i] = a.coef[i];
     for (int i = threadIdx.x; i < BZ; i += BX) {

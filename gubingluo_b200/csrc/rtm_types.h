@@ -103,8 +103,9 @@ struct ShotDev {
 // stencil kernel loads (velocity: p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139;
 // pressure: vx rows z0 .. z0+BZ-1 with the same columns, vz rows z0-10 .. z0+BZ+11,
 // columns x0 .. x0+127).
+// (A_P_RECON: the source pressure again, in the boxes of the reconstruction's own tile height)
 enum RtmTmap { RTM_TMAP_A_P = 0, RTM_TMAP_A_VX, RTM_TMAP_A_VZ, RTM_TMAP_B_P, RTM_TMAP_B_VX, RTM_TMAP_B_VZ,
-               RTM_TMAP_COUNT };
+               RTM_TMAP_A_P_RECON, RTM_TMAP_COUNT };
 #define RTM_TMAP_BYTES 128
 
 // One block's work: the tile of `shot` whose top-left cell is (x0, z0).  x0 is a multiple of
