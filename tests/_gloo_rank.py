@@ -5,7 +5,12 @@ restatement; the GPU library is not needed here), then the ranks sum their stack
 over gloo, exactly as the multi-GPU run sums its device images over NCCL.  Rank 0 writes
 the reduced images to the output file.
 
-    python tests/_gloo_rank.py <rank> <world> <port> <out.npz>
+    python tests/_gloo_rank.py <rank> <world> <port> <out.npz> [fail]
+
+With `fail`, the last rank stops after migrating its shots, before the reduction, as a
+rank whose process died would; the other ranks' reduction must then end with an error (the
+peer's closed connection, at the latest the process group's timeout), not wait for ever.
+They exit with status 4 after writing the error to <out.npz>.failed.
 """
 import os
 import sys
@@ -30,6 +35,7 @@ def survey():
 
 def main():
     rank, world, port, out = int(sys.argv[1]), int(sys.argv[2]), sys.argv[3], sys.argv[4]
+    fail = len(sys.argv) > 5 and sys.argv[5] == "fail"
     import torch
     import torch.distributed as dist
     from gubingluo_b200 import SurveyConfig, shards
@@ -37,7 +43,7 @@ def main():
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = port
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=20 if fail else 60))
     s, shots, vp, rho = survey()
     cfg = SurveyConfig(**{k: s[k] for k in SurveyConfig.__dataclass_fields__})
     parts = shards.lpt_shards(shards.shot_costs(cfg, shots), world)
@@ -48,7 +54,14 @@ def main():
     else:
         imgs = [np.zeros((s["nz"], s["nx"])) for _ in range(3)]
     ts = [torch.from_numpy(np.ascontiguousarray(a, np.float64)) for a in imgs]
-    shards.allreduce_images(ts, dist)
+    if fail and rank == world - 1:
+        os._exit(3)   # ends without leaving the process group, like a crashed rank
+    try:
+        shards.allreduce_images(ts, dist)
+    except Exception as e:   # the peer is gone: report and stop
+        with open(out + ".failed", "w") as f:
+            f.write(f"rank {rank}: {type(e).__name__}: {e}")
+        os._exit(4)
     if rank == 0:
         np.savez(out, image1=ts[0].numpy(), image2s=ts[1].numpy(), illum=ts[2].numpy(),
                  parts=np.array([len(p) for p in parts]))

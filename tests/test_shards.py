@@ -70,3 +70,28 @@ def test_two_gloo_ranks_sum_to_the_single_process_images(tmp_path, oracle):
     for k in ("image1", "image2s", "illum"):
         assert np.abs(ref[k]).max() > 0
         assert rel_l2(red[k], ref[k]) < 1e-12, k
+
+
+def test_a_rank_that_dies_before_the_reduction_ends_the_others(tmp_path):
+    """Failure detection on the host: the second of two gloo ranks exits after its shots and
+    before the image reduction.  The first rank's reduction fails with an error instead of
+    waiting, and it exits with its own status; both end well inside the test's time limit."""
+    import time
+    out = str(tmp_path / "reduced.npz")
+    port = str(_free_port())
+    env = dict(os.environ, PYTHONPATH=ROOT)
+    t0 = time.time()
+    procs = [subprocess.Popen([sys.executable, os.path.join(ROOT, "tests", "_gloo_rank.py"), str(r), "2", port, out,
+                               "fail"], env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT) for r in range(2)]
+    logs = []
+    for p in procs:
+        try:
+            logs.append(p.communicate(timeout=240)[0].decode(errors="replace"))
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            raise
+    assert [p.returncode for p in procs] == [4, 3], "\n".join(logs)
+    assert os.path.exists(out + ".failed") and not os.path.exists(out)
+    assert "rank 0" in open(out + ".failed").read()
+    assert time.time() - t0 < 200
