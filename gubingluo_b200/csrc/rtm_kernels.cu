@@ -184,20 +184,17 @@ __global__ void k_strip_pack(const ShotDev *shots, int it0, int ring0, int nstep
     }
     __syncthreads();
     m = s_max[0];
-    // power-of-two scale so that |x|/scale <= 1 (exact scaling, only the rounding of the
-    // narrow type remains)
-    float scale = 1.0f;
-    if (m > 0.0f) {
-        int e;
-        frexpf(m, &e);
-        scale = ldexpf(1.0f, e);
-    }
-    const float inv = 1.0f / scale;
+    // power-of-two scale 2^e with |x| < 2^e (exact scaling, only the rounding of the narrow
+    // type remains).  The values are divided by ldexpf, not multiplied by 1/scale: for a block
+    // whose largest value is a subnormal float, 1/scale overflows to infinity
+    int e = 0;
+    if (m > 0.0f) frexpf(m, &e);
+    const float scale = ldexpf(1.0f, e);
     const int it = it0 + step;
     if (threadIdx.x == 0) S.strip_scale[(size_t)it * 4 + kind] = scale;
     const size_t dst0 = (size_t)it * S.strip_len + off[kind];
     for (long i = threadIdx.x; i < len[kind]; i += blockDim.x) {
-        float v = src[i] * inv;
+        float v = ldexpf(src[i], -e);
         if (prec == RTM_FP16) ((__half *)S.strips)[dst0 + i] = __float2half_rn(v);
         else ((__nv_bfloat16 *)S.strips)[dst0 + i] = __float2bfloat16_rn(v);
     }
@@ -221,16 +218,11 @@ __global__ void k_gather_pack(const float *g, void *out, float *scale, int nt, i
     }
     __syncthreads();
     m = s_max[0];
-    float sc = 1.0f;
-    if (m > 0.0f) {
-        int e;
-        frexpf(m, &e);
-        sc = ldexpf(1.0f, e);
-    }
-    if (threadIdx.x == 0) scale[it] = sc;
-    const float inv = 1.0f / sc;
+    int e = 0;   // as in k_strip_pack: 2^e > |x|, values divided by ldexpf
+    if (m > 0.0f) frexpf(m, &e);
+    if (threadIdx.x == 0) scale[it] = ldexpf(1.0f, e);
     for (int i = threadIdx.x; i < nrec; i += blockDim.x) {
-        float v = row[i] * inv;
+        float v = ldexpf(row[i], -e);
         if (prec == RTM_FP16) ((__half *)out)[(size_t)it * nrec + i] = __float2half_rn(v);
         else ((__nv_bfloat16 *)out)[(size_t)it * nrec + i] = __float2bfloat16_rn(v);
     }
