@@ -598,7 +598,9 @@ __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6
             const bool zin = (zz >= npml && zz < Z - npml);
             const bool band = cc.xb || !zin;
             gkk[u] = __ldg(&kappa[id]);
-            gp0[u] = pp[id];
+            // a band cell's new p is the sum of its split fields: its old p is needed only on
+            // the grid's edge rows and columns, which keep it (edge tiles only)
+            gp0[u] = (MODE != 3 && band && !edge_tile) ? 0.f : pp[id];
             gs1[u] = (MODE != 3 && band) ? sxp[id] : 0.f;
             gs2[u] = (MODE != 3 && band) ? szp[id] : 0.f;
             gps[u] = 0.f;
