@@ -398,3 +398,27 @@ def test_packed_strips_and_gathers_survive_subnormal_values(rtmlib, prec):
         assert np.isfinite(got[k]).all(), k
         assert np.abs(ref[k]).max() > 0
         assert rel_l2(got[k], ref[k]) < tol, (k, rel_l2(got[k], ref[k]))
+
+
+@pytest.mark.gpu
+def test_tile_heights_do_not_change_the_bits(rtmlib, monkeypatch):
+    """Tile heights (and with them the row groups and the interior/general split of the tiles)
+    only reorganise the work: gathers and images are bit-identical for every choice."""
+    G = rtmlib
+    c = GENERAL[2]
+    v, rho = _random_model(c["nz"], c["nx"], 7)
+    shots = list(range(1, c["nshot"] + 1))
+    s = cfg_from(G, _survey(c, 0))
+    runs = []
+    for vel, recon, pres in ((None, None, None), ("16", "32", "32"), ("8", "8", "8"), ("64", "16", "64")):
+        for k, val in (("RTM_B200_BZ_VEL", vel), ("RTM_B200_BZ_VEL_RECON", recon), ("RTM_B200_BZ_PRES", pres)):
+            if val is None:
+                monkeypatch.delenv(k, raising=False)
+            else:
+                monkeypatch.setenv(k, val)
+        runs.append(G.migrate(s, G.RunOptions(extra_images=1), shots, v, rho))
+    for r in runs[1:]:
+        for k in ("image1", "image2s", "illum", "image3s", "image5s"):
+            assert np.array_equal(r[k], runs[0][k]), k
+        for a, b in zip(r["gathers"], runs[0]["gathers"]):
+            assert np.array_equal(a, b)
