@@ -35,14 +35,18 @@ constexpr int BX = RTM_BX;          // threads (= columns) per block
 constexpr int WW = RTM_STAGE_W;     // staged width: columns x0-12 .. x0+BX+11 (16-byte aligned)
 constexpr int R = RTM_RADIUS;
 // Rows per unrolled group (measured: 2 rows make the forward and receiver velocity kernels
-// 2-5% faster than 4, and the reconstruction 24% slower; the pressure kernels are fastest
-// at 4).  The z window of U rows is 2R+U-1 deep; the velocity kernels stage the rows of the
-// deeper window, so every mode reads one box height.
-constexpr int UV = RTM_GROUP_VEL, UVR = RTM_GROUP_VEL_RECON, UP = RTM_GROUP_PRES;
+// 2-5% faster than 4, and the reconstruction 24% slower; the forward and reconstruction
+// pressure kernels are fastest at 4, the receiver pressure kernel at 2 rows with 6 resident
+// blocks, 5% faster than 4 rows at 5 blocks).  The z window of U rows is 2R+U-1 deep; each
+// kernel family stages the rows of its deepest window, so every mode reads one box height.
+constexpr int UV = RTM_GROUP_VEL, UVR = RTM_GROUP_VEL_RECON, UP = RTM_GROUP_PRES, UPR = RTM_GROUP_PRES_RECV;
 constexpr int QNV_MAX = 2 * R + (UV > UVR ? UV : UVR) - 1;
-constexpr int QNP = 2 * R + UP - 1;
-static_assert(QNV_MAX - 1 == RTM_STAGE_ZEXTRA_VEL && QNP - 1 == RTM_STAGE_ZEXTRA_PRES,
+constexpr int QNP_MAX = 2 * R + (UP > UPR ? UP : UPR) - 1;
+static_assert(QNV_MAX - 1 == RTM_STAGE_ZEXTRA_VEL && QNP_MAX - 1 == RTM_STAGE_ZEXTRA_PRES,
               "staged rows beyond a tile must cover the z window");
+#ifndef RTM_PRES_RECV_BLOCKS
+#define RTM_PRES_RECV_BLOCKS 6   // resident blocks of the fp32 receiver pressure kernel
+#endif
 static_assert(WW == BX + 24, "staged width");
 constexpr long kWaitLimit = 1L << 22;   // polls of a tile's TMA barrier before giving up
 
@@ -531,12 +535,13 @@ __global__ void __launch_bounds__(BX, MODE == 3 && BZ == 8 ? 5 : 6) k_vel(const 
 // PML, source or receiver tests and no split-field loads, in the arithmetic of the general
 // body's interior branch (for the reconstruction: tiles of the interior with no source cell).
 template <int BZ, int MODE, typename ACC>
-__global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6) k_pres(const StepArgs a, int record)
+__global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : RTM_PRES_RECV_BLOCKS) : 6)
+    k_pres(const StepArgs a, int record)
 {
-    constexpr int U = UP, QN = QNP;
+    constexpr int U = MODE == 2 ? UPR : UP, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
-    constexpr int ZH = BZ + QN - 1;   // vz rows z0-10 .. z0+BZ+QN-12, columns x0 .. x0+BX-1
+    constexpr int ZH = BZ + QNP_MAX - 1;   // vz rows z0-10 .. z0+BZ+QNP_MAX-12 (the box height), columns x0 ..
     extern __shared__ __align__(128) float sm[];
     float *svx = sm;
     float *svz = sm + XH * WW;   // XH * WW * 4 bytes is a multiple of 128
@@ -758,7 +763,7 @@ __global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : 5) : 6
 template <int BZ>
 static size_t vel_smem() { return (size_t)(BZ + QNV_MAX - 1) * WW * sizeof(float); }
 template <int BZ>
-static size_t pres_smem() { return ((size_t)BZ * WW + (size_t)(BZ + QNP - 1) * BX) * sizeof(float); }
+static size_t pres_smem() { return ((size_t)BZ * WW + (size_t)(BZ + QNP_MAX - 1) * BX) * sizeof(float); }
 
 template <int BZ, int MODE>
 static void vel_launch(const StepArgs &a, int ntiles, cudaStream_t s)
