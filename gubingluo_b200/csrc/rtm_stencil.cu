@@ -35,17 +35,26 @@ constexpr int BX = RTM_BX;          // threads (= columns) per block
 constexpr int WW = RTM_STAGE_W;     // staged width: columns x0-12 .. x0+BX+11 (16-byte aligned)
 constexpr int R = RTM_RADIUS;
 // Rows per unrolled group (measured: 2 rows make the forward and receiver velocity kernels
-// 2-5% faster than 4, and the reconstruction 24% slower; the forward and reconstruction
-// pressure kernels are fastest at 4, the receiver pressure kernel at 2 rows with 6 resident
-// blocks, 5% faster than 4 rows at 5 blocks).  The z window of U rows is 2R+U-1 deep; each
-// kernel family stages the rows of its deepest window, so every mode reads one box height.
-constexpr int UV = RTM_GROUP_VEL, UVR = RTM_GROUP_VEL_RECON, UP = RTM_GROUP_PRES, UPR = RTM_GROUP_PRES_RECV;
-constexpr int QNV_MAX = 2 * R + (UV > UVR ? UV : UVR) - 1;
-constexpr int QNP_MAX = 2 * R + (UP > UPR ? UP : UPR) - 1;
+// 2-5% faster than 4, and the reconstruction 24% slower; the forward and receiver pressure
+// kernels are fastest at 2 rows with 7 resident blocks (72 registers), 4-9% faster than 4
+// rows at 6 and 5 blocks, while the reconstruction pressure kernel is 4% slower that way
+// than at 4 rows and 6 blocks).  The z window of U rows is 2R+U-1 deep; each kernel family
+// stages the rows of its deepest window, so every mode reads one box height.
+constexpr int UV = RTM_GROUP_VEL, UVR = RTM_GROUP_VEL_RECON;
+constexpr int UP = RTM_GROUP_PRES, UPR = RTM_GROUP_PRES_RECV, UPC = RTM_GROUP_PRES_RECON;
+constexpr int QNV_MAX = 2 * R + RTM_MAX2(UV, UVR) - 1;
+constexpr int QNP_MAX = 2 * R + RTM_MAX2(UP, RTM_MAX2(UPR, UPC)) - 1;
 static_assert(QNV_MAX - 1 == RTM_STAGE_ZEXTRA_VEL && QNP_MAX - 1 == RTM_STAGE_ZEXTRA_PRES,
               "staged rows beyond a tile must cover the z window");
+// resident blocks per SM of the fp32 pressure kernels (forward; receiver pass; reconstruction)
+#ifndef RTM_PRES_FWD_BLOCKS
+#define RTM_PRES_FWD_BLOCKS 7
+#endif
 #ifndef RTM_PRES_RECV_BLOCKS
-#define RTM_PRES_RECV_BLOCKS 6   // resident blocks of the fp32 receiver pressure kernel
+#define RTM_PRES_RECV_BLOCKS 7
+#endif
+#ifndef RTM_PRES_RECON_BLOCKS
+#define RTM_PRES_RECON_BLOCKS 6
 #endif
 static_assert(WW == BX + 24, "staged width");
 constexpr long kWaitLimit = 1L << 22;   // polls of a tile's TMA barrier before giving up
@@ -535,10 +544,12 @@ __global__ void __launch_bounds__(BX, MODE == 3 && BZ == 8 ? 5 : 6) k_vel(const 
 // PML, source or receiver tests and no split-field loads, in the arithmetic of the general
 // body's interior branch (for the reconstruction: tiles of the interior with no source cell).
 template <int BZ, int MODE, typename ACC>
-__global__ void __launch_bounds__(BX, MODE == 2 ? (sizeof(ACC) == 8 ? 4 : RTM_PRES_RECV_BLOCKS) : 6)
+__global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_PRES_RECV_BLOCKS)
+                                     : MODE == 3 ? RTM_PRES_RECON_BLOCKS
+                                                 : RTM_PRES_FWD_BLOCKS)
     k_pres(const StepArgs a, int record)
 {
-    constexpr int U = MODE == 2 ? UPR : UP, QN = 2 * R + U - 1;
+    constexpr int U = MODE == 2 ? UPR : MODE == 3 ? UPC : UP, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QNP_MAX - 1;   // vz rows z0-10 .. z0+BZ+QNP_MAX-12 (the box height), columns x0 ..

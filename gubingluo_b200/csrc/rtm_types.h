@@ -18,7 +18,7 @@
 #define RTM_RADIUS 10
 #define RTM_BX 128       // stencil tile width: columns (= threads) per block
 // rows per unrolled group of the velocity kernels (forward and receiver passes; the
-// reconstruction) and of the pressure kernels (forward and reconstruction; receiver pass)
+// reconstruction) and of the pressure kernels (forward; receiver pass; reconstruction)
 #ifndef RTM_GROUP_VEL
 #define RTM_GROUP_VEL 2
 #endif
@@ -26,18 +26,22 @@
 #define RTM_GROUP_VEL_RECON 4
 #endif
 #ifndef RTM_GROUP_PRES
-#define RTM_GROUP_PRES 4
+#define RTM_GROUP_PRES 2
 #endif
 #ifndef RTM_GROUP_PRES_RECV
 #define RTM_GROUP_PRES_RECV 2
 #endif
+#ifndef RTM_GROUP_PRES_RECON
+#define RTM_GROUP_PRES_RECON 4
+#endif
+#define RTM_MAX2(a, b) ((a) > (b) ? (a) : (b))
 #define RTM_STAGE_W (RTM_BX + 24)                             // staged width: columns x0-12 .. x0+BX+11
 // staged rows beyond a tile's BZ (the z window) of the velocity kernels' p and the pressure
 // kernels' vz
 #define RTM_STAGE_ZEXTRA_VEL \
     (2 * RTM_RADIUS + (RTM_GROUP_VEL > RTM_GROUP_VEL_RECON ? RTM_GROUP_VEL : RTM_GROUP_VEL_RECON) - 2)
 #define RTM_STAGE_ZEXTRA_PRES \
-    (2 * RTM_RADIUS + (RTM_GROUP_PRES > RTM_GROUP_PRES_RECV ? RTM_GROUP_PRES : RTM_GROUP_PRES_RECV) - 2)
+    (2 * RTM_RADIUS + RTM_MAX2(RTM_GROUP_PRES, RTM_MAX2(RTM_GROUP_PRES_RECV, RTM_GROUP_PRES_RECON)) - 2)
 
 // What one launch of the stencil kernels updates.
 enum RtmWaveMode {
