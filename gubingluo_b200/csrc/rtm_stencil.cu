@@ -46,6 +46,9 @@ constexpr int QNV_MAX = 2 * R + RTM_MAX2(UV, UVR) - 1;
 constexpr int QNP_MAX = 2 * R + RTM_MAX2(UP, RTM_MAX2(UPR, UPC)) - 1;
 static_assert(QNV_MAX - 1 == RTM_STAGE_ZEXTRA_VEL && QNP_MAX - 1 == RTM_STAGE_ZEXTRA_PRES,
               "staged rows beyond a tile must cover the z window");
+#ifndef RTM_VEL_RECON_BLOCKS
+#define RTM_VEL_RECON_BLOCKS 6   // resident blocks per SM of the reconstruction velocity kernel
+#endif
 // resident blocks per SM of the fp32 pressure kernels (forward; receiver pass; reconstruction)
 #ifndef RTM_PRES_FWD_BLOCKS
 #define RTM_PRES_FWD_BLOCKS 7
@@ -358,7 +361,7 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
 // 8-row reconstruction tiles (5, which would spill at 6); with its interior-tile body the
 // reconstruction runs 4% faster at 6 than at 5.
 template <int BZ, int MODE>
-__global__ void __launch_bounds__(BX, MODE == 3 && BZ == 8 ? 5 : 6) k_vel(const StepArgs a)
+__global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_BLOCKS) : 6) k_vel(const StepArgs a)
 {
     constexpr int U = MODE == 3 ? UVR : UV, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
