@@ -160,7 +160,7 @@ static int run_units()
     ck("source");
     dump_dev("source", d_src, (size_t)X * Z);
 
-    // model (padded the way the driver pads it: extract + square + edge replicate)
+    // model (padded the way the reference's rtm_model pads it: extract + square + edge replicate)
     std::vector<float> v(nxl * nzl), r(nxl * nzl), vp2(X * Z), rho(X * Z), tmp(nxl * nzl);
     make_model(nxl, nzl, dx, v.data(), r.data(), 1);
     dump_host("model_v", v.data(), v.size());

@@ -1,8 +1,8 @@
 /*
  * rtm_oracle.h — CPU restatement of the reference's 2D acoustic prestack RTM hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for the CUDA product in
- * gubingluo_b200/: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+ * TEST INFRASTRUCTURE ONLY.  The CUDA product is tested against this oracle; the product in
+ * gubingluo_b200/ never uses it: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
  * reference arm may load it.  The product never links or calls it.
  *
  * Every function restates a piece of the reference (gubingluo/gubingluo) and cites the
