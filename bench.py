@@ -39,6 +39,37 @@ WORKLOAD = ("config 2: 1701x351 grid (X x Z = 1801 x 451 padded), dx=dz=12.5 m, 
             "dt=1 ms, 15 Hz Ricker, 64 full-spread shots every 25 grid points, source-illumination-"
             "normalised imaging, FP32 stencil/strips/gathers/accumulators")
 
+MODEL_TEXT = {1: "four flat layers and a dipping 3500 m/s wedge",
+              2: "gradient + random-field + thrust-fault",
+              3: "gradient + random-field + thrust-fault",
+              4: "gradient + random-field",
+              5: "gradient + salt body + water layer"}
+
+
+def workload_text(args, s, shots, meta):
+    """The workload of a --config run (configuration 2's text is WORKLOAD)."""
+    fp32 = args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64
+    if args.config == 2 and s.nt == 4000 and fp32:
+        return WORKLOAD
+    X, Z = s.nx + 2 * s.npml, s.nz + 2 * s.npml
+    if "apertures" in meta:
+        ap = meta["apertures"].values()
+        spread = (f"layout {s.layout}, each shot's aperture drawn from {min(ap)}-{max(ap)} columns and cut at "
+                  f"the model's edges")
+    else:
+        spread = "full spread" if s.layout == 2 else f"layout {s.layout}"
+    form = "FP32 stencil/strips/gathers/accumulators" if fp32 else (
+        f"FP32 stencil, {args.strips} strips, {args.gathers} gathers, "
+        f"{'FP64' if args.accum_fp64 else 'FP32'} accumulators")
+    return (f"config {args.config}: {s.nx}x{s.nz} grid (X x Z = {X} x {Z} padded), dx=dz={s.dx:g} m, "
+            f"{s.npml}-cell PML, nt={s.nt}, dt={s.dt * 1e3:g} ms, {s.fdom:g} Hz Ricker, {len(shots)} shots "
+            f"({spread}), source-illumination-normalised imaging, {form}")
+
+
+def data_text(n, meta):
+    return (f"synthetic (seeded {MODEL_TEXT[n]} model of configuration {n}; gathers modelled in the true model "
+            f"by this library before timing; migration in the {meta['smooth_m']:g} m-smoothed model)")
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -185,10 +216,17 @@ def run_ours(args, rank, world, local_rank):
     s, all_shots, v_true, v_mig, rho, meta = synthetic.config(args.config, nt=args.nt or None)
     B = args.shots_per_step
     K, W = args.steps, args.warmup
+    # per-shot windows when the configuration draws each shot's aperture (else the layout's)
+    s_mig = G.SurveyConfig(**{**s.__dict__, "mode": 1})
+    geo_list = synthetic.shot_geometries(s_mig, all_shots, meta)
+    geo_of = None if geo_list is None else dict(zip(all_shots, geo_list))
+
+    def geoms_for(shots):
+        return None if geo_of is None else [geo_of[sh] for sh in shots]
     # this rank's shots: longest-processing-time partition of the survey by shot cost
     # (nt * X * Z), repeated as needed to fill the steps
     from gubingluo_b200 import shards
-    parts = shards.lpt_shards(shards.shot_costs(G.SurveyConfig(**{**s.__dict__, "mode": 1}), all_shots), world)
+    parts = shards.lpt_shards(shards.shot_costs(s_mig, all_shots, geo_list), world)
     mine = [all_shots[i] for i in parts[rank]] or all_shots[:1]
     need = B * (K + W)
     uniq = mine[: min(len(mine), need)]
@@ -198,19 +236,19 @@ def run_ours(args, rank, world, local_rank):
     # ---- synthetic data: model this rank's gathers in the true model (untimed setup)
     t0 = time.time()
     s_model = G.SurveyConfig(**{**s.__dict__, "mode": 0})
-    with G.Session(s_model, G.RunOptions(device=local_rank, batch=min(len(uniq), 32)), uniq, v_true, rho) as ms:
+    with G.Session(s_model, G.RunOptions(device=local_rank, batch=min(len(uniq), 32)), uniq, v_true, rho,
+                   geometries=geoms_for(uniq)) as ms:
         ms.model()
         gathers = {sh: ms.gather(k) for k, sh in enumerate(uniq)}
     t_data = time.time() - t0
     # ---- migration session: the session holds every shot the steps use (inputs resident)
-    s_mig = G.SurveyConfig(**{**s.__dict__, "mode": 1})
-    ss = G.Session(s_mig, opts, step_shots, v_mig, rho)
+    ss = G.Session(s_mig, opts, step_shots, v_mig, rho, geometries=geoms_for(step_shots))
     for k, sh in enumerate(step_shots):
         ss.set_gather(k, gathers[sh])
-    geo = G.geometry(s_mig, step_shots[0])
+    # shot windows differ in layouts 1, 3, 4 and with per-shot apertures
+    geos = {sh: (G.geometry(s_mig, sh) if geo_of is None else geo_of[sh]) for sh in set(step_shots)}
+    geo = geos[step_shots[0]]
     X, Z, nxi, nzi, nrec = geo.nxpad, geo.nzpad, geo.nxlength, s.nz, geo.nrec
-    w_shot = s.nt * (2.0 * X * Z + nxi * nzi)           # cell-updates of the first shot
-    geos = {sh: G.geometry(s_mig, sh) for sh in set(step_shots)}   # shot windows differ in layouts 1, 3, 4
 
     def w_of(sh):   # cell-updates of one shot: source pass, reconstruction, receiver pass
         g = geos[sh]
@@ -277,11 +315,12 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_e2e:
         host = {}
         for sh in set(step_shots):
-            t = torch.empty((s.nt, nrec), dtype=torch.float32, pin_memory=True)
+            t = torch.empty((s.nt, geos[sh].nrec), dtype=torch.float32, pin_memory=True)
             t.numpy()[:] = gathers[sh]
             host[sh] = t
         img_host = torch.empty((s.nz, s.nx), dtype=torch.float32, pin_memory=True)
-        h2d = B * s.nt * nrec * 4
+        # bytes per step: the timed steps' gathers (their receiver counts differ with the window)
+        h2d = sum(host[sh].numel() * 4 for sh in step_shots[W * B:(W + K) * B]) // K
         d2h = s.nz * s.nx * 4
         ss.reset_images()
         if dist:
@@ -328,7 +367,7 @@ def run_ours(args, rank, world, local_rank):
                 "kernel_ms": {k: round(v[0], 4) for k, v in sampled.items()}}
     return dict(value=value, gcell=gcell, ms_total=ms_total, launches=launches, e2e=e2e, roofline=roofline,
                 clocks=clock_info, shots_done=shots_done, t_data=t_data, X=X, Z=Z, nxi=nxi, nzi=nzi, nrec=nrec,
-                w_shot=w_shot, s=s, shots_per_launch=nshots_launch)
+                w_shot=w_timed / (K * B), s=s, shots_per_launch=nshots_launch, meta=meta, all_shots=all_shots)
 
 
 # ------------------------------------------------------------------------------------------
@@ -452,13 +491,31 @@ def run_real(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def cpu_sample(args, s, v_mig, rho, nrec, w_shot):
+def survey_shot_work(s, shots, meta):
+    """Oracle geometry of every shot (with its own aperture where the configuration draws
+    one) and its cell-updates nt (2 X Z + nxi nzi); shot windows differ in layouts 1, 3, 4."""
+    from oracle import oracle as O
+
+    out = []
+    for ish in shots:
+        om = (meta["apertures"][ish] - 1) * s.dx if "apertures" in meta else s.offsetmax
+        g = O.geometry(s.layout, ish, s.nx, s.nz, s.nt, s.dx, s.dz, s.dt, s.npml, s.spx0, s.spz0, s.dspx,
+                       s.offset, om)
+        out.append((ish, om, s.nt * (2.0 * g.nxpad * g.nzpad + g.nxlength * s.nz)))
+    return out
+
+
+def cpu_sample(args, s, v_mig, rho, shots, meta, w_shot):
     """The CPU restatement of the reference's path (oracle, FP32, OpenMP) on one shot of the
-    same grid for --cpu-sample-steps steps; returns shots/s of the full nt and the sample."""
+    survey (the one of median cell-updates) for --cpu-sample-steps steps; returns shots/s of
+    the full nt at w_shot cell-updates per shot, and the sample."""
     from oracle import oracle as O
 
     nt_s = args.cpu_sample_steps
-    g = O.geometry(s.layout, 1, s.nx, s.nz, nt_s, s.dx, s.dz, s.dt, s.npml, s.spx0, s.spz0, s.dspx)
+    work = sorted(survey_shot_work(s, shots, meta), key=lambda t: (t[2], t[0]))
+    ish, om, _ = work[len(work) // 2]
+    g = O.geometry(s.layout, ish, s.nx, s.nz, nt_s, s.dx, s.dz, s.dt, s.npml, s.spx0, s.spz0, s.dspx, s.offset,
+                   om)
     vp2 = O.pad_model(v_mig, g.nx1, g.nx2, s.npml, True)
     rp = O.pad_model(rho, g.nx1, g.nx2, s.npml, False)
     vpmax = float(np.sqrt(np.float32(vp2.max()), dtype=np.float32))
@@ -472,8 +529,8 @@ def cpu_sample(args, s, v_mig, rho, nrec, w_shot):
     gcell = cells / sec * 1e-9
     return {"value": gcell * 1e9 / w_shot, "unit": "shots/s", "cores": O.num_threads(), "kind": "port",
             "gcell_updates_per_s": round(gcell, 4), "seconds": round(sec, 2),
-            "sample": f"1 shot of the same {g.nxpad}x{g.nzpad} grid for {nt_s} of {s.nt} time steps (source pass, "
-                      f"reconstruction, receiver pass, imaging), scaled to the full nt"}
+            "sample": f"shot {ish} ({g.nxpad}x{g.nzpad} padded grid) for {nt_s} of {s.nt} time steps (source "
+                      f"pass, reconstruction, receiver pass, imaging), scaled to the full nt"}
 
 
 def run_reference(args, rank):
@@ -482,11 +539,12 @@ def run_reference(args, rank):
     from gubingluo_b200 import synthetic
 
     s, shots, v_true, v_mig, rho, meta = synthetic.config(args.config, nt=args.nt or None)
-    X, Z = s.nx + 2 * s.npml, s.nz + 2 * s.npml
-    w_shot = s.nt * (2.0 * X * Z + s.nx * s.nz)
+    # mean cell-updates per shot of the survey
+    ws = [w for _, _, w in survey_shot_work(s, shots, meta)]
+    w_shot = sum(ws) / len(ws)
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_sample(args, s, v_mig, rho, s.nx, w_shot)
+        r = cpu_sample(args, s, v_mig, rho, shots, meta, w_shot)
         if i >= args.warmup:
             vals.append(r)
     value = statistics.mean(r["value"] for r in vals)
@@ -494,8 +552,8 @@ def run_reference(args, rank):
     line = {"metric": "shots/s", "value": value, "unit": "shots/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "impl": "reference",
-            "data": "synthetic (seeded model of benchmark configuration 2)",
-            "config": {"workload": WORKLOAD, "shots_per_step": "bounded CPU sample"},
+            "data": f"synthetic (seeded model of benchmark configuration {args.config})",
+            "config": {"workload": workload_text(args, s, shots, meta), "shots_per_step": "bounded CPU sample"},
             "gcell_updates_per_s": statistics.mean(r["gcell_updates_per_s"] for r in vals),
             "cpu_baseline": {**vals[-1], "value": value},
             "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -522,16 +580,16 @@ def main():
         from gubingluo_b200 import synthetic
 
         _, _, _, v_mig, rho, _ = synthetic.config(args.config, nt=args.nt or None)
-        cpu = cpu_sample(args, s, v_mig, rho, r["nrec"], r["w_shot"])
+        cpu = cpu_sample(args, s, v_mig, rho, r["all_shots"], r["meta"], r["w_shot"])
     dtype = "f32" if args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64 else \
         f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {'f64' if args.accum_fp64 else 'f32'} images"
     ws_gb = r["shots_per_launch"] * 12 * r["X"] * r["Z"] * 4 / 1e9
     line = {"metric": "shots/s", "value": r["value"], "unit": "shots/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_total"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": dtype,
-            "data": "synthetic (seeded gradient + random-field + thrust-fault model of configuration 2; gathers "
-                    "modelled in the true model by this library before timing; migration in the 250 m-smoothed model)",
-            "config": {"workload": WORKLOAD, "shots_per_step_per_gpu": args.shots_per_step,
+            "data": data_text(args.config, r["meta"]),
+            "config": {"workload": workload_text(args, s, r["all_shots"], r["meta"]),
+                       "shots_per_step_per_gpu": args.shots_per_step,
                        "shots_per_launch": r["shots_per_launch"], "nt": s.nt,
                        "parallelism": f"shots sharded over {world} GPU(s)",
                        "l2": f"inputs larger than L2: per-launch wavefield+model working set {ws_gb:.1f} GB vs 126 MB L2"},

@@ -14,11 +14,12 @@ from __future__ import annotations
 from . import SurveyConfig, geometry
 
 
-def shot_costs(survey: SurveyConfig, shots) -> list:
-    """nt * nxpad * nzpad of each shot's padded grid."""
+def shot_costs(survey: SurveyConfig, shots, geometries=None) -> list:
+    """nt * nxpad * nzpad of each shot's padded grid (geometries[k] of shot k when given, as
+    for rtm_session_open_geometry; else the survey's layout)."""
     out = []
-    for ishot in shots:
-        g = geometry(survey, int(ishot))
+    for k, ishot in enumerate(shots):
+        g = geometry(survey, int(ishot)) if geometries is None else geometries[k]
         out.append(float(survey.nt) * g.nxpad * g.nzpad)
     return out
 

@@ -4,7 +4,8 @@ The reference ships no data; its benchmark configurations describe velocity mode
 Each builder returns the true velocity, the migration velocity (the true model smoothed in
 velocity), a constant density of 2000 kg/m^3 (the reference's default without a density file,
 RTM_GPU_velstr.cpp:148) and the survey parameters.  Random fields use numpy PCG64 with seed
-20260000 + config number (faults / salt: 20260100 + config number).
+20260000 + config number (faults / salt: 20260100 + config number; per-shot apertures:
+20260200 + config number).
 """
 from __future__ import annotations
 
@@ -12,7 +13,7 @@ import math
 
 import numpy as np
 
-from . import SurveyConfig
+from . import SurveyConfig, geometry
 
 
 def _gaussian_smooth(a: np.ndarray, sigma_z: float, sigma_x: float) -> np.ndarray:
@@ -103,12 +104,15 @@ def config(n: int, nshots: int | None = None, nt: int | None = None):
         zz = np.arange(nz)[:, None] * d
         v = 1500.0 + 0.6 * zz + gaussian_random_field(nz, nx, d, d, 150.0, 60.0, 200.0, rng)
         smooth_m = 250.0
-        # bilateral apertures drawn from 2-8 km: the survey's offsetmax is the widest; each
-        # shot's aperture is set per shot by the caller (meta["apertures"])
+        # each shot's aperture drawn uniformly from 2-8 km (201-801 columns, centred on its
+        # source; cut at the model's edges): meta["apertures"] maps shot number -> columns,
+        # for shot_geometries.  The survey's offsetmax is the widest.
         step = (nx - 1) * d / ns
         s = SurveyConfig(nx=nx, nz=nz, nt=NT, dx=d, dz=d, dt=dt, npml=npml, fdom=fdom, layout=1,
                          spx0=step / 2, spz0=2 * d, dspx=step, offsetmax=8000.0, receiver_depth=2)
         shots = list(range(1, ns + 1))
+        half = np.random.default_rng(20260200 + n).integers(100, 401, size=ns)
+        apertures = {ishot: int(2 * h + 1) for ishot, h in zip(shots, half)}
     elif n == 5:
         nx, nz, d, npml, fdom, dt, NT, ns = 2401, 1001, 7.5, 80, 18.0, 5e-4, 8000, 128
         zz = np.arange(nz)[:, None] * d
@@ -132,11 +136,30 @@ def config(n: int, nshots: int | None = None, nt: int | None = None):
     s.direct, s.direct0 = 1.5, 0.0
     if nt is not None:
         s.nt = nt
+    meta = dict(config=n, smooth_m=smooth_m)
+    if n == 4:
+        meta["apertures"] = apertures
     if nshots is not None:
         shots = shots[:nshots]
     s.dt = float(np.float32(s.dt))
-    meta = dict(config=n, smooth_m=smooth_m)
     return s, shots, v, vm, rho, meta
+
+
+def shot_geometries(survey: SurveyConfig, shots, meta):
+    """Per-shot geometry of a survey whose apertures differ shot by shot (meta["apertures"]:
+    shot number -> columns, layout 1): the reference's layout-1 window of each shot
+    (rtm_model.cu:122-154) with offsetmax set to its own aperture.  None when every shot
+    follows the survey's own layout."""
+    if "apertures" not in meta:
+        return None
+    if survey.layout != 1:
+        raise ValueError("per-shot apertures need layout 1")
+    out = []
+    for ishot in shots:
+        w = meta["apertures"][int(ishot)]
+        sk = SurveyConfig(**{**survey.__dict__, "offsetmax": (w - 1) * survey.dx})
+        out.append(geometry(sk, int(ishot)))
+    return out
 
 
 def write_shot_file(path: str, shots, nt0: int, dt0: float, dx0: float, sgyflag: int = 0,
