@@ -537,9 +537,10 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_B
 // 2: receiver (backward model): overwrite the receiver row with dt*gather[it], then image
 // g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p strips of step it restored,
 // source subtracted).
-// Register budgets (measured): 6 blocks per SM (80 registers, no spills) for the forward
-// pass and the reconstruction, 5 for the receiver pass (4 with fp64 accumulators, which
-// would spill at 5).  A bound of 5 on the forward pass was slower than no bound, 6 faster.
+// Register budgets (measured, no spills): 7 blocks per SM (72 registers) for the forward and
+// receiver passes in their 2-row groups, 6 (80 registers) for the reconstruction in 4-row
+// groups, 4 for the receiver pass with fp64 accumulators (123 registers).  With 4-row groups
+// the receiver pass needed 96 registers (5 blocks) and spilled when capped at 6.
 //
 // Interior tiles (TileRef.interior, set by the host for tiles whose every column lies in
 // [npml, X-npml) and every row in [npml, Z-npml), with no source cell and no receiver) take
