@@ -22,6 +22,8 @@
 // Reference equivalents (gubingluo kernel.cu): forward v :430-500 + :542-713, forward p
 // :501-541 + :714-1185, reconstruction :318-429, strip restore :1294-1400, source :36-47,
 // receivers :48-95, cross-correlation :1401-1416.
+#include <atomic>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -780,25 +782,32 @@ static size_t vel_smem() { return (size_t)(BZ + QNV_MAX - 1) * WW * sizeof(float
 template <int BZ>
 static size_t pres_smem() { return ((size_t)BZ * WW + (size_t)(BZ + QNP_MAX - 1) * BX) * sizeof(float); }
 
+// The dynamic shared-memory limit of a kernel is an attribute of the kernel's instance on
+// each device, so it is set once per device (bit d of `done`; a repeated set is harmless, so
+// two host threads that meet here first both set it).
+template <typename F>
+static void set_smem_once(std::atomic<unsigned long long> &done, F *fn, size_t bytes)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;   // the launch reports the error
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (bit) done.fetch_or(bit, std::memory_order_release);
+}
+
 template <int BZ, int MODE>
 static void vel_launch(const StepArgs &a, int ntiles, cudaStream_t s)
 {
-    static bool init = false;
-    if (!init) {
-        cudaFuncSetAttribute(k_vel<BZ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_smem<BZ>());
-        init = true;
-    }
+    static std::atomic<unsigned long long> done{0};
+    set_smem_once(done, k_vel<BZ, MODE>, vel_smem<BZ>());
     k_vel<BZ, MODE><<<ntiles, BX, vel_smem<BZ>(), s>>>(a);
 }
 template <int BZ, int MODE, typename ACC>
 static void pres_launch_t(const StepArgs &a, int ntiles, int record, cudaStream_t s)
 {
-    static bool init = false;
-    if (!init) {
-        cudaFuncSetAttribute(k_pres<BZ, MODE, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)pres_smem<BZ>());
-        init = true;
-    }
+    static std::atomic<unsigned long long> done{0};
+    set_smem_once(done, k_pres<BZ, MODE, ACC>, pres_smem<BZ>());
     k_pres<BZ, MODE, ACC><<<ntiles, BX, pres_smem<BZ>(), s>>>(a, record);
 }
 template <int BZ, int MODE>
