@@ -16,8 +16,10 @@ steps (inside the timed region).
 --impl reference times the reference's CPU path on the host cores.  The reference has no CPU
 implementation of the stencil or imaging (its host code is serial model preparation and file
 I/O), so this arm runs the CPU restatement of its algorithm (oracle/, FP32, OpenMP on all host
-threads) on a bounded sample: one shot of the same grid for --cpu-sample-steps time steps,
-scaled to shots/s of the full nt.
+threads) on a bounded sample: the survey's shot of median cell-updates, for
+--cpu-sample-steps time steps, scaled to shots/s of the full nt at the survey's mean
+cell-updates per shot.  --config N (1-5) selects another benchmark configuration; its
+per-shot windows (configuration 4 draws each shot's aperture) are used by both arms.
 """
 from __future__ import annotations
 
