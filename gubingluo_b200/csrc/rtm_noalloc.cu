@@ -7,7 +7,9 @@
 //     the device's memory, where a fresh cudaMalloc of two image-sized buffers can fail or
 //     force that allocator to give back its cache;
 //   * multi-stream pipelines that cannot afford the device-wide synchronisation that the
-//     matching cudaFree performs.
+//     matching cudaFree performs.  The copies and the kernel run on the calling thread's
+//     per-thread default stream (cudaStreamPerThread), which does not wait for the caller's
+//     other streams; the call returns once that stream has finished.
 // The image travels through one fixed scratch area that is part of this translation unit's
 // device image: a file-scope __device__ array of kScratchCells cells for the input copy and as
 // many for the filtered result (48 MiB per device in all, kept by every GPU on which this
@@ -16,6 +18,10 @@
 // in, and the kernel writes every output cell (the border included).  There is one scratch
 // area per device, so calls on the same device must not overlap in time: two concurrent calls
 // would read and write the same cells.
+// The scratch address is looked up per device context: after cudaDeviceReset (or under another
+// context of the same device) the module is loaded again, and the next call looks the address
+// up again instead of using the old one.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -54,7 +60,25 @@ __global__ void k_laplace_scratch(float *scratch, int nx, int nz, int dx, int dz
 }
 
 std::mutex g_mu;
-float *g_base[kMaxDevices];   // device address of g_scratch, looked up once per device
+// device address of g_scratch and the context it was looked up in, per device
+float *g_base[kMaxDevices];
+CUcontext g_ctx[kMaxDevices];
+
+// cuCtxGetCurrent from the driver (through the runtime, so the library needs no -lcuda).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (CtxGetCurrentFn)p;
+    });
+    return fn;
+}
 
 }  // namespace
 
@@ -74,26 +98,39 @@ extern "C" int rtm_laplace_image_noalloc(float *image, int nx, int nz, int dx, i
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return rtm::fail(RTM_ERR_ARG, "device index out of range");
+    // cudaFree(0) makes the device's primary context current if no context is yet
+    e = cudaFree(nullptr);
+    if (e != cudaSuccess) return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
+    CtxGetCurrentFn get_ctx = ctx_get_current();
+    CUcontext ctx = nullptr;
+    if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS || !ctx)
+        return rtm::fail(RTM_ERR_CUDA, "no current CUDA context");
     float *base = nullptr;
     {
-        // the first call on a device (that device current) looks the scratch address up
+        // the first call in a device context (that device current) looks the scratch address up
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_base[dev]) {
-            e = cudaGetSymbolAddress((void **)&g_base[dev], g_scratch);
+        if (!g_base[dev] || g_ctx[dev] != ctx) {
+            float *addr = nullptr;
+            e = cudaGetSymbolAddress((void **)&addr, g_scratch);
             if (e != cudaSuccess) {
                 g_base[dev] = nullptr;
+                g_ctx[dev] = nullptr;
                 return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
             }
+            g_base[dev] = addr;
+            g_ctx[dev] = ctx;
         }
         base = g_base[dev];
     }
     const size_t bytes = (size_t)n * sizeof(float);
-    if ((e = cudaMemcpy(base, image, bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+    cudaStream_t st = cudaStreamPerThread;
+    if ((e = cudaMemcpyAsync(base, image, bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
     const int blocks = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
-    k_laplace_scratch<<<blocks, 256>>>(base, nx, nz, dx, dz);
+    k_laplace_scratch<<<blocks, 256, 0, st>>>(base, nx, nz, dx, dz);
     if ((e = cudaGetLastError()) != cudaSuccess) return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
-    if ((e = cudaMemcpy(image, base + kScratchCells, bytes, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(image, base + kScratchCells, bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return rtm::fail(RTM_ERR_CUDA, cudaGetErrorString(e));
     return RTM_OK;
 }

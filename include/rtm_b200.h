@@ -281,8 +281,9 @@ void rtm_laplace_image(float *image, int nx, int nz, int dx, int dz);
  * reference, whose laplacefd1d (image_function.cpp:44-79) runs on the host only.  The image
  * passes through a fixed 48 MiB scratch area per device that is part of the library (input
  * copy + result, at most 6 Mi cells = 6291456 = nx*nz); larger images return RTM_ERR_ARG.
- * Synchronous on the legacy default stream of the current device.  Calls on one device must
- * not overlap (they share the scratch).  The first call on each device looks up the scratch
+ * Runs on the calling thread's per-thread default stream of the current device and returns
+ * when it has finished.  Calls on one device must not overlap (they share the scratch).  The
+ * first call in each device context (again after cudaDeviceReset) looks up the scratch
  * address with that device current; make that first call before any stream capture begins.
  * Returns RTM_OK or an RTM_ERR_* code (message in rtm_last_error()). */
 int rtm_laplace_image_noalloc(float *image, int nx, int nz, int dx, int dz);

@@ -20,7 +20,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_HOST = os.path.join(HERE, "_ref", "libref_host.so")
-REFERENCE_DIR = os.environ.get("RTM_REFERENCE_DIR", "/root/reference")
+# The reference checkout: $RTM_REFERENCE_DIR, else a directory named "reference" beside this
+# repository's root.
+REFERENCE_DIR = os.environ.get("RTM_REFERENCE_DIR") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 _vp = C.c_void_p
 

@@ -47,3 +47,23 @@ def test_noalloc_laplace_matches_host_filter_on_consecutive_calls(rtmlib):
         rc = f(_p(got), nx, nz, dx, dz)
         assert rc == 0, L.rtm_last_error()
         assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_noalloc_laplace_degenerate_shapes(rtmlib):
+    """Images one cell wide or tall, and 2 x 2, are all border: every cell must come back
+    exactly as the host filter gives it (zero), whatever the scratch held before."""
+    f = _noalloc(rtmlib)
+    L = rtmlib.lib()
+    rng = np.random.default_rng(7)
+    # a full call first leaves non-zero values in the scratch
+    big = rng.standard_normal((64, 96)).astype(np.float32)
+    assert f(_p(big), 96, 64, 10, 10) == 0, L.rtm_last_error()
+    for nz, nx in ((1, 257), (311, 1), (2, 2), (1, 1), (3, 2)):
+        img = rng.standard_normal((nz, nx)).astype(np.float32)
+        want = img.copy()
+        L.rtm_laplace_image(_p(want), nx, nz, 10, 10)
+        got = img.copy()
+        rc = f(_p(got), nx, nz, 10, 10)
+        assert rc == 0, L.rtm_last_error()
+        assert np.array_equal(got, want), (nz, nx)
