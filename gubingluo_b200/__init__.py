@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
     L.rtm_session_get_images_extra.argtypes = [vp] * 8
     L.rtm_session_reset_images.argtypes = [vp]
     L.rtm_session_nrec.argtypes = [vp, C.c_int]
+    L.rtm_session_get_pml.argtypes = [vp, C.c_int, vp, vp, vp, vp]
     L.rtm_session_stream.argtypes = [vp]
     L.rtm_session_stream.restype = vp
     L.rtm_session_kernel_ms.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int)]
@@ -349,6 +350,12 @@ class Session:
         n = C.c_int(0)
         ms = lib().rtm_session_kernel_ms(self.h, name.encode(), C.byref(n))
         return ms, n.value
+
+    def pml_profiles(self, k: int, X: int, Z: int):
+        """Shot k's device PML damping profiles (ddx [X], ddz [Z], ddxvx [X-1], ddzvz [Z-1])."""
+        out = [np.zeros(n, np.float32) for n in (X, Z, X - 1, Z - 1)]
+        _check(lib().rtm_session_get_pml(self.h, k, *[_ptr(a) for a in out]))
+        return out
 
     def wavefields(self, slot: int, X: int, Z: int):
         ps = np.zeros((Z, X), np.float32)

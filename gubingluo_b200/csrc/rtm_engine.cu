@@ -144,6 +144,14 @@ struct rtm_session {
     unsigned *d_absmax = nullptr;    // progress snapshots: [2 passes][snaps][B] max |p| bits
     int nsnap = 0;                   // snapshots per pass (0: none)
     unsigned long long config_hash = 0;   // survey, image-relevant options, shots, models
+    // use_graph: the time loop of each pass captured as one CUDA graph, instantiated once per
+    // launch shape (batch size and tile counts) and replayed for every batch of that shape
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;   // kernels per replay
+    };
+    std::map<std::vector<long>, GraphEntry> graphs;
+    bool capturing = false;
 };
 
 namespace rtm {
@@ -632,7 +640,7 @@ static int finish_gather(rtm_session *ss, ShotState &sh)
 static void timing_begin(rtm_session *ss, const char *name, int it, cudaEvent_t *ev_end)
 {
     *ev_end = nullptr;
-    if (it % 64 != 7) return;
+    if (it % 64 != 7 || ss->capturing) return;   // events in a captured graph do not time
     KernelTiming &t = ss->timing[name];
     if (t.used == (int)t.ev.size()) {
         cudaEvent_t a, b;
@@ -821,6 +829,48 @@ static int print_snapshots(rtm_session *ss, const BatchRun &br, int side, const 
     return RTM_OK;
 }
 
+// Run `body` (the launches of one pass's time loop) directly, or, with use_graph, as a CUDA
+// graph: captured from the session stream the first time a launch shape `key` is met,
+// instantiated, kept, and replayed for every later batch of that shape.  A replayed graph
+// launches exactly the kernels, grids and arguments that `body` would: the arguments hold the
+// session's device tables (shots, tiles, tensor maps), which each batch rewrites in place
+// before its passes run, so equal tile counts mean equal launches.  The kernel count of a
+// replay is added to the session's launch count.
+template <typename F>
+static int run_pass(rtm_session *ss, std::vector<long> key, F &&body)
+{
+    if (!ss->o.use_graph) {
+        body();
+        CK(cudaGetLastError());
+        return RTM_OK;
+    }
+    auto it = ss->graphs.find(key);
+    if (it == ss->graphs.end()) {
+        if (ss->graphs.size() >= 16) {   // bound the cache: shapes vary with uneven apertures
+            for (auto &kv : ss->graphs) cudaGraphExecDestroy(kv.second.exec);
+            ss->graphs.clear();
+        }
+        const int l0 = ss->launches;
+        CK(cudaStreamBeginCapture(ss->stream, cudaStreamCaptureModeThreadLocal));
+        ss->capturing = true;
+        body();
+        ss->capturing = false;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ss->stream, &g);
+        if (e != cudaSuccess) return fail(RTM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        rtm_session::GraphEntry ge;
+        e = cudaGraphInstantiate(&ge.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(RTM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        ge.launches = ss->launches - l0;
+        ss->launches = l0;
+        it = ss->graphs.emplace(std::move(key), ge).first;
+    }
+    CK(cudaGraphLaunch(it->second.exec, ss->stream));
+    ss->launches += it->second.launches;
+    return RTM_OK;
+}
+
 // Source pass (rtm_model.cu:322-346): nsteps forward steps with the source added; strips
 // saved after every step when `save` (one small copy kernel, so the stencil kernels carry no
 // strip logic); the gather recorded when `record` (mode 0 fuses the reference's separate
@@ -834,34 +884,45 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
     const int ntsnap = ss->nsnap ? (int)(o.tsnap / ss->s.dt) : 0;
     if (ntsnap) CK(cudaMemsetAsync(ss->d_absmax, 0, sizeof(unsigned) * ss->nsnap * ss->B, st));
     nvtxRangePushA(record && !save ? "rtm: modelling pass" : "rtm: source pass");
-    for (int it = 0; it < nsteps; it++) {
-        a.it = it;
-        a.ring = it % kRing;
-        const int mode = RTM_WAVE_FWD;
-        if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:324-326: |p| before the step
-            launch_absmax(ss->d_shots, br.n, 0, ss->d_absmax + (size_t)(it / ntsnap) * ss->B, st);
-            ss->launches++;
+    auto loop = [&] {
+        for (int it = 0; it < nsteps; it++) {
+            a.it = it;
+            a.ring = it % kRing;
+            const int mode = RTM_WAVE_FWD;
+            if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:324-326: |p| before the step
+                launch_absmax(ss->d_shots, br.n, 0, ss->d_absmax + (size_t)(it / ntsnap) * ss->B, st);
+                ss->launches++;
+            }
+            cudaEvent_t e;
+            timing_begin(ss, "vel_fwd", it, &e);
+            a.tiles = ss->d_tiles;
+            launch_vel(mode, ss->bz_vel, a, br.ntiles, st);
+            timing_end(ss, e);
+            timing_begin(ss, "pres_fwd", it, &e);
+            launch_pres_tiles(ss, br, mode, record ? 1 : 0);
+            timing_end(ss, e);
+            ss->launches += 1;
+            if (save) {
+                launch_strip_save(ss->d_shots, br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
+                ss->launches++;
+            }
+            if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
+                launch_strip_pack(ss->d_shots, br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
+                ss->launches++;
+            }
         }
-        cudaEvent_t e;
-        timing_begin(ss, "vel_fwd", it, &e);
-        a.tiles = ss->d_tiles;
-        launch_vel(mode, ss->bz_vel, a, br.ntiles, st);
-        timing_end(ss, e);
-        timing_begin(ss, "pres_fwd", it, &e);
-        launch_pres_tiles(ss, br, mode, record ? 1 : 0);
-        timing_end(ss, e);
-        ss->launches += 1;
-        if (save) {
-            launch_strip_save(ss->d_shots, br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
-            ss->launches++;
-        }
-        if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
-            launch_strip_pack(ss->d_shots, br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
-            ss->launches++;
+    };
+    if (ntsnap) {   // snapshots read back per pass: no graph
+        loop();
+        CK(cudaGetLastError());
+    } else {
+        int rc = run_pass(ss, {0, br.n, br.ntiles, br.ntiles_p, br.max_strip_len, nsteps, save, record}, loop);
+        if (rc) {
+            nvtxRangePop();
+            return rc;
         }
     }
     nvtxRangePop();
-    CK(cudaGetLastError());
     if (ntsnap) return print_snapshots(ss, br, 0, save ? "source" : "forward", nsteps, ntsnap);
     return RTM_OK;
 }
@@ -919,39 +980,51 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     unsigned *snap_b = ntsnap ? ss->d_absmax + (size_t)ss->nsnap * ss->B : nullptr;
     if (ntsnap) CK(cudaMemsetAsync(snap_b, 0, sizeof(unsigned) * ss->nsnap * ss->B, st));
     nvtxRangePushA("rtm: backward pass");
-    for (int it = s.nt - 2; it >= 0; it--) {
-        a.it = it;
-        cudaEvent_t e;
-        if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:415-417: receiver |p| before the step
-            launch_absmax(ss->d_shots, n, 1, snap_b + (size_t)(it / ntsnap) * ss->B, st);
-            ss->launches++;
+    auto loop = [&] {
+        for (int it = s.nt - 2; it >= 0; it--) {
+            a.it = it;
+            cudaEvent_t e;
+            if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:415-417: receiver |p| before the step
+                launch_absmax(ss->d_shots, n, 1, snap_b + (size_t)(it / ntsnap) * ss->B, st);
+                ss->launches++;
+            }
+            // reconstruction of the source wavefield, then the receiver wavefield and imaging
+            // (which reads the reconstructed pressure of the same step)
+            timing_begin(ss, "vel_recon", it, &e);
+            a.tiles = ss->d_tiles_r;
+            launch_vel(RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r, st);
+            timing_end(ss, e);
+            timing_begin(ss, "pres_recon", it, &e);
+            a.tiles = ss->d_tiles_pr;
+            launch_pres(RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0, st);
+            timing_end(ss, e);
+            timing_begin(ss, "vel_recv", it, &e);
+            a.tiles = ss->d_tiles;
+            launch_vel(RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles, st);
+            timing_end(ss, e);
+            timing_begin(ss, "pres_recv", it, &e);
+            launch_pres_tiles(ss, br, RTM_WAVE_RECEIVER, 0);
+            timing_end(ss, e);
+            ss->launches += 3;
+            if (o.extra_images) {
+                launch_image_extra(ss->d_shots, n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz,
+                                   s.dt, st);
+                ss->launches++;
+            }
         }
-        // reconstruction of the source wavefield, then the receiver wavefield and imaging
-        // (which reads the reconstructed pressure of the same step)
-        timing_begin(ss, "vel_recon", it, &e);
-        a.tiles = ss->d_tiles_r;
-        launch_vel(RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r, st);
-        timing_end(ss, e);
-        timing_begin(ss, "pres_recon", it, &e);
-        a.tiles = ss->d_tiles_pr;
-        launch_pres(RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0, st);
-        timing_end(ss, e);
-        timing_begin(ss, "vel_recv", it, &e);
-        a.tiles = ss->d_tiles;
-        launch_vel(RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles, st);
-        timing_end(ss, e);
-        timing_begin(ss, "pres_recv", it, &e);
-        launch_pres_tiles(ss, br, RTM_WAVE_RECEIVER, 0);
-        timing_end(ss, e);
-        ss->launches += 3;
-        if (o.extra_images) {
-            launch_image_extra(ss->d_shots, n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz, s.dt,
-                               st);
-            ss->launches++;
+    };
+    if (ntsnap) {
+        loop();
+        CK(cudaGetLastError());
+    } else {
+        int rc = run_pass(ss, {1, n, br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr, max_nxi, max_nzi,
+                               a.gather_prec}, loop);
+        if (rc) {
+            nvtxRangePop();
+            return rc;
         }
     }
     nvtxRangePop();
-    CK(cudaGetLastError());
     if (ntsnap) {
         int rc = print_snapshots(ss, br, 1, "backward", s.nt, ntsnap);
         if (rc) return rc;
@@ -1191,6 +1264,20 @@ int rtm_session_get_gather(rtm_session *ss, int k, float *gather)
     CK(cudaStreamSynchronize(ss->stream));
     const float *src = ss->s.mode == 0 ? sh.gather_raw : sh.gather32;
     CK(cudaMemcpy(gather, src, sizeof(float) * (size_t)ss->s.nt * sh.g.nrec, cudaMemcpyDeviceToHost));
+    return RTM_OK;
+}
+
+int rtm_session_get_pml(rtm_session *ss, int k, float *ddx, float *ddz, float *ddxvx, float *ddzvz)
+{
+    if (!ss || k < 0 || k >= (int)ss->shots.size()) return fail(RTM_ERR_ARG, "bad shot index");
+    const ShotState &sh = ss->shots[k];
+    CK(cudaSetDevice(ss->dev));
+    CK(cudaStreamSynchronize(ss->stream));
+    const PmlOffsets o = pml_offsets(sh.X, sh.Z);
+    struct { float *out; int off, n; } part[4] = {
+        {ddx, o.ddx, sh.X}, {ddz, o.ddz, sh.Z}, {ddxvx, o.ddxvx, sh.X - 1}, {ddzvz, o.ddzvz, sh.Z - 1}};
+    for (const auto &q : part)
+        if (q.out) CK(cudaMemcpy(q.out, sh.pml + q.off, sizeof(float) * q.n, cudaMemcpyDeviceToHost));
     return RTM_OK;
 }
 
@@ -1441,6 +1528,8 @@ void rtm_session_close(rtm_session *ss)
     if (!ss) return;
     cudaSetDevice(ss->dev);
     if (ss->stream) cudaStreamSynchronize(ss->stream);
+    for (auto &kv : ss->graphs) cudaGraphExecDestroy(kv.second.exec);
+    ss->graphs.clear();
     for (auto &kv : ss->timing)
         for (auto &e : kv.second.ev) {
             cudaEventDestroy(e.first);

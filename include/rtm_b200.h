@@ -77,7 +77,11 @@ typedef struct rtm_options {
     int gather_precision;    /* RTM_PREC_*: storage of the receiver gathers */
     int accum_fp64;          /* 1: image/illumination accumulation and division in fp64 */
     int batch;               /* shots per launch; 0 = as many as fit in device memory */
-    int use_graph;           /* reserved, ignored */
+    int use_graph;           /* 1: each pass's time loop (source pass; backward pass) runs as one
+                                CUDA graph, captured the first time a launch shape (shots per
+                                batch, tile counts) occurs and replayed for later batches of that
+                                shape; results are bit-identical to direct launches.  Not used with
+                                tsnap snapshots, and per-kernel timing is not sampled. */
     int verbose;             /* print per-batch progress like the reference */
     int extra_images;        /* the reference's other imaging conditions (kernel.cu:1417-1555):
                                 0 off; 1 wavefield decomposition, Poynting-angle and energy-norm
@@ -186,8 +190,14 @@ int rtm_session_model(rtm_session *ss);
 /* Device pointers of the stacked images (nz*nx, float or double per accum_fp64), for
  * reductions across GPUs; valid until rtm_session_close. */
 int rtm_session_image_ptrs(rtm_session *ss, void **image1, void **image2s, void **image2m, void **illum);
-/* Mode 0: copy shot k's modelled (unmuted) gather to the host, [nt][nrec_k]. */
+/* Copy shot k's gather to the host, [nt][nrec_k]: mode 0, the modelled (unmuted) gather;
+ * mode 1, the fp32 gather being migrated, after the direct-wave mute (cuda_mute1,
+ * kernel.cu:96-121) when the survey's mute is on. */
 int rtm_session_get_gather(rtm_session *ss, int k, float *gather);
+/* Copy shot k's device PML damping profiles (cuda_pmlCoeffpx/pz/vx/vz, kernel.cu:174-269,
+ * for the vpmax of the shot's model window): ddx [nxpad], ddz [nzpad], ddxvx [nxpad-1],
+ * ddzvz [nzpad-1]; any pointer may be NULL.  For parity tests. */
+int rtm_session_get_pml(rtm_session *ss, int k, float *ddx, float *ddz, float *ddxvx, float *ddzvz);
 /* Copy the stacked images (nz*nx each; any pointer may be NULL). */
 int rtm_session_get_images(rtm_session *ss, float *image1, float *image2s, float *image2m,
                            float *illum);

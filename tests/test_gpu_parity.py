@@ -3,8 +3,10 @@ fixtures) and against the CPU oracle.
 
 Tolerances (FP32 stencil): gathers and images within 1e-4 rel-L2 of the
 reference / oracle; the reduced-precision forms (fp16/bf16 strips and gathers, fp64
-accumulation) within 1e-3 rel-L2 of the FP64 oracle.  PML profiles and source/receiver
-indices are checked bit-exact.
+accumulation) within 1e-3 rel-L2 of the FP64 oracle (bf16 strips and gathers: 2e-2, below
+the bar; their 8-bit mantissa alone rounds each stored value by up to 2^-9).  Checked bit for
+bit against the reference's own output: the device PML profiles and the device mute mask of
+the reference's unit run; the shot geometry (source cell) through rtm_shot_geometry.
 """
 import ctypes as C
 import os
@@ -73,6 +75,54 @@ def test_forward_matches_reference_steps(rtmlib):
     assert rel_l2(vx, z["fwd_vx"].reshape(Z, X - 1)) < TOL_FP32
     assert rel_l2(vz, z["fwd_vz"].reshape(Z - 1, X)) < TOL_FP32
     assert rel_l2(gat, z["fwd_gather"].reshape(nsteps, nxl)) < TOL_FP32
+
+
+def _units_survey(rtmlib, z, mode):
+    """The survey of the reference's unit run (ref_units.npz): 96 x 64 interior, npml 32,
+    source at (nsx, nsz), receivers on the first interior row, nw = 60 and tlength = 50 for
+    the direct-wave mute (direct = 1.5, direct0 = 0.05 s)."""
+    nxl, nzl, npml, dx, dz, dt, fdom, nt, nsx, nsz, amp, alp = z["units_meta"]
+    nxl, nzl, npml, nt, nsx, nsz = map(int, (nxl, nzl, npml, nt, nsx, nsz))
+    f = lambda v: float(np.float32(v))
+    return rtmlib.SurveyConfig(nx=nxl, nz=nzl, nt=nt, dx=f(dx), dz=f(dz), dt=f(dt), npml=npml, fdom=f(fdom),
+                               amp=f(amp), alp=f(alp), layout=2, spx0=(nsx - npml) * f(dx),
+                               spz0=(nsz - npml) * f(dz), mode=mode, direct=1.5, direct0=f(0.05), mute=1)
+
+
+def test_device_pml_profiles_bit_exact(rtmlib):
+    """The session's device PML profiles (k_setup_pml, from the vpmax of the shot's model
+    window) equal the reference's cuda_pmlCoeffpx/pz/vx/vz output bit for bit.  The
+    reference's unit run used vpmax = 3000 m/s; the model is capped there so that the
+    session's vpmax = sqrt(max v^2) is exactly 3000."""
+    z = np.load(os.path.join(GOLDEN, "ref_units.npz"))
+    assert float(z["units_meta2"][1]) == 3000.0
+    s = _units_survey(rtmlib, z, 1)
+    v = np.minimum(z["model_v"].reshape(s.nz, s.nx), np.float32(3000.0))
+    assert v.max() == np.float32(3000.0)
+    r = z["model_rho"].reshape(s.nz, s.nx)
+    g = rtmlib.geometry(s, 1)
+    with rtmlib.Session(s, rtmlib.RunOptions(), [1], v, r) as ss:
+        got = ss.pml_profiles(0, g.nxpad, g.nzpad)
+    for name, a in zip(("pml_ddx", "pml_ddz", "pml_ddxvx", "pml_ddzvz"), got):
+        assert np.array_equal(a.view(np.int32), z[name].view(np.int32)), name
+
+
+def test_device_mute_mask_bit_exact(rtmlib):
+    """The device mute (k_mute on the session's gather) of an all-ones gather equals the
+    reference's cuda_mute1 mask bit for bit (receivers on the first interior row, the unit
+    run's model, nw = 60, tlength = 50)."""
+    z = np.load(os.path.join(GOLDEN, "ref_units.npz"))
+    s = _units_survey(rtmlib, z, 1)
+    v = z["model_v"].reshape(s.nz, s.nx)
+    r = z["model_rho"].reshape(s.nz, s.nx)
+    assert list(z["mute_meta"]) == [int(np.float32(1.5) / (np.float32(s.fdom) * np.float32(s.dt))), 50]
+    with rtmlib.Session(s, rtmlib.RunOptions(), [1], v, r) as ss:
+        ss.set_gather(0, np.ones((s.nt, ss.nrec(0)), np.float32))
+        got = ss.gather(0)
+    want = z["mute_mask"].reshape(s.nt, s.nx)
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.int32), want.view(np.int32))
+    assert 0 < (got == 0).sum() < got.size   # the mask cuts part of every trace, not all
 
 
 def _random_model(nz, nx, seed):
@@ -422,3 +472,27 @@ def test_tile_heights_do_not_change_the_bits(rtmlib, monkeypatch):
             assert np.array_equal(r[k], runs[0][k]), k
         for a, b in zip(r["gathers"], runs[0]["gathers"]):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("strips", ["fp32", "fp16"])
+def test_graph_replay_is_bitwise_identical(rtmlib, strips):
+    """use_graph: each pass's time loop captured once per launch shape and replayed gives the
+    gathers and images of direct launches bit for bit.  One shot per launch over shots of
+    three window widths (layout 1, offsetmax cut at the model's edges), so that graphs are
+    both captured and replayed, with packed strips too."""
+    G = rtmlib
+    c = GENERAL[2]
+    v, rho = _random_model(c["nz"], c["nx"], 9)
+    s = cfg_from(G, _survey(c, 0))
+    shots = [1, 2, 3, 1, 3]
+    widths = {G.geometry(s, k).nxpad for k in shots}
+    assert len(widths) > 1
+    base = dict(batch=1, strip_precision=strips)
+    want = G.migrate(s, G.RunOptions(**base), shots, v, rho)
+    got = G.migrate(s, G.RunOptions(use_graph=True, **base), shots, v, rho)
+    for k in ("image1", "image2s", "illum"):
+        assert np.array_equal(got[k], want[k]), k
+    for a, b in zip(got["gathers"], want["gathers"]):
+        assert np.array_equal(a, b)
+    assert got["stats"].kernel_launches == want["stats"].kernel_launches
