@@ -94,6 +94,12 @@ def parse():
                     help="real: the recorded-data path (SU file -> resampling -> mute -> migration), one GPU")
     ap.add_argument("--profile-only", action="store_true",
                     help="run --steps steps and exit (for ncu launch lists)")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="skip the configuration-4 comparison (batched mixed precision against plain "
+                         "FP32 one shot per launch) that the N=1 line carries")
+    ap.add_argument("--headline-only", action="store_true", help="run only the configuration-4 comparison")
+    ap.add_argument("--headline-sample", type=int, default=8,
+                    help="plain per-shot arm: every k-th shot of the 256 (default 8: 32 shots)")
     return ap.parse_args()
 
 
@@ -373,6 +379,94 @@ def run_ours(args, rank, world, local_rank):
 
 
 # ------------------------------------------------------------------------------------------
+def run_headline(args, local_rank):
+    """Configuration 4 (3201 x 801 grid, 10 m, 40-cell PML, nt = 5000 at 0.8 ms, 20 Hz; 256
+    shots whose apertures are drawn from 201-801 columns), two arms on the same GPU:
+
+      batched: all 256 shots in one session, as many per launch as device memory holds,
+               fp16 boundary strips and gathers, fp64 image accumulation;
+      plain per-shot: plain FP32 (strips, gathers, accumulators), one shot per launch with
+               each pass's time loop replayed as a CUDA graph, on every k-th shot of the
+               survey (--headline-sample; the apertures are drawn independently of the shot
+               number, so the sample has the survey's spread); also timed without the graph.
+
+    Both are timed with CUDA events on the session stream, gathers resident.  The ratio is
+    taken at equal work per shot: Gcell-updates/s of the batched arm over that of the
+    per-shot arm (= shots/s over shots/s when both arms' shots have the same mean size).
+    The image error of both forms against the FP64 oracle is tested in
+    tests/test_gpu_configs.py (narrowest and widest aperture, full nt)."""
+    import torch
+    import gubingluo_b200 as G
+    from gubingluo_b200 import synthetic
+
+    torch.cuda.set_device(local_rank)
+    s, shots, v_true, v_mig, rho, meta = synthetic.config(4, nt=args.nt or None)
+    s_mig = G.SurveyConfig(**{**s.__dict__, "mode": 1})
+    geo_of = dict(zip(shots, synthetic.shot_geometries(s_mig, shots, meta)))
+
+    def w_of(sh):
+        g = geo_of[sh]
+        return s.nt * (2.0 * g.nxpad * g.nzpad + g.nxlength * s.nz)
+    t0 = time.time()
+    s_model = G.SurveyConfig(**{**s.__dict__, "mode": 0})
+    gathers = {}
+    for k0 in range(0, len(shots), 64):
+        part = shots[k0:k0 + 64]
+        with G.Session(s_model, G.RunOptions(device=local_rank, batch=64), part, v_true, rho,
+                       geometries=[geo_of[sh] for sh in part]) as ms:
+            ms.model()
+            for k, sh in enumerate(part):
+                gathers[sh] = ms.gather(k)
+    t_data = time.time() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(opts, arm_shots, warm):
+        ss = G.Session(s_mig, opts, arm_shots, v_mig, rho, geometries=[geo_of[sh] for sh in arm_shots])
+        for k, sh in enumerate(arm_shots):
+            ss.set_gather(k, gathers[sh])
+        stream = torch.cuda.ExternalStream(ss.stream())
+        ss.run_range(0, warm)
+        ss.reset_images()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        st = ss.run_range(0, len(arm_shots))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ss.close()
+        w = sum(w_of(sh) for sh in arm_shots)
+        return {"shots": len(arm_shots), "seconds": round(ms * 1e-3, 3),
+                "shots_per_s": round(len(arm_shots) / (ms * 1e-3), 4),
+                "gcell_updates_per_s": round(w / (ms * 1e-3) * 1e-9, 3),
+                "mean_cell_updates_per_shot": w / len(arm_shots), "batches": st.batches,
+                "kernel_launches": st.kernel_launches}
+
+    batched = timed(G.RunOptions(device=local_rank, strip_precision="fp16", gather_precision="fp16",
+                                 accum_fp64=True), shots, 4)
+    sample = shots[args.headline_sample // 2::args.headline_sample]
+    plain = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), sample, 1)
+    nog = sample[:8]
+    plain_nograph = timed(G.RunOptions(device=local_rank, batch=1), nog, 1)
+    # the graph arm on the same 8 shots, for the launch-gap comparison
+    plain_graph8 = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), nog, 1)
+    ap = meta["apertures"]
+    return {"workload": ("config 4: 3201x801 grid (10 m), 40-cell PML, nt=%d, dt=0.8 ms, 20 Hz Ricker, 256 shots, "
+                         "apertures drawn from %d-%d columns (layout-1 windows cut at the model's edges), "
+                         "gradient + random-field model, gathers modelled by this library before timing"
+                         % (s.nt, min(ap.values()), max(ap.values()))),
+            "batched_mixed": {**batched, "form": "fp16 strips + fp16 gathers + fp64 images, all 256 shots, "
+                                                   "as many per launch as fit"},
+            "plain_fp32_per_shot": {**plain, "form": "fp32, one shot per launch, CUDA graph per pass",
+                                    "sample": f"every {args.headline_sample}th shot ({len(sample)} shots)"},
+            "plain_fp32_per_shot_no_graph": {**plain_nograph, "form": "fp32, one shot per launch, direct launches",
+                                             "sample": f"the first {len(nog)} shots of that sample"},
+            "plain_fp32_per_shot_graph_same_8": plain_graph8,
+            "ratio": round(batched["gcell_updates_per_s"] / plain["gcell_updates_per_s"], 3),
+            "ratio_basis": "Gcell-updates/s (shots/s at equal work per shot)",
+            "target": 3.0, "setup_seconds_data_modelling": round(t_data, 2)}
+
+
+# ------------------------------------------------------------------------------------------
 REAL_WORKLOAD = ("recorded-data path on the configuration-2 model (1701x351, dx=dz=12.5 m, 50-cell PML, nt=4000 at "
                  "1 ms): 64 off-end shots every 200 m, 241 receivers from 0 to 6000 m every 25 m, 2000 samples at "
                  "2 ms, one SU file; per shot F-K (x2) + windowed-sinc (x2) resampling to 481 traces x 4000 samples, "
@@ -573,6 +667,10 @@ def main():
     if args.workload == "real":
         run_real(args, rank, world, local_rank)
         return
+    if args.headline_only:
+        if rank == 0:
+            print(json.dumps({"headline": run_headline(args, local_rank)}), flush=True)
+        return
     r = run_ours(args, rank, world, local_rank)
     if r is None or rank != 0:
         return
@@ -583,6 +681,9 @@ def main():
 
         _, _, _, v_mig, rho, _ = synthetic.config(args.config, nt=args.nt or None)
         cpu = cpu_sample(args, s, v_mig, rho, r["all_shots"], r["meta"], r["w_shot"])
+    headline = None
+    if world == 1 and not args.no_headline and args.config == 2 and not args.profile_only:
+        headline = run_headline(args, local_rank)
     dtype = "f32" if args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64 else \
         f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {'f64' if args.accum_fp64 else 'f32'} images"
     ws_gb = r["shots_per_launch"] * 12 * r["X"] * r["Z"] * 4 / 1e9
@@ -598,6 +699,8 @@ def main():
             "gcell_updates_per_s": r["gcell"],
             "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
             "clocks": r["clocks"], "setup_seconds_data_modelling": round(r["t_data"], 2)}
+    if headline is not None:
+        line["headline"] = headline
     print(json.dumps(line), flush=True)
 
 

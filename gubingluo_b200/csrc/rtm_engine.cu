@@ -131,6 +131,9 @@ struct rtm_session {
     // rows per tile (measured): 32 for the forward and receiver velocity kernels, 16 for the
     // velocity reconstruction and the pressure kernels
     int bz_vel = 32, bz_vel_recon = 16, bz_pres = 16;
+    // kernel form: four columns by U rows per thread (rtm_stencil_v.cu, default) or one column
+    // per thread (rtm_stencil.cu, RTM_B200_KERNELS=scalar); the results are the same bits
+    bool vec = true;
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -422,6 +425,11 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         if (e && *e) ss->bz_vel_recon = std::atoi(e);
         e = std::getenv("RTM_B200_BZ_PRES");
         if (e && *e) ss->bz_pres = std::atoi(e);
+        e = std::getenv("RTM_B200_KERNELS");
+        if (e && *e) {
+            if (!std::strcmp(e, "scalar")) ss->vec = false;
+            else if (std::strcmp(e, "vector")) return fail(RTM_ERR_ARG, "RTM_B200_KERNELS must be scalar or vector");
+        }
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
         for (int bz : {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres})
             if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
@@ -794,12 +802,24 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     return RTM_OK;
 }
 
+// Stencil launches in the session's kernel form.
+static void vel_step(rtm_session *ss, int mode, int bz, const StepArgs &a, int ntiles)
+{
+    if (ss->vec) launch_vel4(mode, bz, a, ntiles, ss->stream);
+    else launch_vel(mode, bz, a, ntiles, ss->stream);
+}
+static void pres_step(rtm_session *ss, int mode, int bz, const StepArgs &a, int ntiles, int record)
+{
+    if (ss->vec) launch_pres4(mode, bz, a, ntiles, record, ss->stream);
+    else launch_pres(mode, bz, a, ntiles, record, ss->stream);
+}
+
 // Full-grid pressure update of one step (interior tiles are flagged in the tile list).
 static void launch_pres_tiles(rtm_session *ss, BatchRun &br, int mode, int record)
 {
     StepArgs &a = br.a;
     a.tiles = ss->d_tiles_p;
-    launch_pres(mode, ss->bz_pres, a, br.ntiles_p, record, ss->stream);
+    pres_step(ss, mode, ss->bz_pres, a, br.ntiles_p, record);
     ss->launches++;
 }
 
@@ -896,7 +916,7 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
             cudaEvent_t e;
             timing_begin(ss, "vel_fwd", it, &e);
             a.tiles = ss->d_tiles;
-            launch_vel(mode, ss->bz_vel, a, br.ntiles, st);
+            vel_step(ss, mode, ss->bz_vel, a, br.ntiles);
             timing_end(ss, e);
             timing_begin(ss, "pres_fwd", it, &e);
             launch_pres_tiles(ss, br, mode, record ? 1 : 0);
@@ -992,15 +1012,15 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             // (which reads the reconstructed pressure of the same step)
             timing_begin(ss, "vel_recon", it, &e);
             a.tiles = ss->d_tiles_r;
-            launch_vel(RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r, st);
+            vel_step(ss, RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r);
             timing_end(ss, e);
             timing_begin(ss, "pres_recon", it, &e);
             a.tiles = ss->d_tiles_pr;
-            launch_pres(RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0, st);
+            pres_step(ss, RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0);
             timing_end(ss, e);
             timing_begin(ss, "vel_recv", it, &e);
             a.tiles = ss->d_tiles;
-            launch_vel(RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles, st);
+            vel_step(ss, RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles);
             timing_end(ss, e);
             timing_begin(ss, "pres_recv", it, &e);
             launch_pres_tiles(ss, br, RTM_WAVE_RECEIVER, 0);

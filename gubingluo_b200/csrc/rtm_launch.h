@@ -8,6 +8,10 @@
 // list built for that bz.
 void launch_vel(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s);
 void launch_pres(int mode, int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s);
+// The same launches with four columns by U rows per thread (rtm_stencil_v.cu): same tile
+// lists, staged boxes and results, 32 * bz / U threads per block.
+void launch_vel4(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s);
+void launch_pres4(int mode, int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s);
 void launch_setup_pml(float *pml, int X, int Z, int npml, float dx, float dz, float dt, float vpmax, cudaStream_t s);
 void launch_setup_source(float *src, int sbx0, int sbz0, int sbnx, int sbnz, int nsx, int nsz, float amp, float alp,
                          float dx2, float dz2, float dt, cudaStream_t s);

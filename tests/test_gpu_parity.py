@@ -496,3 +496,35 @@ def test_graph_replay_is_bitwise_identical(rtmlib, strips):
     for a, b in zip(got["gathers"], want["gathers"]):
         assert np.array_equal(a, b)
     assert got["stats"].kernel_launches == want["stats"].kernel_launches
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["fp32", "fp64", "fp16"])
+def test_vector_kernel_form_is_bitwise_identical(rtmlib, monkeypatch, form):
+    """The four-columns-by-U-rows kernels (default) give the bits of the one-column kernels
+    (RTM_B200_KERNELS=scalar): gathers and images of the general cases (partial tiles, npml
+    13-40, layouts 1-4, receivers below z = 0), at every tile height, with fp64 accumulators
+    and the other imaging conditions, and with packed strips and gathers."""
+    G = rtmlib
+    opts = dict(fp32=dict(), fp64=dict(accum_fp64=True, extra_images=1),
+                fp16=dict(strip_precision="fp16", gather_precision="fp16"))[form]
+    heights = [(None, None, None), ("16", "32", "32"), ("8", "8", "8")]
+    for ci, c in enumerate(GENERAL):
+        v, rho = _random_model(c["nz"], c["nx"], 20 + ci)
+        shots = list(range(1, c["nshot"] + 1))
+        s = cfg_from(G, _survey(c, 0))
+        for vel, recon, pres in heights[:1] if ci else heights:
+            for k, val in (("RTM_B200_BZ_VEL", vel), ("RTM_B200_BZ_VEL_RECON", recon), ("RTM_B200_BZ_PRES", pres)):
+                if val is None:
+                    monkeypatch.delenv(k, raising=False)
+                else:
+                    monkeypatch.setenv(k, val)
+            monkeypatch.setenv("RTM_B200_KERNELS", "scalar")
+            want = G.migrate(s, G.RunOptions(**opts), shots, v, rho)
+            monkeypatch.setenv("RTM_B200_KERNELS", "vector")
+            got = G.migrate(s, G.RunOptions(**opts), shots, v, rho)
+            keys = ["image1", "image2s", "illum"] + (["image3s", "image4s", "image5s"] if form == "fp64" else [])
+            for k in keys:
+                assert np.array_equal(got[k], want[k]), (ci, vel, k)
+            for a, b in zip(got["gathers"], want["gathers"]):
+                assert np.array_equal(a, b), (ci, vel)
