@@ -306,6 +306,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
     kern = {k: ss.kernel_ms(k) for k in ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv")}
+    tiles = ss.tile_heights()
     if args.profile_only:
         ss.close()
         return None
@@ -373,7 +374,7 @@ def run_ours(args, rank, world, local_rank):
                 "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 4),
                 "launches_sampled": sampled[dom][1],
                 "kernel_ms": {k: round(v[0], 4) for k, v in sampled.items()}}
-    return dict(value=value, gcell=gcell, ms_total=ms_total, launches=launches, e2e=e2e, roofline=roofline,
+    return dict(value=value, gcell=gcell, ms_total=ms_total, launches=launches, e2e=e2e, roofline=roofline, tiles=tiles,
                 clocks=clock_info, shots_done=shots_done, t_data=t_data, X=X, Z=Z, nxi=nxi, nzi=nzi, nrec=nrec,
                 w_shot=w_timed / (K * B), s=s, shots_per_launch=nshots_launch, meta=meta, all_shots=all_shots)
 
@@ -695,6 +696,7 @@ def main():
                        "shots_per_step_per_gpu": args.shots_per_step,
                        "shots_per_launch": r["shots_per_launch"], "nt": s.nt,
                        "parallelism": f"shots sharded over {world} GPU(s)",
+                       "tile_rows": r["tiles"],
                        "l2": f"inputs larger than L2: per-launch wavefield+model working set {ws_gb:.1f} GB vs 126 MB L2"},
             "gcell_updates_per_s": r["gcell"],
             "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],

@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
     L.rtm_session_reset_images.argtypes = [vp]
     L.rtm_session_nrec.argtypes = [vp, C.c_int]
     L.rtm_session_get_pml.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.rtm_session_tile_heights.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.rtm_session_stream.argtypes = [vp]
     L.rtm_session_stream.restype = vp
     L.rtm_session_kernel_ms.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int)]
@@ -350,6 +351,12 @@ class Session:
         n = C.c_int(0)
         ms = lib().rtm_session_kernel_ms(self.h, name.encode(), C.byref(n))
         return ms, n.value
+
+    def tile_heights(self):
+        """Rows per tile in use: {"vel", "vel_recon", "pres"} (tuned per launch shape)."""
+        v = [C.c_int(0) for _ in range(3)]
+        _check(lib().rtm_session_tile_heights(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("vel", "vel_recon", "pres"), [x.value for x in v]))
 
     def pml_profiles(self, k: int, X: int, Z: int):
         """Shot k's device PML damping profiles (ddx [X], ddz [Z], ddxvx [X-1], ddzvz [Z-1])."""

@@ -7,6 +7,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -134,6 +135,7 @@ struct rtm_session {
     // kernel form: four columns by U rows per thread (rtm_stencil_v.cu, default) or one column
     // per thread (rtm_stencil.cu, RTM_B200_KERNELS=scalar); the results are the same bits
     bool vec = true;
+    bool tune = true;                // choose the tile heights per launch shape by timing them
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -425,6 +427,10 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         if (e && *e) ss->bz_vel_recon = std::atoi(e);
         e = std::getenv("RTM_B200_BZ_PRES");
         if (e && *e) ss->bz_pres = std::atoi(e);
+        // tile heights set by hand turn the tuner off; so does RTM_B200_TUNE=0
+        for (const char *v : {"RTM_B200_BZ_VEL", "RTM_B200_BZ_VEL_RECON", "RTM_B200_BZ_PRES"})
+            if ((e = std::getenv(v)) && *e) ss->tune = false;
+        if ((e = std::getenv("RTM_B200_TUNE")) && *e && std::atoi(e) == 0) ss->tune = false;
         e = std::getenv("RTM_B200_KERNELS");
         if (e && *e) {
             if (!std::strcmp(e, "scalar")) ss->vec = false;
@@ -587,8 +593,9 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         }
     }
     CK(cudaMemsetAsync(ss->d_err, 0, sizeof(int), ss->stream));
-    const int bz_min = std::min(std::min(ss->bz_vel, ss->bz_vel_recon), ss->bz_pres);
-    int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX) * ((big.Z + bz_min - 1) / bz_min);
+    // tile tables sized for the shortest tile height the tuner or the environment may choose
+    const int bz_min = 8;
+    int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX + 1) * ((big.Z + bz_min - 1) / bz_min + 1);
     ss->max_tiles = tiles_per_shot * B;
     ss->d_tiles = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_tiles_p = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
@@ -776,6 +783,8 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.ntiles_p = (int)tiles_p.size();
     br.ntiles_r = (int)tiles_r.size();
     br.ntiles_pr = (int)tiles_pr.size();
+    if (std::max(std::max(br.ntiles, br.ntiles_p), std::max(br.ntiles_r, br.ntiles_pr)) > ss->max_tiles)
+        return fail(RTM_ERR_ARG, "tile table overflow");
     CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles, tiles.data(), sizeof(TileRef) * br.ntiles, cudaMemcpyHostToDevice, st));
@@ -936,7 +945,8 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
         loop();
         CK(cudaGetLastError());
     } else {
-        int rc = run_pass(ss, {0, br.n, br.ntiles, br.ntiles_p, br.max_strip_len, nsteps, save, record}, loop);
+        int rc = run_pass(ss, {0, br.n, br.ntiles, br.ntiles_p, br.max_strip_len, nsteps, save, record, ss->bz_vel,
+                               ss->bz_pres, ss->vec}, loop);
         if (rc) {
             nvtxRangePop();
             return rc;
@@ -1038,7 +1048,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         CK(cudaGetLastError());
     } else {
         int rc = run_pass(ss, {1, n, br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr, max_nxi, max_nzi,
-                               a.gather_prec}, loop);
+                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->vec}, loop);
         if (rc) {
             nvtxRangePop();
             return rc;
@@ -1072,10 +1082,140 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     return RTM_OK;
 }
 
+// ---- tile-height tuner ---------------------------------------------------------------
+// The stencil kernels take 8-, 16- or 32-row tiles; which is fastest depends on the grid
+// (partial tiles, the share of PML-band and edge tiles), on the shots per launch (blocks to
+// fill 148 SMs) and on the kernel form.  Before the first batch of a launch shape, each height
+// is timed on that batch's own buffers: two untimed and four timed source-pass steps (velocity
+// and pressure) and backward steps (reconstruction and receiver pass) with CUDA events per
+// kernel, no strips saved.  Each kernel family keeps its fastest height: forward and receiver
+// velocity (bz_vel), reconstruction velocity (bz_vel_recon), pressure (bz_pres).  The batch is
+// set up again afterwards, so the trial steps leave nothing behind; tile heights do not change
+// the results (tested bit for bit).  Choices are kept per process by launch shape and, with
+// RTM_B200_TUNE_CACHE=<file>, in that file ("key vel vel_recon pres" lines) across processes.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, std::array<int, 3>> g_tune;
+bool g_tune_loaded = false;
+}  // namespace
+
+static std::string tune_key(rtm_session *ss, int k0, int n)
+{
+    int xmax = 0;
+    for (int j = 0; j < n; j++) xmax = std::max(xmax, ss->shots[k0 + j].X);
+    char b[200];
+    std::snprintf(b, sizeof b, "%s/X%d/Z%d/npml%d/n%d/strip%d/gather%d/acc%d/extra%d/mode%d", ss->vec ? "vector" : "scalar",
+                  xmax, ss->shots[k0].Z, ss->s.npml, n, ss->o.strip_precision, ss->o.gather_precision, ss->o.accum_fp64,
+                  ss->o.extra_images, ss->s.mode);
+    return b;
+}
+
+static int tune_heights(rtm_session *ss, int k0, int n)
+{
+    if (!ss->tune) return RTM_OK;
+    const std::string key = tune_key(ss, k0, n);
+    const char *path = std::getenv("RTM_B200_TUNE_CACHE");
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        if (!g_tune_loaded && path && *path) {
+            g_tune_loaded = true;
+            if (FILE *f = std::fopen(path, "r")) {
+                char k[200];
+                int v[3];
+                while (std::fscanf(f, "%199s %d %d %d", k, &v[0], &v[1], &v[2]) == 4) g_tune[k] = {v[0], v[1], v[2]};
+                std::fclose(f);
+            }
+        }
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            ss->bz_vel = it->second[0];
+            ss->bz_vel_recon = it->second[1];
+            ss->bz_pres = it->second[2];
+            return RTM_OK;
+        }
+    }
+    const int cand[3] = {8, 16, 32};
+    const char *names[6] = {"vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv"};
+    double ms[3][6] = {};
+    cudaEvent_t ev[2][6][4];
+    for (auto &a : ev)
+        for (auto &b : a)
+            for (auto &e : b) CK(cudaEventCreate(&e));
+    cudaStream_t st = ss->stream;
+    int rc = RTM_OK;
+    const int steps = 6, warm = 2;
+    for (int c = 0; c < 3 && rc == RTM_OK; c++) {
+        ss->bz_vel = ss->bz_vel_recon = ss->bz_pres = cand[c];
+        BatchRun br;
+        if ((rc = batch_setup(ss, k0, n, br))) break;
+        StepArgs a = br.a;
+        for (int it = 0; it < steps; it++) {
+            const int t = it - warm;
+            a.it = std::min(it + 1, ss->s.nt - 2);
+            auto rec = [&](int k, int side) {
+                if (t >= 0) cudaEventRecord(ev[side][k][t], st);
+            };
+            rec(0, 0); a.tiles = ss->d_tiles; vel_step(ss, RTM_WAVE_FWD, ss->bz_vel, a, br.ntiles); rec(0, 1);
+            rec(1, 0); a.tiles = ss->d_tiles_p; pres_step(ss, RTM_WAVE_FWD, ss->bz_pres, a, br.ntiles_p, 0); rec(1, 1);
+            rec(2, 0); a.tiles = ss->d_tiles_r; vel_step(ss, RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r); rec(2, 1);
+            rec(3, 0); a.tiles = ss->d_tiles_pr; pres_step(ss, RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0); rec(3, 1);
+            rec(4, 0); a.tiles = ss->d_tiles; vel_step(ss, RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles); rec(4, 1);
+            rec(5, 0); a.tiles = ss->d_tiles_p; pres_step(ss, RTM_WAVE_RECEIVER, ss->bz_pres, a, br.ntiles_p, 0); rec(5, 1);
+        }
+        ss->launches += 6 * steps;
+        if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = fail(RTM_ERR_CUDA, "tile-height trial launches failed");
+            break;
+        }
+        for (int k = 0; k < 6; k++)
+            for (int t = 0; t < steps - warm; t++) {
+                float m = 0.f;
+                cudaEventElapsedTime(&m, ev[0][k][t], ev[1][k][t]);
+                ms[c][k] += m;
+            }
+    }
+    for (auto &a : ev)
+        for (auto &b : a)
+            for (auto &e : b) cudaEventDestroy(e);
+    if (rc) return rc;
+    if ((rc = check_kernel_flag(ss))) return rc;
+    auto best = [&](std::initializer_list<int> ks) {
+        int bi = 0;
+        double bm = 1e300;
+        for (int c = 0; c < 3; c++) {
+            double m = 0;
+            for (int k : ks) m += ms[c][k];
+            if (m < bm) bm = m, bi = c;
+        }
+        return cand[bi];
+    };
+    std::array<int, 3> pick = {best({0, 4}), best({2}), best({1, 3, 5})};
+    ss->bz_vel = pick[0];
+    ss->bz_vel_recon = pick[1];
+    ss->bz_pres = pick[2];
+    if (ss->o.verbose) {
+        std::printf("rtm_b200: tile heights for %s: vel %d, vel_recon %d, pres %d (ms per 4 steps:", key.c_str(), pick[0],
+                    pick[1], pick[2]);
+        for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 6; k++) std::printf(" %s@%d=%.3f", names[k], cand[c], ms[c][k]);
+        std::printf(")\n");
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = pick;
+    if (path && *path)
+        if (FILE *f = std::fopen(path, "a")) {
+            std::fprintf(f, "%s %d %d %d\n", key.c_str(), pick[0], pick[1], pick[2]);
+            std::fclose(f);
+        }
+    return RTM_OK;
+}
+
 static int run_batch(rtm_session *ss, int k0, int n)
 {
     BatchRun br;
-    int rc = batch_setup(ss, k0, n, br);
+    int rc = tune_heights(ss, k0, n);
+    if (rc) return rc;
+    rc = batch_setup(ss, k0, n, br);
     if (rc) return rc;
     nvtxRangePushA("rtm: batch");
     if (!(rc = batch_forward(ss, br, ss->s.nt, true, ss->s.mode == 0))) rc = batch_backward(ss, br);
@@ -1298,6 +1438,15 @@ int rtm_session_get_pml(rtm_session *ss, int k, float *ddx, float *ddz, float *d
         {ddx, o.ddx, sh.X}, {ddz, o.ddz, sh.Z}, {ddxvx, o.ddxvx, sh.X - 1}, {ddzvz, o.ddzvz, sh.Z - 1}};
     for (const auto &q : part)
         if (q.out) CK(cudaMemcpy(q.out, sh.pml + q.off, sizeof(float) * q.n, cudaMemcpyDeviceToHost));
+    return RTM_OK;
+}
+
+int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres)
+{
+    if (!ss) return fail(RTM_ERR_ARG, "null session");
+    if (bz_vel) *bz_vel = ss->bz_vel;
+    if (bz_vel_recon) *bz_vel_recon = ss->bz_vel_recon;
+    if (bz_pres) *bz_pres = ss->bz_pres;
     return RTM_OK;
 }
 

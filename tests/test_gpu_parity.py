@@ -528,3 +528,33 @@ def test_vector_kernel_form_is_bitwise_identical(rtmlib, monkeypatch, form):
                 assert np.array_equal(got[k], want[k]), (ci, vel, k)
             for a, b in zip(got["gathers"], want["gathers"]):
                 assert np.array_equal(a, b), (ci, vel)
+
+
+@pytest.mark.gpu
+def test_tile_height_tuner(rtmlib, monkeypatch, tmp_path):
+    """The tuner times 8-, 16- and 32-row tiles before the first batch of a launch shape,
+    keeps a height per kernel family, records it in RTM_B200_TUNE_CACHE, and changes no bit
+    of the results (RTM_B200_TUNE=0 runs the default heights)."""
+    G = rtmlib
+    c = dict(GENERAL[1], nx=97)   # a launch shape no other test uses
+    v, rho = _random_model(c["nz"], c["nx"], 31)
+    shots = list(range(1, c["nshot"] + 1))
+    s = cfg_from(G, _survey(c, 0))
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("RTM_B200_TUNE_CACHE", str(cache))
+    for k in ("RTM_B200_BZ_VEL", "RTM_B200_BZ_VEL_RECON", "RTM_B200_BZ_PRES", "RTM_B200_TUNE"):
+        monkeypatch.delenv(k, raising=False)
+    with G.Session(s, G.RunOptions(), shots, v, rho) as ss:
+        ss.run()
+        h = ss.tile_heights()
+        tuned = ss.images()
+        gathers = [ss.gather(k) for k in range(len(shots))]
+    assert set(h.values()) <= {8, 16, 32}
+    lines = cache.read_text().split("\n")
+    assert any(ln.split()[1:] == [str(h["vel"]), str(h["vel_recon"]), str(h["pres"])] for ln in lines if ln), lines
+    monkeypatch.setenv("RTM_B200_TUNE", "0")
+    want = G.migrate(s, G.RunOptions(), shots, v, rho)
+    for k in ("image1", "image2s", "illum"):
+        assert np.array_equal(tuned[k], want[k]), k
+    for a, b in zip(gathers, want["gathers"]):
+        assert np.array_equal(a, b)
