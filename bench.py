@@ -50,7 +50,7 @@ MODEL_TEXT = {1: "four flat layers and a dipping 3500 m/s wedge",
 
 def workload_text(args, s, shots, meta):
     """The workload of a --config run (configuration 2's text is WORKLOAD)."""
-    fp32 = args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64
+    fp32 = args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64 and not args.accum_kahan
     if args.config == 2 and s.nt == 4000 and fp32:
         return WORKLOAD
     X, Z = s.nx + 2 * s.npml, s.nz + 2 * s.npml
@@ -62,7 +62,8 @@ def workload_text(args, s, shots, meta):
         spread = "full spread" if s.layout == 2 else f"layout {s.layout}"
     form = "FP32 stencil/strips/gathers/accumulators" if fp32 else (
         f"FP32 stencil, {args.strips} strips, {args.gathers} gathers, "
-        f"{'FP64' if args.accum_fp64 else 'FP32'} accumulators")
+        f"{'compensated FP32 pair (Kahan)' if args.accum_kahan else 'FP64' if args.accum_fp64 else 'FP32'} "
+        f"accumulators")
     return (f"config {args.config}: {s.nx}x{s.nz} grid (X x Z = {X} x {Z} padded), dx=dz={s.dx:g} m, "
             f"{s.npml}-cell PML, nt={s.nt}, dt={s.dt * 1e3:g} ms, {s.fdom:g} Hz Ricker, {len(shots)} shots "
             f"({spread}), source-illumination-normalised imaging, {form}")
@@ -87,6 +88,8 @@ def parse():
     ap.add_argument("--strips", default="fp32", choices=["fp32", "fp16", "bf16"])
     ap.add_argument("--gathers", default="fp32", choices=["fp32", "fp16", "bf16"])
     ap.add_argument("--accum-fp64", action="store_true")
+    ap.add_argument("--accum-kahan", action="store_true",
+                    help="per-shot accumulation in compensated fp32 pairs, stacked in fp64")
     ap.add_argument("--cpu-sample-steps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -240,7 +243,7 @@ def run_ours(args, rank, world, local_rank):
     uniq = mine[: min(len(mine), need)]
     step_shots = [uniq[(i * B + j) % len(uniq)] for i in range(K + W) for j in range(B)]
     opts = G.RunOptions(device=local_rank, strip_precision=args.strips, gather_precision=args.gathers,
-                        accum_fp64=args.accum_fp64, batch=args.batch or B)
+                        accum_fp64=2 if args.accum_kahan else int(args.accum_fp64), batch=args.batch or B)
     # ---- synthetic data: model this rank's gathers in the true model (untimed setup)
     t0 = time.time()
     s_model = G.SurveyConfig(**{**s.__dict__, "mode": 0})
@@ -264,7 +267,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ss.stream())
     ptrs = ss.image_ptrs()
     npix = s.nx * s.nz
-    typestr = "<f8" if args.accum_fp64 else "<f4"
+    typestr = "<f8" if (args.accum_fp64 or args.accum_kahan) else "<f4"
     img_views = [torch.as_tensor(_CudaArray(ptrs[k], npix, typestr), device=f"cuda:{local_rank}")
                  for k in ("image1", "image2s", "illum")] if dist else []
 
@@ -355,7 +358,7 @@ def run_ours(args, rank, world, local_rank):
     ss.close()
 
     # ---- roofline of the dominant kernel
-    accum_bytes = 8 if args.accum_fp64 else 4
+    accum_bytes = 8 if (args.accum_fp64 or args.accum_kahan) else 4
     sampled = {k: v for k, v in kern.items() if v[0] > 0}
     dom = max(sampled, key=lambda k: sampled[k][0])
     launch_ms = sampled[dom][0]
@@ -685,8 +688,9 @@ def main():
     headline = None
     if world == 1 and not args.no_headline and args.config == 2 and not args.profile_only:
         headline = run_headline(args, local_rank)
-    dtype = "f32" if args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64 else \
-        f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {'f64' if args.accum_fp64 else 'f32'} images"
+    acc_txt = "kahan-f32 images" if args.accum_kahan else "f64 images" if args.accum_fp64 else "f32 images"
+    dtype = "f32" if acc_txt == "f32 images" and args.strips == "fp32" and args.gathers == "fp32" else \
+        f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {acc_txt}"
     ws_gb = r["shots_per_launch"] * 12 * r["X"] * r["Z"] * 4 / 1e9
     line = {"metric": "shots/s", "value": r["value"], "unit": "shots/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_total"] / args.steps, "higher_is_better": True,

@@ -211,7 +211,7 @@ class RunOptions:
     device: int = 0
     strip_precision: str = "fp32"
     gather_precision: str = "fp32"
-    accum_fp64: bool = False
+    accum_fp64: int = 0     # 0 fp32, 1 (or True) fp64, 2 compensated fp32 pairs; 1 and 2 stack in fp64
     batch: int = 0
     use_graph: bool = False
     verbose: bool = False

@@ -437,6 +437,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             else if (std::strcmp(e, "vector")) return fail(RTM_ERR_ARG, "RTM_B200_KERNELS must be scalar or vector");
         }
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
+        if (o.accum_fp64 < 0 || o.accum_fp64 > 2) return fail(RTM_ERR_ARG, "accum_fp64 must be 0, 1 or 2");
         for (int bz : {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres})
             if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
     }
@@ -1066,7 +1067,8 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         int nwin = 50;   // rtm_model.cu:70, :464-465
         while (2 * nwin >= sh.nxi) nwin -= 3;
         fill_finalize_shot(fin.data() + j * finalize_shot_size(), ss->slots[j].g1, ss->slots[j].illum,
-                           o.extra_images ? ss->slots[j].gx : nullptr, sh.g.nx1, sh.nxi, nwin, sh.pitch, s.npml);
+                           o.extra_images ? ss->slots[j].gx : nullptr, sh.g.nx1, sh.nxi, nwin, sh.pitch, s.npml,
+                           o.accum_fp64);
     }
     CK(cudaMemcpyAsync(ss->d_fin, fin.data(), fin.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ss->d_nonfinite, 0x7f, sizeof(int), st));   // 0x7f7f7f7f: none

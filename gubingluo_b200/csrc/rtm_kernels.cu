@@ -239,7 +239,19 @@ struct FinalizeShot {
     const void *g1, *illum;   // [Z][pitch]: interior cell (iz, lx) at (iz+npml)*pitch + lx+npml
     const void *gx[4];        // the other imaging conditions' g2, g3, g3t, g4 (null when off)
     int nx1, nxi, nwin, pitch, npml;
+    int acc;                  // RtmAccum of g1 and illum (fp32, fp64 or compensated fp32 pairs)
 };
+
+// Value of a per-shot accumulator cell: fp32, fp64, or a compensated pair (s - c in double).
+__device__ __forceinline__ double acc_value(const void *a, size_t ip, int acc)
+{
+    if (acc == RTM_ACC_FP64) return ((const double *)a)[ip];
+    if (acc == RTM_ACC_KAHAN) {
+        const float2 v = ((const float2 *)a)[ip];
+        return (double)v.x - (double)v.y;
+    }
+    return ((const float *)a)[ip];
+}
 
 // Taper weight of interior column lx (cuda_taper_calculate, kernel.cu:1591-1604).
 __device__ __forceinline__ float taper_at(int lx, int nwin, int nxl)
@@ -268,8 +280,8 @@ __global__ void k_finalize(const FinalizeShot *fs, int nshots, int nx, int nz, i
             const float tp = taper_at(lx, f.nwin, f.nxi);
             const size_t ip = (size_t)(iz + f.npml) * f.pitch + lx + f.npml;
             if (fp64) {
-                double g = ((const double *)f.g1)[ip] * (double)tp;
-                double il = ((const double *)f.illum)[ip] * (double)tp;
+                double g = acc_value(f.g1, ip, f.acc) * (double)tp;
+                double il = acc_value(f.illum, ip, f.acc) * (double)tp;
                 if (!isfinite(g) || !isfinite(il)) bad = min(bad, s);
                 ((double *)image2s)[i] += g / (il + 1.0e-6);
                 ((double *)image1)[i] += g;
@@ -337,7 +349,7 @@ __global__ void k_finalize_extra(const FinalizeShot *fs, int nshots, int nx, int
             if (lx < 0 || lx >= f.nxi) continue;
             const T tp = (T)taper_at(lx, f.nwin, f.nxi);
             const size_t ip = (size_t)(iz + f.npml) * f.pitch + lx + f.npml;
-            const T il = ((const T *)f.illum)[ip] * tp;
+            const T il = (T)acc_value(f.illum, ip, f.acc) * tp;
             const T g[4] = {((const T *)f.gx[0])[ip] * tp, ((const T *)f.gx[1])[ip] * tp,
                             ((const T *)f.gx[2])[ip] * tp, ((const T *)f.gx[3])[ip] * tp};
             const int gi[3] = {0, 1, 3};   // g2 -> image3, g3 -> image4, g4 -> image5
@@ -516,9 +528,10 @@ void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float d
 }
 size_t finalize_shot_size() { return sizeof(FinalizeShot); }
 void fill_finalize_shot(void *dst, const void *g1, const void *illum, const void *const *gx, int nx1, int nxi,
-                        int nwin, int pitch, int npml)
+                        int nwin, int pitch, int npml, int acc)
 {
     FinalizeShot f;
+    f.acc = acc;
     f.g1 = g1;
     f.illum = illum;
     for (int k = 0; k < 4; k++) f.gx[k] = gx ? gx[k] : nullptr;

@@ -30,7 +30,7 @@ void launch_absmax(const ShotDev *shots, int nshots, int side, unsigned *out, cu
 void launch_inject(const ShotDev *shots, int nshots, int maxrec, int it, float dt, int gather_prec, cudaStream_t s);
 size_t finalize_shot_size();
 void fill_finalize_shot(void *dst, const void *g1, const void *illum, const void *const *gx, int nx1, int nxi,
-                        int nwin, int pitch, int npml);
+                        int nwin, int pitch, int npml, int acc);
 void launch_image_extra(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, int parity, int fp64,
                         float dx, float dz, float dt, cudaStream_t s);
 void launch_finalize_extra(const void *fs, int nshots, int nx, int nz, int fp64, void *const img[7], cudaStream_t s);

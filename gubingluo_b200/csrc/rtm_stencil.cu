@@ -492,8 +492,12 @@ template <int BZ, int MODE>
 static void pres_launch(const StepArgs &a, int ntiles, int record, cudaStream_t s)
 {
     if constexpr (MODE == 2) {
-        if (a.accum_fp64) {
+        if (a.accum_fp64 == RTM_ACC_FP64) {
             pres_launch_t<BZ, MODE, double>(a, ntiles, record, s);
+            return;
+        }
+        if (a.accum_fp64 == RTM_ACC_KAHAN) {
+            pres_launch_t<BZ, MODE, KahanAcc>(a, ntiles, record, s);
             return;
         }
     }

@@ -144,6 +144,22 @@ template <typename ACC>
 __device__ __forceinline__ ACC image_g1(ACC og1, float ps, float pn) { return og1 + (ACC)ps * (ACC)pn; }
 template <typename ACC>
 __device__ __forceinline__ ACC image_il(ACC oil, float ps) { return oil + (ACC)ps * (ACC)ps; }
+// Compensated fp32 accumulator (Kahan): the running sum s and the compensation c, whose
+// negative is the low-order part lost so far, so the sum is s - c.  Each term enters as
+// fma(a, b, -c), the product exact before its one rounding.
+__device__ __forceinline__ KahanAcc kahan_add(KahanAcc o, float a, float b)
+{
+    const float y = __fmaf_rn(a, b, -o.c);
+    const float t = __fadd_rn(o.s, y);
+    KahanAcc r;
+    r.c = __fsub_rn(__fsub_rn(t, o.s), y);
+    r.s = t;
+    return r;
+}
+template <>
+__device__ __forceinline__ KahanAcc image_g1<KahanAcc>(KahanAcc og1, float ps, float pn) { return kahan_add(og1, ps, pn); }
+template <>
+__device__ __forceinline__ KahanAcc image_il<KahanAcc>(KahanAcc oil, float ps) { return kahan_add(oil, ps, ps); }
 template <typename ACC>
 __device__ __forceinline__ void image_cell(ACC *__restrict__ g1p, ACC *__restrict__ ilp, unsigned id, ACC og1, ACC oil,
                                            float ps, float pn)

@@ -18,6 +18,7 @@
 // damp, vel_inc, p_interior, p_recon, image_cell).  The reference kernels these replace are
 // listed in rtm_stencil.cu.
 #include <atomic>
+#include <type_traits>
 
 #include "rtm_launch.h"
 #include "rtm_stencil_common.cuh"
@@ -43,7 +44,11 @@ __device__ __forceinline__ float4 f4(const float (&a)[4]) { return make_float4(a
 template <typename ACC>
 __device__ __forceinline__ void ld_acc4(const ACC *p, ACC (&o)[4])
 {
-    if constexpr (sizeof(ACC) == 4) {
+    if constexpr (std::is_same<ACC, KahanAcc>::value) {
+        const float4 a = ld4((const float *)p), b = ld4((const float *)p + 4);
+        o[0].s = a.x; o[0].c = a.y; o[1].s = a.z; o[1].c = a.w;
+        o[2].s = b.x; o[2].c = b.y; o[3].s = b.z; o[3].c = b.w;
+    } else if constexpr (sizeof(ACC) == 4) {
         const float4 v = ld4((const float *)p);
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
     } else {
@@ -55,7 +60,10 @@ __device__ __forceinline__ void ld_acc4(const ACC *p, ACC (&o)[4])
 template <typename ACC>
 __device__ __forceinline__ void st_acc4(ACC *p, const ACC (&v)[4])
 {
-    if constexpr (sizeof(ACC) == 4) {
+    if constexpr (std::is_same<ACC, KahanAcc>::value) {
+        st4((float *)p, make_float4(v[0].s, v[0].c, v[1].s, v[1].c));
+        st4((float *)p + 4, make_float4(v[2].s, v[2].c, v[3].s, v[3].c));
+    } else if constexpr (sizeof(ACC) == 4) {
         st4((float *)p, make_float4(v[0], v[1], v[2], v[3]));
     } else {
         reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
@@ -448,8 +456,12 @@ template <int MODE>
 void pres4_dispatch(int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s)
 {
     if constexpr (MODE == 2) {
-        if (a.accum_fp64) {
+        if (a.accum_fp64 == RTM_ACC_FP64) {
             pres4_dispatch_t<MODE, double>(bz, a, ntiles, record, s);
+            return;
+        }
+        if (a.accum_fp64 == RTM_ACC_KAHAN) {
+            pres4_dispatch_t<MODE, KahanAcc>(bz, a, ntiles, record, s);
             return;
         }
     }

@@ -107,6 +107,16 @@ struct ShotDev {
     const float *vp2_b;
 };
 
+// Imaging accumulator of RTM_ACC_KAHAN: compensated fp32 pair (8 bytes, as a double), the
+// accumulated value being s - c.
+struct KahanAcc {
+    float s, c;
+    __host__ __device__ KahanAcc() : s(0.f), c(0.f) {}
+    __host__ __device__ KahanAcc(int) : s(0.f), c(0.f) {}
+};
+// Per-shot accumulation of g1 and illum (rtm_options.accum_fp64): fp32, fp64, compensated fp32.
+enum RtmAccum { RTM_ACC_FP32 = 0, RTM_ACC_FP64 = 1, RTM_ACC_KAHAN = 2 };
+
 // TMA tensor maps of one slot: the staged fields of the two wavefields with the box each
 // stencil kernel loads (velocity: p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139;
 // pressure: vx rows z0 .. z0+BZ-1 with the same columns, vz rows z0-10 .. z0+BZ+11,

@@ -558,3 +558,24 @@ def test_tile_height_tuner(rtmlib, monkeypatch, tmp_path):
         assert np.array_equal(tuned[k], want[k]), k
     for a, b in zip(gathers, want["gathers"]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_compensated_fp32_accumulation(rtmlib, monkeypatch):
+    """accum_fp64 = 2: compensated fp32 pairs (Kahan) for the per-shot g1 and illumination,
+    stacked in fp64: within 1e-6 rel-L2 of fp64 accumulation of the same FP32 wavefields, and
+    the same bits from both kernel forms."""
+    G = rtmlib
+    c = GENERAL[0]
+    v, rho = _random_model(c["nz"], c["nx"], 13)
+    shots = [1, 2]
+    s = cfg_from(G, _survey(c, 0))
+    d64 = G.migrate(s, G.RunOptions(accum_fp64=1), shots, v, rho)
+    dk = G.migrate(s, G.RunOptions(accum_fp64=2), shots, v, rho)
+    for k in ("image1", "image2s", "illum"):
+        assert np.abs(d64["f64"][k]).max() > 0
+        assert rel_l2(dk["f64"][k], d64["f64"][k]) < 1e-6, (k, rel_l2(dk["f64"][k], d64["f64"][k]))
+    monkeypatch.setenv("RTM_B200_KERNELS", "scalar")
+    ds = G.migrate(s, G.RunOptions(accum_fp64=2), shots, v, rho)
+    for k in ("image1", "image2s", "illum"):
+        assert np.array_equal(ds["f64"][k], dk["f64"][k]), k
