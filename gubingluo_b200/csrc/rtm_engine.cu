@@ -96,6 +96,7 @@ struct ShotState {
 
 struct Slot {
     WaveDev a{}, b{};
+    WaveDev a2{}, b2{};   // whole-step kernel: second buffers of p, vx, vz (sx, sz are a's and b's)
     void *strips = nullptr;
     float *strip_scale = nullptr, *strip_stage = nullptr;
     void *g1 = nullptr, *illum = nullptr;
@@ -136,6 +137,11 @@ struct rtm_session {
     // per thread (rtm_stencil.cu, RTM_B200_KERNELS=scalar); the results are the same bits
     bool vec = true;
     bool tune = true;                // choose the tile heights per launch shape by timing them
+    // whole-step kernel (rtm_step.cu): velocity and pressure of a step in one launch over
+    // tz_step-row tiles, two buffers per field, four descriptor tables (which buffer is
+    // current for each wavefield)
+    bool fused = false;
+    int tz_step = 32;
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -327,10 +333,11 @@ static int upload_model(rtm_session *ss, const std::vector<float> &vp2, const st
     return RTM_OK;
 }
 
-static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, int Z, int strip_len, int nxi, int nzi)
+static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, int Z, int strip_len, int nxi, int nzi,
+                         bool fused)
 {
     size_t field = (size_t)pitch * Z * sizeof(float) + 256;
-    size_t b = 10 * field;
+    size_t b = (fused ? 16 : 10) * field;
     b += (size_t)s.nt * strip_len * elem_size(o.strip_precision) + 256;
     if (o.strip_precision != RTM_PREC_FP32) {
         b += (size_t)s.nt * 4 * sizeof(float) + 256;
@@ -413,7 +420,17 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     CK(cudaMemGetInfo(&free_b, &total_b));
     const ShotState &big = *std::max_element(ss->shots.begin(), ss->shots.end(),
                                              [](const ShotState &a, const ShotState &b) { return a.X < b.X; });
-    size_t per_slot = slot_bytes(s, o, big.pitch, big.Z, big.strip_len, big.nxi, big.nzi);
+    {
+        // RTM_B200_FUSED=1: the whole-step kernel; RTM_B200_TZ_STEP: its rows per tile (16, 32)
+        const char *e = std::getenv("RTM_B200_FUSED");
+        if (e && *e) ss->fused = std::atoi(e) != 0;
+        if ((e = std::getenv("RTM_B200_TZ_STEP")) && *e) {
+            ss->tz_step = std::atoi(e);
+            ss->tune = false;
+        }
+        if (ss->tz_step != 16 && ss->tz_step != 32) return fail(RTM_ERR_ARG, "RTM_B200_TZ_STEP must be 16 or 32");
+    }
+    size_t per_slot = slot_bytes(s, o, big.pitch, big.Z, big.strip_len, big.nxi, big.nzi, ss->fused);
     size_t fixed = model_bytes + shot_bytes_total + (o.extra_images ? 11 : 4) * ((size_t)s.nx * s.nz * 8 + 256) + (size_t)s.nt * 4 + 4096 +
                    (size_t)(64 << 20);
     size_t budget = (size_t)(free_b * 0.92);
@@ -556,11 +573,16 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->slots.resize(B);
     for (Slot &sl : ss->slots) {
         const size_t fb = (size_t)big.pitch * big.Z * 4;
-        float **f[10] = {&sl.a.p, &sl.a.vx, &sl.a.vz, &sl.a.sx, &sl.a.sz, &sl.b.p, &sl.b.vx, &sl.b.vz, &sl.b.sx, &sl.b.sz};
-        for (float **pp : f) {
-            *pp = (float *)ss->arena.take(fb);
-            if (!*pp) return fail(RTM_ERR_NOMEM, "device arena exhausted (fields)");
+        float **f[16] = {&sl.a.p,  &sl.a.vx,  &sl.a.vz,  &sl.a.sx, &sl.a.sz, &sl.b.p, &sl.b.vx, &sl.b.vz,
+                         &sl.b.sx, &sl.b.sz,  &sl.a2.p,  &sl.a2.vx, &sl.a2.vz, &sl.b2.p, &sl.b2.vx, &sl.b2.vz};
+        for (int i = 0; i < (ss->fused ? 16 : 10); i++) {
+            *f[i] = (float *)ss->arena.take(fb);
+            if (!*f[i]) return fail(RTM_ERR_NOMEM, "device arena exhausted (fields)");
         }
+        sl.a2.sx = sl.a.sx;
+        sl.a2.sz = sl.a.sz;
+        sl.b2.sx = sl.b.sx;
+        sl.b2.sz = sl.b.sz;
         sl.strips = ss->arena.take((size_t)s.nt * big.strip_len * elem_size(o.strip_precision));
         if (o.strip_precision != RTM_PREC_FP32) {
             sl.strip_scale = (float *)ss->arena.take((size_t)s.nt * 4 * 4);
@@ -580,7 +602,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     }
     // descriptor and tile tables, tensor maps, kernel error flag
     ss->arena.label = "tables and flags";
-    ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B);
+    ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B * (ss->fused ? 4 : 1));
     ss->d_tmaps = ss->arena.take((size_t)B * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
     ss->d_err = (int *)ss->arena.take(sizeof(int));
     ss->d_nonfinite = (int *)ss->arena.take(sizeof(int));
@@ -678,7 +700,42 @@ struct BatchRun {
     int k0 = 0, n = 0, ntiles = 0, ntiles_p = 0, ntiles_r = 0, ntiles_pr = 0, maxrec = 0, max_strip_len = 0;
     std::vector<ShotDev> hd;
     StepArgs a{};
+    // whole-step kernel: which buffer holds the current source (pa) and receiver (pb) fields
+    int pa = 0, pb = 0;
 };
+
+// Descriptor tables of a batch.  One table (hd as built) for the split kernels; with the
+// whole-step kernel four, one per (pa, pb): in table 2 pa + pb, `a` is the source wavefield's
+// buffer pa and `an` the other one, likewise b / bn with pb, so every kernel reads the current
+// fields through `a` and `b` whatever the step.
+static ShotDev *table(rtm_session *ss, const BatchRun &br) { return ss->d_shots + (size_t)(2 * br.pa + br.pb) * ss->B; }
+
+static int upload_tables(rtm_session *ss, const BatchRun &br)
+{
+    const int n = br.n;
+    if (!ss->fused) {
+        CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, ss->stream));
+        return RTM_OK;
+    }
+    std::vector<ShotDev> t(4 * (size_t)ss->B);
+    for (int pa = 0; pa < 2; pa++)
+        for (int pb = 0; pb < 2; pb++)
+            for (int j = 0; j < n; j++) {
+                ShotDev d = br.hd[j];
+                const WaveDev A0 = br.hd[j].a, A1 = br.hd[j].an, B0 = br.hd[j].b, B1 = br.hd[j].bn;
+                d.a = pa ? A1 : A0;
+                d.an = pa ? A0 : A1;
+                d.b = pb ? B1 : B0;
+                d.bn = pb ? B0 : B1;
+                d.par_a = pa;
+                d.par_b = pb;
+                t[(size_t)(2 * pa + pb) * ss->B + j] = d;
+            }
+    CK(cudaMemcpyAsync(ss->d_shots, t.data(), sizeof(ShotDev) * t.size(), cudaMemcpyHostToDevice, ss->stream));
+    // the host copy must live until the copy has read it
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
 
 // Bind shots [k0, k0+n) to slots 0..n-1, zero their wavefields and accumulators, upload
 // the descriptor and (shot, tile) tables.
@@ -723,10 +780,13 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         {
             const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA_VEL, ph = ss->bz_pres + RTM_STAGE_ZEXTRA_PRES;
             const int vhr = ss->bz_vel_recon + RTM_STAGE_ZEXTRA_VEL;
+            // whole-step kernel: p of both buffers of each wavefield (placeholders when off)
+            const int sw = RTM_BX + 48, sh_ = ss->tz_step + 38;
+            float *a2p = ss->fused ? sl.a2.p : sl.a.p, *b2p = ss->fused ? sl.b2.p : sl.b.p;
             struct { float *f; int w, h; } m[RTM_TMAP_COUNT] = {
                 {sl.a.p, RTM_STAGE_W, vh}, {sl.a.vx, RTM_STAGE_W, ss->bz_pres}, {sl.a.vz, RTM_BX, ph},
                 {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph},
-                {sl.a.p, RTM_STAGE_W, vhr}};
+                {sl.a.p, RTM_STAGE_W, vhr}, {sl.a.p, sw, sh_}, {a2p, sw, sh_}, {sl.b.p, sw, sh_}, {b2p, sw, sh_}};
             for (int t = 0; t < RTM_TMAP_COUNT; t++) {
                 CUtensorMap cm;
                 int rc = encode_field_map(&cm, m[t].f, sh.pitch, sh.Z, m[t].w, m[t].h);
@@ -749,9 +809,30 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
                     v.push_back({j, x0, z0, (fast && inside) ? 1 : 0});
                 }
         };
-        add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
+        if (ss->fused) {
+            // whole-step tiles of tz_step rows, interior ones (cells and velocity halo in the
+            // interior, full orders, no source or receiver) in their own lists: full grid
+            // (fast: tiles, others: tiles_p) and reconstruction region (tiles_r, tiles_pr)
+            const int tz = ss->tz_step, np = std::max(s.npml, RTM_RADIUS);
+            auto fast_tile = [&](int x0, int z0, bool recon) {
+                const bool vel_in = x0 - 12 >= np && x0 + RTM_BX + 12 <= sh.X - np - 1 && z0 - 10 >= np &&
+                                    z0 + tz + 10 <= sh.Z - np - 1;
+                const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x0 + RTM_BX && z0 < sh.sbz0 + sh.sbnz &&
+                                 sh.sbz0 < z0 + tz;
+                const bool rec = !recon && sh.g.rz >= z0 && sh.g.rz < z0 + tz && x0 < sh.g.rx0 + sh.g.nrec &&
+                                 sh.g.rx0 < x0 + RTM_BX;
+                return fast && vel_in && !src && !rec;
+            };
+            for (int z0 = 0; z0 < sh.Z; z0 += tz)
+                for (int x0 = 0; x0 < sh.X; x0 += RTM_BX)
+                    (fast_tile(x0, z0, false) ? tiles : tiles_p).push_back({j, x0, z0, 1});
+            for (int z0 = zr0; z0 < zr1; z0 += tz)
+                for (int x0 = xr0; x0 < xr1; x0 += RTM_BX)
+                    (fast_tile(x0, z0, true) ? tiles_r : tiles_pr).push_back({j, x0, z0, 1});
+        }
+        if (!ss->fused) add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
         // pressure tiles: interior tiles (no PML, source or receiver cell) go to their own list
-        for (int z0 = 0; z0 < sh.Z; z0 += ss->bz_pres)
+        for (int z0 = 0; z0 < (ss->fused ? 0 : sh.Z); z0 += ss->bz_pres)
             for (int x0 = 0; x0 < sh.X; x0 += RTM_BX) {
                 const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
                 const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
@@ -759,10 +840,10 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
                 const bool rec = sh.g.rz >= z0 && sh.g.rz < z1 && x0 < sh.g.rx0 + sh.g.nrec && sh.g.rx0 < x1;
                 tiles_p.push_back({j, x0, z0, (fast && inside && !src && !rec) ? 1 : 0});
             }
-        add_tiles(tiles_r, ss->bz_vel_recon, xr0, xr1, zr0, zr1);
+        if (!ss->fused) add_tiles(tiles_r, ss->bz_vel_recon, xr0, xr1, zr0, zr1);
         // reconstruction pressure tiles: interior when inside the pressure interior with no
         // source cell
-        for (int z0 = zr0; z0 < zr1; z0 += ss->bz_pres)
+        for (int z0 = zr0; z0 < (ss->fused ? zr0 : zr1); z0 += ss->bz_pres)
             for (int x0 = xr0; x0 < xr1; x0 += RTM_BX) {
                 const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
                 const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
@@ -772,8 +853,9 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
         br.max_strip_len = std::max(br.max_strip_len, sh.strip_len);
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
-        float *f[10] = {sl.a.p, sl.a.vx, sl.a.vz, sl.a.sx, sl.a.sz, sl.b.p, sl.b.vx, sl.b.vz, sl.b.sx, sl.b.sz};
-        for (float *p : f) CK(cudaMemsetAsync(p, 0, fb, st));
+        float *f[16] = {sl.a.p,  sl.a.vx, sl.a.vz,  sl.a.sx,  sl.a.sz, sl.b.p,   sl.b.vx,  sl.b.vz,
+                        sl.b.sx, sl.b.sz, sl.a2.p, sl.a2.vx, sl.a2.vz, sl.b2.p, sl.b2.vx, sl.b2.vz};
+        for (int i = 0; i < (ss->fused ? 16 : 10); i++) CK(cudaMemsetAsync(f[i], 0, fb, st));
         size_t ib = (size_t)sh.pitch * sh.Z * (o.accum_fp64 ? 8 : 4);
         CK(cudaMemsetAsync(sl.g1, 0, ib, st));
         CK(cudaMemsetAsync(sl.illum, 0, ib, st));
@@ -786,7 +868,13 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.ntiles_pr = (int)tiles_pr.size();
     if (std::max(std::max(br.ntiles, br.ntiles_p), std::max(br.ntiles_r, br.ntiles_pr)) > ss->max_tiles)
         return fail(RTM_ERR_ARG, "tile table overflow");
-    CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
+    for (int j = 0; j < n; j++) {
+        const Slot &sl = ss->slots[j];
+        br.hd[j].an = sl.a2;
+        br.hd[j].bn = sl.b2;
+    }
+    br.pa = br.pb = 0;
+    if (int rc = upload_tables(ss, br)) return rc;
     CK(cudaMemcpyAsync(ss->d_tmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles, tiles.data(), sizeof(TileRef) * br.ntiles, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ss->d_tiles_p, tiles_p.data(), sizeof(TileRef) * br.ntiles_p, cudaMemcpyHostToDevice, st));
@@ -920,24 +1008,36 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
             a.ring = it % kRing;
             const int mode = RTM_WAVE_FWD;
             if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:324-326: |p| before the step
-                launch_absmax(ss->d_shots, br.n, 0, ss->d_absmax + (size_t)(it / ntsnap) * ss->B, st);
+                launch_absmax(table(ss, br), br.n, 0, ss->d_absmax + (size_t)(it / ntsnap) * ss->B, st);
                 ss->launches++;
             }
             cudaEvent_t e;
-            timing_begin(ss, "vel_fwd", it, &e);
-            a.tiles = ss->d_tiles;
-            vel_step(ss, mode, ss->bz_vel, a, br.ntiles);
-            timing_end(ss, e);
-            timing_begin(ss, "pres_fwd", it, &e);
-            launch_pres_tiles(ss, br, mode, record ? 1 : 0);
-            timing_end(ss, e);
-            ss->launches += 1;
+            if (ss->fused) {   // velocity and pressure in one launch per tile kind; then swap buffers
+                timing_begin(ss, "step_fwd", it, &e);
+                a.shots = table(ss, br);
+                a.tiles = ss->d_tiles;
+                launch_step(mode, ss->tz_step, true, a, br.ntiles, record ? 1 : 0, st);
+                a.tiles = ss->d_tiles_p;
+                launch_step(mode, ss->tz_step, false, a, br.ntiles_p, record ? 1 : 0, st);
+                timing_end(ss, e);
+                ss->launches += 2;
+                br.pa ^= 1;
+            } else {
+                timing_begin(ss, "vel_fwd", it, &e);
+                a.tiles = ss->d_tiles;
+                vel_step(ss, mode, ss->bz_vel, a, br.ntiles);
+                timing_end(ss, e);
+                timing_begin(ss, "pres_fwd", it, &e);
+                launch_pres_tiles(ss, br, mode, record ? 1 : 0);
+                timing_end(ss, e);
+                ss->launches += 1;
+            }
             if (save) {
-                launch_strip_save(ss->d_shots, br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
+                launch_strip_save(table(ss, br), br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
                 ss->launches++;
             }
             if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
-                launch_strip_pack(ss->d_shots, br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
+                launch_strip_pack(table(ss, br), br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
                 ss->launches++;
             }
         }
@@ -946,8 +1046,11 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
         loop();
         CK(cudaGetLastError());
     } else {
+        const int pa0 = br.pa;
         int rc = run_pass(ss, {0, br.n, br.ntiles, br.ntiles_p, br.max_strip_len, nsteps, save, record, ss->bz_vel,
-                               ss->bz_pres, ss->vec}, loop);
+                               ss->bz_pres, ss->vec, ss->fused, ss->tz_step, pa0, br.pb}, loop);
+        // a replayed graph swaps the buffers as the captured loop did
+        if (!rc && ss->fused && ss->o.use_graph) br.pa = pa0 ^ (nsteps & 1);
         if (rc) {
             nvtxRangePop();
             return rc;
@@ -955,6 +1058,29 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
     }
     nvtxRangePop();
     if (ntsnap) return print_snapshots(ss, br, 0, save ? "source" : "forward", nsteps, ntsnap);
+    return RTM_OK;
+}
+
+// With the whole-step kernel the current fields may lie in the second buffers; copy them to
+// the first ones, where the readers of a slot's fields look (rtm_session_get_wavefields,
+// rtm_forward).
+static int settle_fields(rtm_session *ss, BatchRun &br)
+{
+    if (!ss->fused) return RTM_OK;
+    for (int j = 0; j < br.n; j++) {
+        const ShotState &sh = ss->shots[br.k0 + j];
+        Slot &sl = ss->slots[j];
+        const size_t fb = (size_t)sh.pitch * sh.Z * 4;
+        const int par[2] = {br.pa, br.pb};
+        const WaveDev *from[2] = {&sl.a2, &sl.b2}, *to[2] = {&sl.a, &sl.b};
+        for (int w = 0; w < 2; w++)
+            if (par[w]) {
+                CK(cudaMemcpyAsync(to[w]->p, from[w]->p, fb, cudaMemcpyDeviceToDevice, ss->stream));
+                CK(cudaMemcpyAsync(to[w]->vx, from[w]->vx, fb, cudaMemcpyDeviceToDevice, ss->stream));
+                CK(cudaMemcpyAsync(to[w]->vz, from[w]->vz, fb, cudaMemcpyDeviceToDevice, ss->stream));
+            }
+    }
+    br.pa = br.pb = 0;
     return RTM_OK;
 }
 
@@ -981,18 +1107,19 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             br.hd[j].gather = sh.gather32;
         }
     }
-    CK(cudaMemcpyAsync(ss->d_shots, br.hd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, st));
+    if (int rc = upload_tables(ss, br)) return rc;
     a.gather_prec = o.gather_precision;
     // ps = final forward p; vxs = vzs = 0 (rtm_model.cu:367-372); the receiver wavefield
     // starts from rest with the last gather sample injected (:410)
     for (int j = 0; j < n; j++) {
         ShotState &sh = ss->shots[br.k0 + j];
         Slot &sl = ss->slots[j];
+        const WaveDev &ca = br.pa ? sl.a2 : sl.a;   // the current source-side buffer
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
-        CK(cudaMemsetAsync(sl.a.vx, 0, fb, st));
-        CK(cudaMemsetAsync(sl.a.vz, 0, fb, st));
+        CK(cudaMemsetAsync(ca.vx, 0, fb, st));
+        CK(cudaMemsetAsync(ca.vz, 0, fb, st));
     }
-    launch_inject(ss->d_shots, n, br.maxrec, s.nt - 1, s.dt, o.gather_precision, st);
+    launch_inject(table(ss, br), n, br.maxrec, s.nt - 1, s.dt, o.gather_precision, st);
     ss->launches++;
     // the other imaging conditions compare each step with the pressures before it
     // (rtm_model.cu:419-420); their kernel keeps ps_pre/p_pre current from then on
@@ -1002,8 +1129,8 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             const ShotState &sh = ss->shots[br.k0 + j];
             const Slot &sl = ss->slots[j];
             const size_t fb = (size_t)sh.pitch * sh.Z * 4;
-            CK(cudaMemcpyAsync(sl.ps_pre, sl.a.p, fb, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(sl.p_pre, sl.b.p, fb, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(sl.ps_pre, (br.pa ? sl.a2 : sl.a).p, fb, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(sl.p_pre, (br.pb ? sl.b2 : sl.b).p, fb, cudaMemcpyDeviceToDevice, st));
             max_nxi = std::max(max_nxi, sh.nxi);
             max_nzi = std::max(max_nzi, sh.nzi);
         }
@@ -1016,11 +1143,36 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             a.it = it;
             cudaEvent_t e;
             if (ntsnap && it % ntsnap == 0) {   // rtm_model.cu:415-417: receiver |p| before the step
-                launch_absmax(ss->d_shots, n, 1, snap_b + (size_t)(it / ntsnap) * ss->B, st);
+                launch_absmax(table(ss, br), n, 1, snap_b + (size_t)(it / ntsnap) * ss->B, st);
                 ss->launches++;
             }
             // reconstruction of the source wavefield, then the receiver wavefield and imaging
             // (which reads the reconstructed pressure of the same step)
+            if (ss->fused) {
+                timing_begin(ss, "step_recon", it, &e);
+                a.shots = table(ss, br);
+                a.tiles = ss->d_tiles_r;
+                launch_step(RTM_WAVE_RECON, ss->tz_step, true, a, br.ntiles_r, 0, st);
+                a.tiles = ss->d_tiles_pr;
+                launch_step(RTM_WAVE_RECON, ss->tz_step, false, a, br.ntiles_pr, 0, st);
+                timing_end(ss, e);
+                br.pa ^= 1;
+                timing_begin(ss, "step_recv", it, &e);
+                a.shots = table(ss, br);
+                a.tiles = ss->d_tiles;
+                launch_step(RTM_WAVE_RECEIVER, ss->tz_step, true, a, br.ntiles, 0, st);
+                a.tiles = ss->d_tiles_p;
+                launch_step(RTM_WAVE_RECEIVER, ss->tz_step, false, a, br.ntiles_p, 0, st);
+                timing_end(ss, e);
+                br.pb ^= 1;
+                ss->launches += 4;
+                if (o.extra_images) {
+                    launch_image_extra(table(ss, br), n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx,
+                                       s.dz, s.dt, st);
+                    ss->launches++;
+                }
+                continue;
+            }
             timing_begin(ss, "vel_recon", it, &e);
             a.tiles = ss->d_tiles_r;
             vel_step(ss, RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r);
@@ -1048,8 +1200,14 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         loop();
         CK(cudaGetLastError());
     } else {
+        const int pa0 = br.pa, pb0 = br.pb;
         int rc = run_pass(ss, {1, n, br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr, max_nxi, max_nzi,
-                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->vec}, loop);
+                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->vec, ss->fused,
+                               ss->tz_step, pa0, pb0}, loop);
+        if (!rc && ss->fused && ss->o.use_graph) {   // a replayed graph swaps as the captured loop did
+            br.pa = pa0 ^ ((s.nt - 1) & 1);
+            br.pb = pb0 ^ ((s.nt - 1) & 1);
+        }
         if (rc) {
             nvtxRangePop();
             return rc;
@@ -1060,6 +1218,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         int rc = print_snapshots(ss, br, 1, "backward", s.nt, ntsnap);
         if (rc) return rc;
     }
+    if (int rc = settle_fields(ss, br)) return rc;
     nvtxRangePushA("rtm: stacking");
     std::vector<char> fin(finalize_shot_size() * n);
     for (int j = 0; j < n; j++) {
@@ -1106,10 +1265,76 @@ static std::string tune_key(rtm_session *ss, int k0, int n)
     int xmax = 0;
     for (int j = 0; j < n; j++) xmax = std::max(xmax, ss->shots[k0 + j].X);
     char b[200];
-    std::snprintf(b, sizeof b, "%s/X%d/Z%d/npml%d/n%d/strip%d/gather%d/acc%d/extra%d/mode%d", ss->vec ? "vector" : "scalar",
+    std::snprintf(b, sizeof b, "%s/X%d/Z%d/npml%d/n%d/strip%d/gather%d/acc%d/extra%d/mode%d",
+                  ss->fused ? "step" : ss->vec ? "vector" : "scalar",
                   xmax, ss->shots[k0].Z, ss->s.npml, n, ss->o.strip_precision, ss->o.gather_precision, ss->o.accum_fp64,
                   ss->o.extra_images, ss->s.mode);
     return b;
+}
+
+// The whole-step kernel's tile height (16 or 32 rows), timed the same way: source-pass,
+// reconstruction and receiver steps, each kind's fast and general launches together.  The
+// choice is recorded as "key tz tz tz".
+static int tune_step_height(rtm_session *ss, int k0, int n, const std::string &key, const char *path)
+{
+    const int cand[2] = {16, 32};
+    double ms[2] = {0, 0};
+    cudaEvent_t ev[2][4];
+    for (auto &b : ev)
+        for (auto &e : b) CK(cudaEventCreate(&e));
+    cudaStream_t st = ss->stream;
+    int rc = RTM_OK;
+    const int steps = 6, warm = 2;
+    for (int c = 0; c < 2 && rc == RTM_OK; c++) {
+        ss->tz_step = cand[c];
+        BatchRun br;
+        if ((rc = batch_setup(ss, k0, n, br))) break;
+        StepArgs a = br.a;
+        for (int it = 0; it < steps; it++) {
+            const int t = it - warm;
+            a.it = std::min(it + 1, ss->s.nt - 2);
+            if (t >= 0) cudaEventRecord(ev[0][t], st);
+            const int modes[3] = {RTM_WAVE_FWD, RTM_WAVE_RECON, RTM_WAVE_RECEIVER};
+            for (int m : modes) {
+                a.shots = table(ss, br);
+                const bool recon = m == RTM_WAVE_RECON;
+                a.tiles = recon ? ss->d_tiles_r : ss->d_tiles;
+                launch_step(m, ss->tz_step, true, a, recon ? br.ntiles_r : br.ntiles, 0, st);
+                a.tiles = recon ? ss->d_tiles_pr : ss->d_tiles_p;
+                launch_step(m, ss->tz_step, false, a, recon ? br.ntiles_pr : br.ntiles_p, 0, st);
+                if (m == RTM_WAVE_RECEIVER) br.pb ^= 1;
+                else br.pa ^= 1;
+            }
+            if (t >= 0) cudaEventRecord(ev[1][t], st);
+        }
+        ss->launches += 6 * steps;
+        if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = fail(RTM_ERR_CUDA, "tile-height trial launches failed");
+            break;
+        }
+        for (int t = 0; t < steps - warm; t++) {
+            float m = 0.f;
+            cudaEventElapsedTime(&m, ev[0][t], ev[1][t]);
+            ms[c] += m;
+        }
+    }
+    for (auto &b : ev)
+        for (auto &e : b) cudaEventDestroy(e);
+    if (rc) return rc;
+    if ((rc = check_kernel_flag(ss))) return rc;
+    const int tz = ms[0] < ms[1] ? cand[0] : cand[1];
+    ss->tz_step = tz;
+    if (ss->o.verbose)
+        std::printf("rtm_b200: step tile height for %s: %d (ms per 4 steps: 16 rows %.3f, 32 rows %.3f)\n", key.c_str(),
+                    tz, ms[0], ms[1]);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = {tz, tz, tz};
+    if (path && *path)
+        if (FILE *f = std::fopen(path, "a")) {
+            std::fprintf(f, "%s %d %d %d\n", key.c_str(), tz, tz, tz);
+            std::fclose(f);
+        }
+    return RTM_OK;
 }
 
 static int tune_heights(rtm_session *ss, int k0, int n)
@@ -1130,12 +1355,17 @@ static int tune_heights(rtm_session *ss, int k0, int n)
         }
         auto it = g_tune.find(key);
         if (it != g_tune.end()) {
+            if (ss->fused) {
+                ss->tz_step = it->second[0];
+                return RTM_OK;
+            }
             ss->bz_vel = it->second[0];
             ss->bz_vel_recon = it->second[1];
             ss->bz_pres = it->second[2];
             return RTM_OK;
         }
     }
+    if (ss->fused) return tune_step_height(ss, k0, n, key, path);
     const int cand[3] = {8, 16, 32};
     const char *names[6] = {"vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv"};
     double ms[3][6] = {};
@@ -1446,9 +1676,9 @@ int rtm_session_get_pml(rtm_session *ss, int k, float *ddx, float *ddz, float *d
 int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres)
 {
     if (!ss) return fail(RTM_ERR_ARG, "null session");
-    if (bz_vel) *bz_vel = ss->bz_vel;
-    if (bz_vel_recon) *bz_vel_recon = ss->bz_vel_recon;
-    if (bz_pres) *bz_pres = ss->bz_pres;
+    if (bz_vel) *bz_vel = ss->fused ? ss->tz_step : ss->bz_vel;
+    if (bz_vel_recon) *bz_vel_recon = ss->fused ? ss->tz_step : ss->bz_vel_recon;
+    if (bz_pres) *bz_pres = ss->fused ? ss->tz_step : ss->bz_pres;
     return RTM_OK;
 }
 
@@ -1726,7 +1956,8 @@ int rtm_forward(const rtm_survey *s, const rtm_options *o, int ishot, const floa
     BatchRun br;
     const ShotState &sh = ss->shots[0];
     const Slot &sl = ss->slots[0];
-    if (!(rc = batch_setup(ss, 0, 1, br)) && !(rc = batch_forward(ss, br, nsteps, false, true))) {
+    if (!(rc = batch_setup(ss, 0, 1, br)) && !(rc = batch_forward(ss, br, nsteps, false, true)) &&
+        !(rc = settle_fields(ss, br))) {
         cudaError_t e = cudaStreamSynchronize(ss->stream);
         if (e != cudaSuccess) rc = fail(RTM_ERR_CUDA, cudaGetErrorString(e));
         if (!rc) rc = check_kernel_flag(ss);

@@ -12,6 +12,11 @@ void launch_pres(int mode, int bz, const StepArgs &a, int ntiles, int record, cu
 // lists, staged boxes and results, 32 * bz / U threads per block.
 void launch_vel4(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s);
 void launch_pres4(int mode, int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s);
+// One whole time step (velocities and pressure) of one wavefield (rtm_step.cu): reads the
+// shots' a / b fields, writes an / bn; tz rows per tile (16 or 32), 256 threads per block;
+// `fast`: the tile list holds only interior tiles (the branch-free instance).
+void launch_step(int mode, int tz, bool fast, const StepArgs &a, int ntiles, int record, cudaStream_t s);
+size_t step_smem_bytes(int tz);
 void launch_setup_pml(float *pml, int X, int Z, int npml, float dx, float dz, float dt, float vpmax, cudaStream_t s);
 void launch_setup_source(float *src, int sbx0, int sbz0, int sbnx, int sbnz, int nsx, int nsz, float amp, float alp,
                          float dx2, float dz2, float dt, cudaStream_t s);

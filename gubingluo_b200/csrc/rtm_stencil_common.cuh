@@ -265,6 +265,49 @@ __device__ __forceinline__ void vel_apply(const StepArgs &a, const ShotDev &S, c
     if (z < Z - 1) vzp[id] = nvz;
 }
 
+// New vx / vz of one existing cell (x, z) from the raw derivative sums, for kernels that
+// write every cell of a second buffer: the damped update (modes 0 and 2); in the
+// reconstruction, the interior update, the restored strip of step it+1, or the old value
+// where the reconstruction leaves the cell alone.  Same operations as vel_apply.
+template <int MODE>
+__device__ __forceinline__ float vx_value(const StepArgs &a, const ShotDev &S, const ShotK &k, const PmlOffsets &o,
+                                          int x, int z, int X, int Z, int npml, float dx, float ir, float ov)
+{
+    if (MODE == 3) {
+        const bool zin = (z >= npml && z < Z - npml);
+        if (zin && x >= npml && x <= X - npml - 2) return __fadd_rn(ov, vel_inc(dx, a.dtx, ir));
+        const int svx = strip_col_vx(x, X, npml, k.nzi);
+        if (zin && svx >= 0) {   // read_d_vxpml, kernel.cu:1294-1320
+            const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 0] : 1.0f;
+            return load_strip(S.strips, (size_t)(a.it + 1) * k.strip_len + svx + (size_t)(z - npml) * R, a.strip_prec,
+                              sc);
+        }
+        return ov;
+    }
+    const bool band = (x < npml) || (x >= X - npml - 1);
+    const float c1 = band ? S.pml[o.c1vx + x] : 1.0f, ic2 = band ? S.pml[o.ic2vx + x] : 1.0f;
+    return damp(ov, vel_inc(dx, a.dtx, ir), c1, ic2);
+}
+template <int MODE>
+__device__ __forceinline__ float vz_value(const StepArgs &a, const ShotDev &S, const ShotK &k, const PmlOffsets &o,
+                                          int x, int z, int X, int Z, int npml, float dz, float ir, float ow)
+{
+    if (MODE == 3) {
+        const bool xin = (x >= npml && x < X - npml);
+        if (z >= npml && z <= Z - npml - 2 && xin) return __fadd_rn(ow, vel_inc(dz, a.dtz, ir));
+        if (xin) {
+            const int srow = strip_row_tb(z, npml, Z - npml - 1, k.nxi);
+            if (srow >= 0) {   // read_d_vzpml, kernel.cu:1321-1347
+                const float sc = a.strip_prec ? S.strip_scale[(size_t)(a.it + 1) * 4 + 1] : 1.0f;
+                return load_strip(S.strips, (size_t)(a.it + 1) * k.strip_len + 2 * (size_t)R * k.nzi + srow + (x - npml),
+                                  a.strip_prec, sc);
+            }
+        }
+        return ow;
+    }
+    return damp(ow, vel_inc(dz, a.dtz, ir), S.pml[o.c1vz + z], S.pml[o.ic2vz + z]);
+}
+
 // Per-column constants of the pressure update.
 struct PresCol {
     bool xb, xin;        // column in the x PML band / in the image interior
@@ -274,14 +317,17 @@ struct PresCol {
 };
 
 // Pressure update of one cell (x, z) from the raw derivative sums dx, dz; `upd` is false on
-// the grid's edge rows and columns, which keep their pressure (kernel.cu:714-1185).
+// the grid's edge rows and columns, which keep their pressure (kernel.cu:714-1185).  Returns the
+// cell's new pressure (its old one where nothing changes it) and sets *wr when the one-buffer
+// kernels must store it; the split fields, the recorded gather and the imaging accumulators are
+// written here.
 template <int MODE, typename ACC>
-__device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, const ShotK &k, const PresCol &cc,
-                                           float wit, float *__restrict__ pp, float *__restrict__ sxp,
-                                           float *__restrict__ szp, ACC *__restrict__ g1p, ACC *__restrict__ ilp,
-                                           unsigned id, int x, int z, int Z, int npml, bool upd, float dx,
-                                           float dz, float kk, float p0, float s1o, float s2o, float ps, ACC og1,
-                                           ACC oil, float c1z, float ic2z, int record)
+__device__ __forceinline__ float pres_value(const StepArgs &a, const ShotDev &S, const ShotK &k, const PresCol &cc,
+                                            float wit, float *__restrict__ sxp, float *__restrict__ szp,
+                                            ACC *__restrict__ g1p, ACC *__restrict__ ilp, unsigned id, int x, int z,
+                                            int Z, int npml, bool upd, float dx, float dz, float kk, float p0,
+                                            float s1o, float s2o, float ps, ACC og1, ACC oil, float c1z, float ic2z,
+                                            int record, bool *wr_out)
 {
     const float ddx = dx * a.dtx, ddz = dz * a.dtz;
     const bool zin = (z >= npml && z < Z - npml);
@@ -315,8 +361,8 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
             pn -= S.src[(z - k.sbz0) * k.sbnx + (x - k.sbx0)] * wit;
             wr = true;
         }
-        if (wr) pp[id] = pn;
-        return;
+        *wr_out = wr;
+        return pn;
     }
     // full-grid pressure update with split-field PML
     float pn = p0;
@@ -338,7 +384,6 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
             pn += S.src[(z - k.sbz0) * k.sbnx + (x - k.sbx0)] * wit;
             wr = true;
         }
-        if (wr) pp[id] = pn;
         if (record && z == k.rz && cc.recc)   // kernel.cu:48-71
             ((float *)S.gather)[(size_t)a.it * k.nrec + (x - k.rx0)] = pn;
     } else {
@@ -346,9 +391,24 @@ __device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, 
             pn = a.dt * gather_at(a, S, x - k.rx0);
             wr = true;
         }
-        if (wr) pp[id] = pn;
         if (zin && cc.xin) image_cell<ACC>(g1p, ilp, id, og1, oil, ps, pn);   // kernel.cu:1401-1416
     }
+    *wr_out = wr;
+    return pn;
+}
+
+template <int MODE, typename ACC>
+__device__ __forceinline__ void pres_apply(const StepArgs &a, const ShotDev &S, const ShotK &k, const PresCol &cc,
+                                           float wit, float *__restrict__ pp, float *__restrict__ sxp,
+                                           float *__restrict__ szp, ACC *__restrict__ g1p, ACC *__restrict__ ilp,
+                                           unsigned id, int x, int z, int Z, int npml, bool upd, float dx,
+                                           float dz, float kk, float p0, float s1o, float s2o, float ps, ACC og1,
+                                           ACC oil, float c1z, float ic2z, int record)
+{
+    bool wr;
+    const float pn = pres_value<MODE, ACC>(a, S, k, cc, wit, sxp, szp, g1p, ilp, id, x, z, Z, npml, upd, dx, dz, kk, p0,
+                                           s1o, s2o, ps, og1, oil, c1z, ic2z, record, &wr);
+    if (wr) pp[id] = pn;
 }
 
 }  // namespace

@@ -579,3 +579,58 @@ def test_compensated_fp32_accumulation(rtmlib, monkeypatch):
     ds = G.migrate(s, G.RunOptions(accum_fp64=2), shots, v, rho)
     for k in ("image1", "image2s", "illum"):
         assert np.array_equal(ds["f64"][k], dk["f64"][k]), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["fp32", "fp64", "fp16", "kahan"])
+def test_whole_step_kernel_is_bitwise_identical(rtmlib, monkeypatch, form):
+    """The whole-step kernel (velocity and pressure of a step in one launch, two buffers per
+    field; RTM_B200_FUSED=1) gives the bits of the split kernels: gathers, images (the other
+    imaging conditions too) and the final wavefields of the general cases, at 16- and 32-row
+    tiles, with packed strips and gathers, fp64 and compensated accumulators, and with the
+    passes replayed as CUDA graphs."""
+    G = rtmlib
+    opts = dict(fp32=dict(), fp64=dict(accum_fp64=1, extra_images=1),
+                fp16=dict(strip_precision="fp16", gather_precision="fp16", use_graph=True),
+                kahan=dict(accum_fp64=2, batch=1))[form]
+    for ci, c in enumerate(GENERAL):
+        v, rho = _random_model(c["nz"], c["nx"], 40 + ci)
+        shots = list(range(1, c["nshot"] + 1))
+        s = cfg_from(G, _survey(c, 0))
+        monkeypatch.setenv("RTM_B200_FUSED", "0")
+        want = G.migrate(s, G.RunOptions(**opts), shots, v, rho)
+        for tz in ("16", "32"):
+            monkeypatch.setenv("RTM_B200_FUSED", "1")
+            monkeypatch.setenv("RTM_B200_TZ_STEP", tz)
+            got = G.migrate(s, G.RunOptions(**opts), shots, v, rho)
+            keys = ["image1", "image2s", "illum"] + (["image3s", "image4s", "image5s", "imagetrue"] if form == "fp64" else [])
+            for k in keys:
+                assert np.array_equal(got[k], want[k]), (ci, tz, k)
+            for a, b in zip(got["gathers"], want["gathers"]):
+                assert np.array_equal(a, b), (ci, tz)
+        monkeypatch.delenv("RTM_B200_TZ_STEP")
+
+
+@pytest.mark.gpu
+def test_whole_step_kernel_wavefields_and_forward(rtmlib, monkeypatch):
+    """With the whole-step kernel, the final wavefields of a migration and the fields after a
+    number of forward steps (odd and even, so either buffer ends current) are those of the
+    split kernels, bit for bit."""
+    G = rtmlib
+    c = GENERAL[1]
+    v, rho = _random_model(c["nz"], c["nx"], 50)
+    s = cfg_from(G, _survey(c, 0))
+    g = G.geometry(s, 1)
+    res = {}
+    for fused in ("0", "1"):
+        monkeypatch.setenv("RTM_B200_FUSED", fused)
+        with G.Session(s, G.RunOptions(batch=1), [1], v, rho) as ss:
+            ss.run()
+            res[fused] = ss.wavefields(0, g.nxpad, g.nzpad)
+        for nsteps in (37, 60):
+            res[(fused, nsteps)] = G.forward(s, G.RunOptions(), 1, v, rho, nsteps)
+    for a, b in zip(res["1"], res["0"]):
+        assert np.array_equal(a, b)
+    for nsteps in (37, 60):
+        for a, b in zip(res[("1", nsteps)], res[("0", nsteps)]):
+            assert np.array_equal(a, b), nsteps
