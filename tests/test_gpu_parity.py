@@ -476,12 +476,13 @@ def test_tile_heights_do_not_change_the_bits(rtmlib, monkeypatch):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("strips", ["fp32", "fp16"])
-def test_graph_replay_is_bitwise_identical(rtmlib, strips):
+def test_graph_replay_is_bitwise_identical(rtmlib, monkeypatch, strips):
     """use_graph: each pass's time loop captured once per launch shape and replayed gives the
     gathers and images of direct launches bit for bit.  One shot per launch over shots of
     three window widths (layout 1, offsetmax cut at the model's edges), so that graphs are
     both captured and replayed, with packed strips too."""
     G = rtmlib
+    monkeypatch.setenv("RTM_B200_TUNE", "0")   # tile-height trials would add launches to the first run only
     c = GENERAL[2]
     v, rho = _random_model(c["nz"], c["nx"], 9)
     s = cfg_from(G, _survey(c, 0))
