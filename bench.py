@@ -183,6 +183,11 @@ def ncu_traffic_per_unit(kernel: str, X: int, Z: int):
 
 
 # ------------------------------------------------------------------------------------------
+# kernel families timed by the session (split kernels; whole-step kernel)
+KERNEL_FAMILIES = ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv", "step_fwd", "step_recon",
+                   "step_recv")
+
+
 def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int) -> float:
     """Algorithmic DRAM bytes of one launch of `kind` for one shot: every array the kernel
     must read or write, once (4-byte fields; PML split fields excluded as thin bands).
@@ -191,6 +196,8 @@ def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum
       vel_recon:  read ps, 1/rho; read+write vxs, vzs on the interior  24 B per interior cell
       pres_recon: read vxs, vzs, kappa; read+write ps on the interior  20 B per interior cell
       pres_recv adds the imaging: read ps, read+write g1 and illum     4 + 4*accum B per interior cell
+      step_fwd, step_recv (whole step): read p, vx, vz, 1/rho, kappa; write p, vx, vz   32 B per padded cell
+      step_recon: the same on the interior, with both strip sets       32 B per interior cell
     plus the boundary strips the reconstruction kernels read (the forward strips are written
     by a separate copy kernel)."""
     cells, inner = X * Z, nxi * nzi
@@ -202,6 +209,10 @@ def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum
         "pres_recon": 20 * inner + strips,
         "vel_recv": 24 * cells,
         "pres_recv": 20 * cells + (4 + 4 * accum_bytes) * inner + 4 * nrec,
+        # whole-step kernel: read p, vx, vz, 1/rho, kappa; write p, vx, vz once per cell
+        "step_fwd": 32 * cells,
+        "step_recon": 32 * inner + 2 * strips,
+        "step_recv": 32 * cells + (4 + 4 * accum_bytes) * inner + 4 * nrec,
     }
     return table[kind]
 
@@ -308,7 +319,7 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
-    kern = {k: ss.kernel_ms(k) for k in ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv")}
+    kern = {k: ss.kernel_ms(k) for k in KERNEL_FAMILIES}
     tiles = ss.tile_heights()
     if args.profile_only:
         ss.close()
@@ -551,7 +562,7 @@ def run_real(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     ms_total = e0.elapsed_time(e1)
-    kern = {k: ss.kernel_ms(k) for k in ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv")}
+    kern = {k: ss.kernel_ms(k) for k in KERNEL_FAMILIES}
     # e2e: file -> images, every step
     img_host = torch.empty((s.nz, s.nx), dtype=torch.float32, pin_memory=True)
     ss.reset_images()
