@@ -80,6 +80,11 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
 
     constexpr bool fast = FAST;   // the host launches interior tiles and the others apart
     const ShotK k = shot_ints(S);
+    // general tiles whose cells of a phase all have full local orders use the full-order
+    // coefficients like interior tiles (the table row of order R holds the same values)
+    const bool edgeA = x0 - 12 < R - 1 || x0 + BX + 11 > X - 1 - R;         // vx orders (columns)
+    const bool edgeB = z0 - 10 < R - 1 || z0 + TZ + 9 > Z - 1 - R;          // vz orders (rows)
+    const bool edgeC = x0 < R || x0 + BX - 1 > X - 1 - R || z0 < R || z0 + TZ - 1 > Z - 1 - R;   // p orders
     auto c10 = [&](int j) { return a.c10[j]; };
     // local orders (cuda_norderx / cuda_norderz / cuda_norder), as table rows; at least 1
     auto ordv = [&](int i, int n) { return max(min(min(i + 1, n - 1 - i), R), 1); };
@@ -114,7 +119,8 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
                     nv[j] = MODE == 3 ? __fadd_rn(comp(ov[u], j), vel_inc(dx[j], a.dtx, comp(ir[u], j)))
                                       : __fsub_rn(comp(ov[u], j), vel_inc(dx[j], a.dtx, comp(ir[u], j)));
             } else {
-                dx4<12, 13>(rw, dx, [&](int jj, int j) { return s_tab[(ordv(x + jj, X) - 1) * R + j]; });
+                if (edgeA) dx4<12, 13>(rw, dx, [&](int jj, int j) { return s_tab[(ordv(x + jj, X) - 1) * R + j]; });
+                else dx4<12, 13>(rw, dx, [&](int, int j) { return c10(j); });
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int xj = x + j;
@@ -154,7 +160,7 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
         }
         const float *col = &sp[(UQ * rg) * PW + 24 + 4 * q];   // staged row of grid row zq-9, word of column x
         float dz[UQ][4];
-        if (fast) dz4<UQ, PW>(col, dz, [&](int, int, int j) { return c10(j); });
+        if (fast || !edgeB) dz4<UQ, PW>(col, dz, [&](int, int, int j) { return c10(j); });
         else dz4<UQ, PW>(col, dz, [&](int u, int, int j) { return s_tab[(ordv(zq + u, Z) - 1) * R + j]; });
 #pragma unroll
         for (int u = 0; u < UQ; u++) {
@@ -235,7 +241,7 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
         const float *rowb = &svx[(UQ * rg) * VXW + 4 * q];   // new vx of row zq, word of column x-12
         const float *colb = &svz[(UQ * rg) * BX + 4 * q];    // new vz of row zq-10, word of column x
         float dz[UQ][4];
-        if (fast) dz4<UQ, BX>(colb, dz, [&](int, int, int j) { return c10(j); });
+        if (fast || !edgeC) dz4<UQ, BX>(colb, dz, [&](int, int, int j) { return c10(j); });
         else
             dz4<UQ, BX>(colb, dz, [&](int u, int jj, int j) {
                 const int xj = x + jj, zz = zq + u;
@@ -270,11 +276,13 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
                 }
                 continue;
             }
-            dx4<11, 12>(rowb + u * VXW, dx, [&](int jj, int j) {
-                const int xj = x + jj;
-                const int rp = max(min(min(min(xj, X - 1 - xj), min(z, Z - 1 - z)), R), 1);
-                return s_tab[(rp - 1) * R + j];
-            });
+            if (edgeC)
+                dx4<11, 12>(rowb + u * VXW, dx, [&](int jj, int j) {
+                    const int xj = x + jj;
+                    const int rp = max(min(min(min(xj, X - 1 - xj), min(z, Z - 1 - z)), R), 1);
+                    return s_tab[(rp - 1) * R + j];
+                });
+            else dx4<11, 12>(rowb + u * VXW, dx, [&](int, int j) { return c10(j); });
             const float c1z = S.pml[o.c1z + z], ic2z = S.pml[o.ic2z + z];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
