@@ -133,9 +133,14 @@ struct rtm_session {
     // rows per tile (measured): 32 for the forward and receiver velocity kernels, 16 for the
     // velocity reconstruction and the pressure kernels
     int bz_vel = 32, bz_vel_recon = 16, bz_pres = 16;
-    // kernel form: four columns by U rows per thread (rtm_stencil_v.cu, default) or one column
-    // per thread (rtm_stencil.cu, RTM_B200_KERNELS=scalar); the results are the same bits
-    bool vec = true;
+    // kernel form per family (forward/receiver velocity, reconstruction velocity, forward/receiver
+    // pressure, reconstruction pressure): four columns by U rows per thread (rtm_stencil_v.cu)
+    // or one column per thread (rtm_stencil.cu); the results are the same bits.  Chosen by the
+    // tuner with the tile heights; without it the measured defaults (one column per thread for
+    // the full-grid kernels, four columns for the reconstruction), or all of one form with
+    // RTM_B200_KERNELS=scalar|vector.
+    bool vec[4] = {false, true, false, true};
+    bool forms_fixed = false;
     bool tune = true;                // choose the tile heights per launch shape by timing them
     // whole-step kernel (rtm_step.cu): velocity and pressure of a step in one launch over
     // tz_step-row tiles, two buffers per field, four descriptor tables (which buffer is
@@ -450,8 +455,10 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         if ((e = std::getenv("RTM_B200_TUNE")) && *e && std::atoi(e) == 0) ss->tune = false;
         e = std::getenv("RTM_B200_KERNELS");
         if (e && *e) {
-            if (!std::strcmp(e, "scalar")) ss->vec = false;
-            else if (std::strcmp(e, "vector")) return fail(RTM_ERR_ARG, "RTM_B200_KERNELS must be scalar or vector");
+            if (std::strcmp(e, "scalar") && std::strcmp(e, "vector"))
+                return fail(RTM_ERR_ARG, "RTM_B200_KERNELS must be scalar or vector");
+            for (bool &v : ss->vec) v = !std::strcmp(e, "vector");
+            ss->forms_fixed = true;
         }
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
         if (o.accum_fp64 < 0 || o.accum_fp64 > 2) return fail(RTM_ERR_ARG, "accum_fp64 must be 0, 1 or 2");
@@ -900,15 +907,21 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     return RTM_OK;
 }
 
+// The kernel forms as bits (1: four columns per thread) of vel, vel_recon, pres, pres_recon.
+static int form_bits(const rtm_session *ss)
+{
+    return (ss->vec[0] ? 1 : 0) | (ss->vec[1] ? 2 : 0) | (ss->vec[2] ? 4 : 0) | (ss->vec[3] ? 8 : 0);
+}
+
 // Stencil launches in the session's kernel form.
 static void vel_step(rtm_session *ss, int mode, int bz, const StepArgs &a, int ntiles)
 {
-    if (ss->vec) launch_vel4(mode, bz, a, ntiles, ss->stream);
+    if (ss->vec[mode == RTM_WAVE_RECON ? 1 : 0]) launch_vel4(mode, bz, a, ntiles, ss->stream);
     else launch_vel(mode, bz, a, ntiles, ss->stream);
 }
 static void pres_step(rtm_session *ss, int mode, int bz, const StepArgs &a, int ntiles, int record)
 {
-    if (ss->vec) launch_pres4(mode, bz, a, ntiles, record, ss->stream);
+    if (ss->vec[mode == RTM_WAVE_RECON ? 3 : 2]) launch_pres4(mode, bz, a, ntiles, record, ss->stream);
     else launch_pres(mode, bz, a, ntiles, record, ss->stream);
 }
 
@@ -1048,7 +1061,7 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
     } else {
         const int pa0 = br.pa;
         int rc = run_pass(ss, {0, br.n, br.ntiles, br.ntiles_p, br.max_strip_len, nsteps, save, record, ss->bz_vel,
-                               ss->bz_pres, ss->vec, ss->fused, ss->tz_step, pa0, br.pb}, loop);
+                               ss->bz_pres, form_bits(ss), ss->fused, ss->tz_step, pa0, br.pb}, loop);
         // a replayed graph swaps the buffers as the captured loop did
         if (!rc && ss->fused && ss->o.use_graph) br.pa = pa0 ^ (nsteps & 1);
         if (rc) {
@@ -1202,7 +1215,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     } else {
         const int pa0 = br.pa, pb0 = br.pb;
         int rc = run_pass(ss, {1, n, br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr, max_nxi, max_nzi,
-                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->vec, ss->fused,
+                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, form_bits(ss), ss->fused,
                                ss->tz_step, pa0, pb0}, loop);
         if (!rc && ss->fused && ss->o.use_graph) {   // a replayed graph swaps as the captured loop did
             br.pa = pa0 ^ ((s.nt - 1) & 1);
@@ -1243,20 +1256,24 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     return RTM_OK;
 }
 
-// ---- tile-height tuner ---------------------------------------------------------------
-// The stencil kernels take 8-, 16- or 32-row tiles; which is fastest depends on the grid
-// (partial tiles, the share of PML-band and edge tiles), on the shots per launch (blocks to
-// fill 148 SMs) and on the kernel form.  Before the first batch of a launch shape, each height
-// is timed on that batch's own buffers: two untimed and four timed source-pass steps (velocity
-// and pressure) and backward steps (reconstruction and receiver pass) with CUDA events per
-// kernel, no strips saved.  Each kernel family keeps its fastest height: forward and receiver
-// velocity (bz_vel), reconstruction velocity (bz_vel_recon), pressure (bz_pres).  The batch is
-// set up again afterwards, so the trial steps leave nothing behind; tile heights do not change
-// the results (tested bit for bit).  Choices are kept per process by launch shape and, with
-// RTM_B200_TUNE_CACHE=<file>, in that file ("key vel vel_recon pres" lines) across processes.
+// ---- tile-height and kernel-form tuner ------------------------------------------------
+// The split stencil kernels take 8-, 16- or 32-row tiles in two forms (one column per thread;
+// four columns by U rows per thread); which is fastest depends on the grid (partial tiles, the
+// share of PML-band and edge tiles), on the shots per launch (blocks to fill 148 SMs) and on
+// the kernel.  Before the first batch of a launch shape, every (height, form) is timed on that
+// batch's own buffers: two untimed and four timed source-pass steps (velocity and pressure)
+// and backward steps (reconstruction and receiver pass) with CUDA events per kernel, no strips
+// saved.  Forward/receiver velocity and reconstruction velocity each keep their fastest pair;
+// the pressure kernels share one height (one tile list), and the forward/receiver and the
+// reconstruction pressure take their faster form at it.  The batch is set up again afterwards,
+// so the trial steps leave nothing behind; heights and forms do not change the results (tested
+// bit for bit).  Choices are kept per process by launch shape and, with
+// RTM_B200_TUNE_CACHE=<file>, in that file ("key vel vel_recon pres forms" lines, forms a
+// bit set of vel, vel_recon, pres, pres_recon) across processes.  The whole-step kernel's tile
+// height is chosen the same way (tune_step_height).
 namespace {
 std::mutex g_tune_mu;
-std::map<std::string, std::array<int, 3>> g_tune;
+std::map<std::string, std::array<int, 4>> g_tune;
 bool g_tune_loaded = false;
 }  // namespace
 
@@ -1266,7 +1283,7 @@ static std::string tune_key(rtm_session *ss, int k0, int n)
     for (int j = 0; j < n; j++) xmax = std::max(xmax, ss->shots[k0 + j].X);
     char b[200];
     std::snprintf(b, sizeof b, "%s/X%d/Z%d/npml%d/n%d/strip%d/gather%d/acc%d/extra%d/mode%d",
-                  ss->fused ? "step" : ss->vec ? "vector" : "scalar",
+                  ss->fused ? "step" : ss->forms_fixed ? (ss->vec[0] ? "vector" : "scalar") : "split",
                   xmax, ss->shots[k0].Z, ss->s.npml, n, ss->o.strip_precision, ss->o.gather_precision, ss->o.accum_fp64,
                   ss->o.extra_images, ss->s.mode);
     return b;
@@ -1274,7 +1291,7 @@ static std::string tune_key(rtm_session *ss, int k0, int n)
 
 // The whole-step kernel's tile height (16 or 32 rows), timed the same way: source-pass,
 // reconstruction and receiver steps, each kind's fast and general launches together.  The
-// choice is recorded as "key tz tz tz".
+// choice is recorded as "key tz tz tz 0".
 static int tune_step_height(rtm_session *ss, int k0, int n, const std::string &key, const char *path)
 {
     const int cand[2] = {16, 32};
@@ -1328,10 +1345,10 @@ static int tune_step_height(rtm_session *ss, int k0, int n, const std::string &k
         std::printf("rtm_b200: step tile height for %s: %d (ms per 4 steps: 16 rows %.3f, 32 rows %.3f)\n", key.c_str(),
                     tz, ms[0], ms[1]);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tune[key] = {tz, tz, tz};
+    g_tune[key] = {tz, tz, tz, 0};
     if (path && *path)
         if (FILE *f = std::fopen(path, "a")) {
-            std::fprintf(f, "%s %d %d %d\n", key.c_str(), tz, tz, tz);
+            std::fprintf(f, "%s %d %d %d 0\n", key.c_str(), tz, tz, tz);
             std::fclose(f);
         }
     return RTM_OK;
@@ -1348,8 +1365,9 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             g_tune_loaded = true;
             if (FILE *f = std::fopen(path, "r")) {
                 char k[200];
-                int v[3];
-                while (std::fscanf(f, "%199s %d %d %d", k, &v[0], &v[1], &v[2]) == 4) g_tune[k] = {v[0], v[1], v[2]};
+                int v[4];
+                while (std::fscanf(f, "%199s %d %d %d %d", k, &v[0], &v[1], &v[2], &v[3]) == 5)
+                    g_tune[k] = {v[0], v[1], v[2], v[3]};
                 std::fclose(f);
             }
         }
@@ -1362,13 +1380,19 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             ss->bz_vel = it->second[0];
             ss->bz_vel_recon = it->second[1];
             ss->bz_pres = it->second[2];
+            for (int f = 0; f < 4; f++) ss->vec[f] = (it->second[3] >> f) & 1;
             return RTM_OK;
         }
     }
     if (ss->fused) return tune_step_height(ss, k0, n, key, path);
-    const int cand[3] = {8, 16, 32};
+    // candidates: tile height x kernel form (both forms unless RTM_B200_KERNELS fixes one)
+    std::vector<std::pair<int, int>> cand;   // (bz, vector form)
+    for (int bz : {8, 16, 32})
+        for (int f = 0; f < 2; f++)
+            if (!ss->forms_fixed || f == (ss->vec[0] ? 1 : 0)) cand.push_back({bz, f});
+    const int nc = (int)cand.size();
     const char *names[6] = {"vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv"};
-    double ms[3][6] = {};
+    std::vector<std::array<double, 6>> ms(nc, std::array<double, 6>{});
     cudaEvent_t ev[2][6][4];
     for (auto &a : ev)
         for (auto &b : a)
@@ -1376,8 +1400,9 @@ static int tune_heights(rtm_session *ss, int k0, int n)
     cudaStream_t st = ss->stream;
     int rc = RTM_OK;
     const int steps = 6, warm = 2;
-    for (int c = 0; c < 3 && rc == RTM_OK; c++) {
-        ss->bz_vel = ss->bz_vel_recon = ss->bz_pres = cand[c];
+    for (int c = 0; c < nc && rc == RTM_OK; c++) {
+        ss->bz_vel = ss->bz_vel_recon = ss->bz_pres = cand[c].first;
+        for (bool &v : ss->vec) v = cand[c].second != 0;
         BatchRun br;
         if ((rc = batch_setup(ss, k0, n, br))) break;
         StepArgs a = br.a;
@@ -1411,32 +1436,50 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             for (auto &e : b) cudaEventDestroy(e);
     if (rc) return rc;
     if ((rc = check_kernel_flag(ss))) return rc;
-    auto best = [&](std::initializer_list<int> ks) {
+    // velocity families: the fastest (height, form) each; pressure families share a height,
+    // each taking its faster form at that height
+    auto argmin = [&](auto cost) {
         int bi = 0;
-        double bm = 1e300;
-        for (int c = 0; c < 3; c++) {
-            double m = 0;
-            for (int k : ks) m += ms[c][k];
-            if (m < bm) bm = m, bi = c;
-        }
-        return cand[bi];
+        for (int c = 1; c < nc; c++)
+            if (cost(c) < cost(bi)) bi = c;
+        return bi;
     };
-    std::array<int, 3> pick = {best({0, 4}), best({2}), best({1, 3, 5})};
-    ss->bz_vel = pick[0];
-    ss->bz_vel_recon = pick[1];
-    ss->bz_pres = pick[2];
+    const int cv = argmin([&](int c) { return ms[c][0] + ms[c][4]; });
+    const int cr = argmin([&](int c) { return ms[c][2]; });
+    int best_bz = 0, fp = 0, fpr = 0;
+    double best = 1e300;
+    for (int bz : {8, 16, 32}) {
+        double pf = 1e300, pr = 1e300;
+        int f1 = 0, f2 = 0;
+        for (int c = 0; c < nc; c++)
+            if (cand[c].first == bz) {
+                if (ms[c][1] + ms[c][5] < pf) pf = ms[c][1] + ms[c][5], f1 = cand[c].second;
+                if (ms[c][3] < pr) pr = ms[c][3], f2 = cand[c].second;
+            }
+        if (pf + pr < best) best = pf + pr, best_bz = bz, fp = f1, fpr = f2;
+    }
+    ss->bz_vel = cand[cv].first;
+    ss->bz_vel_recon = cand[cr].first;
+    ss->bz_pres = best_bz;
+    ss->vec[0] = cand[cv].second;
+    ss->vec[1] = cand[cr].second;
+    ss->vec[2] = fp;
+    ss->vec[3] = fpr;
+    const std::array<int, 4> pick = {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, form_bits(ss)};
     if (ss->o.verbose) {
-        std::printf("rtm_b200: tile heights for %s: vel %d, vel_recon %d, pres %d (ms per 4 steps:", key.c_str(), pick[0],
-                    pick[1], pick[2]);
-        for (int c = 0; c < 3; c++)
-            for (int k = 0; k < 6; k++) std::printf(" %s@%d=%.3f", names[k], cand[c], ms[c][k]);
+        std::printf("rtm_b200: tiles for %s: vel %d%s, vel_recon %d%s, pres %d%s/%s (ms per 4 steps:", key.c_str(),
+                    pick[0], ss->vec[0] ? "v" : "s", pick[1], ss->vec[1] ? "v" : "s", pick[2], ss->vec[2] ? "v" : "s",
+                    ss->vec[3] ? "v" : "s");
+        for (int c = 0; c < nc; c++)
+            for (int k = 0; k < 6; k++)
+                std::printf(" %s@%d%s=%.3f", names[k], cand[c].first, cand[c].second ? "v" : "s", ms[c][k]);
         std::printf(")\n");
     }
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune[key] = pick;
     if (path && *path)
         if (FILE *f = std::fopen(path, "a")) {
-            std::fprintf(f, "%s %d %d %d\n", key.c_str(), pick[0], pick[1], pick[2]);
+            std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), pick[0], pick[1], pick[2], pick[3]);
             std::fclose(f);
         }
     return RTM_OK;

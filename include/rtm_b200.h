@@ -234,9 +234,12 @@ unsigned long long rtm_session_config_hash(rtm_session *ss);
  * number of guard bands of the session (0 when the mode is off). */
 int rtm_session_guard_count(rtm_session *ss);
 /* Rows per stencil tile in use: forward and receiver velocity, reconstruction velocity,
- * pressure (with the whole-step kernel, its tile height in all three).  Chosen per launch shape by timing 8, 16 and 32 rows before the first batch of that
- * shape (RTM_B200_TUNE=0, or RTM_B200_BZ_VEL / _VEL_RECON / _PRES set, turns that off; choices
- * persist across processes in RTM_B200_TUNE_CACHE=<file>).  Any pointer may be NULL. */
+ * pressure (with the whole-step kernel, its tile height in all three).  Chosen, with the kernel
+ * form of each family, per launch shape by timing 8-, 16- and 32-row tiles in both forms before
+ * the first batch of that shape (RTM_B200_TUNE=0, or RTM_B200_BZ_VEL / _VEL_RECON / _PRES set,
+ * turns that off; RTM_B200_KERNELS=scalar|vector fixes the form; choices persist across
+ * processes in RTM_B200_TUNE_CACHE=<file>).  Any pointer may be NULL. */
+
 int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres);
 /* Number of traces of shot k. */
 int rtm_session_nrec(rtm_session *ss, int k);
