@@ -239,7 +239,6 @@ int rtm_session_guard_count(rtm_session *ss);
  * the first batch of that shape (RTM_B200_TUNE=0, or RTM_B200_BZ_VEL / _VEL_RECON / _PRES set,
  * turns that off; RTM_B200_KERNELS=scalar|vector fixes the form; choices persist across
  * processes in RTM_B200_TUNE_CACHE=<file>).  Any pointer may be NULL. */
-
 int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres);
 /* Number of traces of shot k. */
 int rtm_session_nrec(rtm_session *ss, int k);
