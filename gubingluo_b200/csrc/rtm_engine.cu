@@ -150,6 +150,7 @@ struct rtm_session {
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
+    int *d_counts = nullptr;         // tile counts of the batch's four lists (fixed-grid launches)
     int max_tiles = 0;
     std::map<std::string, rtm::KernelTiming> timing;
     int launches = 0;
@@ -632,6 +633,8 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->d_tiles_r = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_tiles_pr = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_fin = ss->arena.take(finalize_shot_size() * B);
+    ss->d_counts = (int *)ss->arena.take(4 * sizeof(int));
+    if (!ss->d_counts) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_tiles_r || !ss->d_tiles_pr || !ss->d_fin)
         return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     CK(cudaStreamSynchronize(ss->stream));
@@ -709,7 +712,22 @@ struct BatchRun {
     StepArgs a{};
     // whole-step kernel: which buffer holds the current source (pa) and receiver (pb) fields
     int pa = 0, pb = 0;
+    // grid of the launches over each tile list: its tile count, or with use_graph a bound that
+    // depends only on the batch size (n times the most tiles any shot of the session has), so
+    // that one captured graph serves batches of any windows; likewise the strip kernels' and
+    // the other imaging conditions' extents
+    int grid[4] = {0, 0, 0, 0};
+    int strip_grid = 0, ex_nxi = 0, ex_nzi = 0;
 };
+
+// Launch arguments of a stencil launch over tile list L: the grid, and in fixed-grid mode the
+// device tile counts that the blocks past the batch's tiles check.
+static int list_grid(rtm_session *ss, BatchRun &br, StepArgs &a, int L)
+{
+    a.counts = ss->o.use_graph ? ss->d_counts : nullptr;
+    a.list = L;
+    return br.grid[L];
+}
 
 // Descriptor tables of a batch.  One table (hd as built) for the split kernels; with the
 // whole-step kernel four, one per (pa, pb): in table 2 pa + pb, `a` is the source wavefield's
@@ -742,6 +760,71 @@ static int upload_tables(rtm_session *ss, const BatchRun &br)
     // the host copy must live until the copy has read it
     CK(cudaStreamSynchronize(ss->stream));
     return RTM_OK;
+}
+
+// The tiles of one shot (batch slot j) in the four lists of a batch: 0 full-grid velocity
+// (whole-step kernel: full-grid interior tiles), 1 full-grid pressure (whole-step: the other
+// full-grid tiles), 2 reconstruction velocity (whole-step: interior tiles of the
+// reconstruction region), 3 reconstruction pressure (whole-step: the other tiles there).
+static void shot_tiles(const rtm_session *ss, const ShotState &sh, int j, bool fast, std::vector<TileRef> *const L[4])
+{
+    const rtm_survey &s = ss->s;
+    std::vector<TileRef> &tiles = *L[0], &tiles_p = *L[1], &tiles_r = *L[2], &tiles_pr = *L[3];
+    // whole-grid tiles, and the reconstruction's tiles: it writes only the interior and the
+    // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10)
+    const int xr0 = (s.npml - RTM_RADIUS) & ~3, xr1 = sh.X - s.npml + RTM_RADIUS;
+    const int zr0 = s.npml - RTM_RADIUS, zr1 = sh.Z - s.npml + RTM_RADIUS;
+    // velocity tiles: interior when every column lies in [npml, X-npml-1) and every row in
+    // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies
+    auto add_tiles = [&](std::vector<TileRef> &v, int bz, int xa, int xb, int za, int zb) {
+        for (int z0 = za; z0 < zb; z0 += bz)
+            for (int x0 = xa; x0 < xb; x0 += RTM_BX) {
+                const bool inside = x0 >= s.npml && x0 + RTM_BX <= sh.X - s.npml - 1 && z0 >= s.npml &&
+                                    z0 + bz <= sh.Z - s.npml - 1;
+                v.push_back({j, x0, z0, (fast && inside) ? 1 : 0});
+            }
+    };
+    if (ss->fused) {
+        // whole-step tiles of tz_step rows, interior ones (cells and velocity halo in the
+        // interior, full orders, no source or receiver) in their own lists: full grid
+        // (fast: tiles, others: tiles_p) and reconstruction region (tiles_r, tiles_pr)
+        const int tz = ss->tz_step, np = std::max(s.npml, RTM_RADIUS);
+        auto fast_tile = [&](int x0, int z0, bool recon) {
+            const bool vel_in = x0 - 12 >= np && x0 + RTM_BX + 12 <= sh.X - np - 1 && z0 - 10 >= np &&
+                                z0 + tz + 10 <= sh.Z - np - 1;
+            const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x0 + RTM_BX && z0 < sh.sbz0 + sh.sbnz &&
+                             sh.sbz0 < z0 + tz;
+            const bool rec = !recon && sh.g.rz >= z0 && sh.g.rz < z0 + tz && x0 < sh.g.rx0 + sh.g.nrec &&
+                             sh.g.rx0 < x0 + RTM_BX;
+            return fast && vel_in && !src && !rec;
+        };
+        for (int z0 = 0; z0 < sh.Z; z0 += tz)
+            for (int x0 = 0; x0 < sh.X; x0 += RTM_BX)
+                (fast_tile(x0, z0, false) ? tiles : tiles_p).push_back({j, x0, z0, 1});
+        for (int z0 = zr0; z0 < zr1; z0 += tz)
+            for (int x0 = xr0; x0 < xr1; x0 += RTM_BX)
+                (fast_tile(x0, z0, true) ? tiles_r : tiles_pr).push_back({j, x0, z0, 1});
+    }
+    if (!ss->fused) add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
+    // pressure tiles: interior tiles (no PML, source or receiver cell) go to their own list
+    for (int z0 = 0; z0 < (ss->fused ? 0 : sh.Z); z0 += ss->bz_pres)
+        for (int x0 = 0; x0 < sh.X; x0 += RTM_BX) {
+            const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
+            const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
+            const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
+            const bool rec = sh.g.rz >= z0 && sh.g.rz < z1 && x0 < sh.g.rx0 + sh.g.nrec && sh.g.rx0 < x1;
+            tiles_p.push_back({j, x0, z0, (fast && inside && !src && !rec) ? 1 : 0});
+        }
+    if (!ss->fused) add_tiles(tiles_r, ss->bz_vel_recon, xr0, xr1, zr0, zr1);
+    // reconstruction pressure tiles: interior when inside the pressure interior with no
+    // source cell
+    for (int z0 = zr0; z0 < (ss->fused ? zr0 : zr1); z0 += ss->bz_pres)
+        for (int x0 = xr0; x0 < xr1; x0 += RTM_BX) {
+            const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
+            const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
+            const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
+            tiles_pr.push_back({j, x0, z0, (fast && inside && !src) ? 1 : 0});
+        }
 }
 
 // Bind shots [k0, k0+n) to slots 0..n-1, zero their wavefields and accumulators, upload
@@ -802,61 +885,10 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
             }
             d.tmaps = (const char *)ss->d_tmaps + (size_t)j * RTM_TMAP_COUNT * RTM_TMAP_BYTES;
         }
-        // whole-grid tiles, and the reconstruction's tiles: it writes only the interior and the
-        // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10)
-        const int xr0 = (s.npml - RTM_RADIUS) & ~3, xr1 = sh.X - s.npml + RTM_RADIUS;
-        const int zr0 = s.npml - RTM_RADIUS, zr1 = sh.Z - s.npml + RTM_RADIUS;
-        // velocity tiles: interior when every column lies in [npml, X-npml-1) and every row in
-        // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies
-        auto add_tiles = [&](std::vector<TileRef> &v, int bz, int xa, int xb, int za, int zb) {
-            for (int z0 = za; z0 < zb; z0 += bz)
-                for (int x0 = xa; x0 < xb; x0 += RTM_BX) {
-                    const bool inside = x0 >= s.npml && x0 + RTM_BX <= sh.X - s.npml - 1 && z0 >= s.npml &&
-                                        z0 + bz <= sh.Z - s.npml - 1;
-                    v.push_back({j, x0, z0, (fast && inside) ? 1 : 0});
-                }
-        };
-        if (ss->fused) {
-            // whole-step tiles of tz_step rows, interior ones (cells and velocity halo in the
-            // interior, full orders, no source or receiver) in their own lists: full grid
-            // (fast: tiles, others: tiles_p) and reconstruction region (tiles_r, tiles_pr)
-            const int tz = ss->tz_step, np = std::max(s.npml, RTM_RADIUS);
-            auto fast_tile = [&](int x0, int z0, bool recon) {
-                const bool vel_in = x0 - 12 >= np && x0 + RTM_BX + 12 <= sh.X - np - 1 && z0 - 10 >= np &&
-                                    z0 + tz + 10 <= sh.Z - np - 1;
-                const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x0 + RTM_BX && z0 < sh.sbz0 + sh.sbnz &&
-                                 sh.sbz0 < z0 + tz;
-                const bool rec = !recon && sh.g.rz >= z0 && sh.g.rz < z0 + tz && x0 < sh.g.rx0 + sh.g.nrec &&
-                                 sh.g.rx0 < x0 + RTM_BX;
-                return fast && vel_in && !src && !rec;
-            };
-            for (int z0 = 0; z0 < sh.Z; z0 += tz)
-                for (int x0 = 0; x0 < sh.X; x0 += RTM_BX)
-                    (fast_tile(x0, z0, false) ? tiles : tiles_p).push_back({j, x0, z0, 1});
-            for (int z0 = zr0; z0 < zr1; z0 += tz)
-                for (int x0 = xr0; x0 < xr1; x0 += RTM_BX)
-                    (fast_tile(x0, z0, true) ? tiles_r : tiles_pr).push_back({j, x0, z0, 1});
+        {
+            std::vector<TileRef> *L[4] = {&tiles, &tiles_p, &tiles_r, &tiles_pr};
+            shot_tiles(ss, sh, j, fast, L);
         }
-        if (!ss->fused) add_tiles(tiles, ss->bz_vel, 0, sh.X, 0, sh.Z);
-        // pressure tiles: interior tiles (no PML, source or receiver cell) go to their own list
-        for (int z0 = 0; z0 < (ss->fused ? 0 : sh.Z); z0 += ss->bz_pres)
-            for (int x0 = 0; x0 < sh.X; x0 += RTM_BX) {
-                const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
-                const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
-                const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
-                const bool rec = sh.g.rz >= z0 && sh.g.rz < z1 && x0 < sh.g.rx0 + sh.g.nrec && sh.g.rx0 < x1;
-                tiles_p.push_back({j, x0, z0, (fast && inside && !src && !rec) ? 1 : 0});
-            }
-        if (!ss->fused) add_tiles(tiles_r, ss->bz_vel_recon, xr0, xr1, zr0, zr1);
-        // reconstruction pressure tiles: interior when inside the pressure interior with no
-        // source cell
-        for (int z0 = zr0; z0 < (ss->fused ? zr0 : zr1); z0 += ss->bz_pres)
-            for (int x0 = xr0; x0 < xr1; x0 += RTM_BX) {
-                const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
-                const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
-                const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
-                tiles_pr.push_back({j, x0, z0, (fast && inside && !src) ? 1 : 0});
-            }
         br.maxrec = std::max(br.maxrec, sh.g.nrec);
         br.max_strip_len = std::max(br.max_strip_len, sh.strip_len);
         size_t fb = (size_t)sh.pitch * sh.Z * 4;
@@ -875,6 +907,27 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     br.ntiles_pr = (int)tiles_pr.size();
     if (std::max(std::max(br.ntiles, br.ntiles_p), std::max(br.ntiles_r, br.ntiles_pr)) > ss->max_tiles)
         return fail(RTM_ERR_ARG, "tile table overflow");
+    const int counts[4] = {br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr};
+    CK(cudaMemcpyAsync(ss->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, st));
+    for (int L = 0; L < 4; L++) br.grid[L] = counts[L];
+    br.strip_grid = br.max_strip_len;
+    for (int j = 0; j < n; j++) {
+        br.ex_nxi = std::max(br.ex_nxi, ss->shots[k0 + j].nxi);
+        br.ex_nzi = std::max(br.ex_nzi, ss->shots[k0 + j].nzi);
+    }
+    if (o.use_graph) {   // bounds over every shot of the session
+        int most[4] = {0, 0, 0, 0};
+        for (const ShotState &sh : ss->shots) {
+            std::vector<TileRef> t4[4];
+            std::vector<TileRef> *L[4] = {&t4[0], &t4[1], &t4[2], &t4[3]};
+            shot_tiles(ss, sh, 0, fast, L);
+            for (int l = 0; l < 4; l++) most[l] = std::max(most[l], (int)t4[l].size());
+            br.strip_grid = std::max(br.strip_grid, sh.strip_len);
+            br.ex_nxi = std::max(br.ex_nxi, sh.nxi);
+            br.ex_nzi = std::max(br.ex_nzi, sh.nzi);
+        }
+        for (int l = 0; l < 4; l++) br.grid[l] = n * most[l];
+    }
     for (int j = 0; j < n; j++) {
         const Slot &sl = ss->slots[j];
         br.hd[j].an = sl.a2;
@@ -930,7 +983,7 @@ static void launch_pres_tiles(rtm_session *ss, BatchRun &br, int mode, int recor
 {
     StepArgs &a = br.a;
     a.tiles = ss->d_tiles_p;
-    pres_step(ss, mode, ss->bz_pres, a, br.ntiles_p, record);
+    pres_step(ss, mode, ss->bz_pres, a, list_grid(ss, br, a, 1), record);
     ss->launches++;
 }
 
@@ -1029,16 +1082,16 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
                 timing_begin(ss, "step_fwd", it, &e);
                 a.shots = table(ss, br);
                 a.tiles = ss->d_tiles;
-                launch_step(mode, ss->tz_step, true, a, br.ntiles, record ? 1 : 0, st);
+                launch_step(mode, ss->tz_step, true, a, list_grid(ss, br, a, 0), record ? 1 : 0, st);
                 a.tiles = ss->d_tiles_p;
-                launch_step(mode, ss->tz_step, false, a, br.ntiles_p, record ? 1 : 0, st);
+                launch_step(mode, ss->tz_step, false, a, list_grid(ss, br, a, 1), record ? 1 : 0, st);
                 timing_end(ss, e);
                 ss->launches += 2;
                 br.pa ^= 1;
             } else {
                 timing_begin(ss, "vel_fwd", it, &e);
                 a.tiles = ss->d_tiles;
-                vel_step(ss, mode, ss->bz_vel, a, br.ntiles);
+                vel_step(ss, mode, ss->bz_vel, a, list_grid(ss, br, a, 0));
                 timing_end(ss, e);
                 timing_begin(ss, "pres_fwd", it, &e);
                 launch_pres_tiles(ss, br, mode, record ? 1 : 0);
@@ -1046,7 +1099,7 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
                 ss->launches += 1;
             }
             if (save) {
-                launch_strip_save(table(ss, br), br.n, br.max_strip_len, it, a.ring, o.strip_precision, st);
+                launch_strip_save(table(ss, br), br.n, br.strip_grid, it, a.ring, o.strip_precision, st);
                 ss->launches++;
             }
             if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
@@ -1060,7 +1113,7 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
         CK(cudaGetLastError());
     } else {
         const int pa0 = br.pa;
-        int rc = run_pass(ss, {0, br.n, br.ntiles, br.ntiles_p, br.max_strip_len, nsteps, save, record, ss->bz_vel,
+        int rc = run_pass(ss, {0, br.n, br.grid[0], br.grid[1], br.strip_grid, nsteps, save, record, ss->bz_vel,
                                ss->bz_pres, form_bits(ss), ss->fused, ss->tz_step, pa0, br.pb}, loop);
         // a replayed graph swaps the buffers as the captured loop did
         if (!rc && ss->fused && ss->o.use_graph) br.pa = pa0 ^ (nsteps & 1);
@@ -1136,7 +1189,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     ss->launches++;
     // the other imaging conditions compare each step with the pressures before it
     // (rtm_model.cu:419-420); their kernel keeps ps_pre/p_pre current from then on
-    int max_nxi = 0, max_nzi = 0;
+    int max_nxi = 0, max_nzi = 0;   // (the launches use br.ex_nxi, br.ex_nzi)
     if (o.extra_images)
         for (int j = 0; j < n; j++) {
             const ShotState &sh = ss->shots[br.k0 + j];
@@ -1165,22 +1218,22 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
                 timing_begin(ss, "step_recon", it, &e);
                 a.shots = table(ss, br);
                 a.tiles = ss->d_tiles_r;
-                launch_step(RTM_WAVE_RECON, ss->tz_step, true, a, br.ntiles_r, 0, st);
+                launch_step(RTM_WAVE_RECON, ss->tz_step, true, a, list_grid(ss, br, a, 2), 0, st);
                 a.tiles = ss->d_tiles_pr;
-                launch_step(RTM_WAVE_RECON, ss->tz_step, false, a, br.ntiles_pr, 0, st);
+                launch_step(RTM_WAVE_RECON, ss->tz_step, false, a, list_grid(ss, br, a, 3), 0, st);
                 timing_end(ss, e);
                 br.pa ^= 1;
                 timing_begin(ss, "step_recv", it, &e);
                 a.shots = table(ss, br);
                 a.tiles = ss->d_tiles;
-                launch_step(RTM_WAVE_RECEIVER, ss->tz_step, true, a, br.ntiles, 0, st);
+                launch_step(RTM_WAVE_RECEIVER, ss->tz_step, true, a, list_grid(ss, br, a, 0), 0, st);
                 a.tiles = ss->d_tiles_p;
-                launch_step(RTM_WAVE_RECEIVER, ss->tz_step, false, a, br.ntiles_p, 0, st);
+                launch_step(RTM_WAVE_RECEIVER, ss->tz_step, false, a, list_grid(ss, br, a, 1), 0, st);
                 timing_end(ss, e);
                 br.pb ^= 1;
                 ss->launches += 4;
                 if (o.extra_images) {
-                    launch_image_extra(table(ss, br), n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx,
+                    launch_image_extra(table(ss, br), n, br.ex_nxi, br.ex_nzi, o.extra_images == 2, o.accum_fp64, s.dx,
                                        s.dz, s.dt, st);
                     ss->launches++;
                 }
@@ -1188,22 +1241,22 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             }
             timing_begin(ss, "vel_recon", it, &e);
             a.tiles = ss->d_tiles_r;
-            vel_step(ss, RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r);
+            vel_step(ss, RTM_WAVE_RECON, ss->bz_vel_recon, a, list_grid(ss, br, a, 2));
             timing_end(ss, e);
             timing_begin(ss, "pres_recon", it, &e);
             a.tiles = ss->d_tiles_pr;
-            pres_step(ss, RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0);
+            pres_step(ss, RTM_WAVE_RECON, ss->bz_pres, a, list_grid(ss, br, a, 3), 0);
             timing_end(ss, e);
             timing_begin(ss, "vel_recv", it, &e);
             a.tiles = ss->d_tiles;
-            vel_step(ss, RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles);
+            vel_step(ss, RTM_WAVE_RECEIVER, ss->bz_vel, a, list_grid(ss, br, a, 0));
             timing_end(ss, e);
             timing_begin(ss, "pres_recv", it, &e);
             launch_pres_tiles(ss, br, RTM_WAVE_RECEIVER, 0);
             timing_end(ss, e);
             ss->launches += 3;
             if (o.extra_images) {
-                launch_image_extra(ss->d_shots, n, max_nxi, max_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz,
+                launch_image_extra(ss->d_shots, n, br.ex_nxi, br.ex_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz,
                                    s.dt, st);
                 ss->launches++;
             }
@@ -1214,7 +1267,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         CK(cudaGetLastError());
     } else {
         const int pa0 = br.pa, pb0 = br.pb;
-        int rc = run_pass(ss, {1, n, br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr, max_nxi, max_nzi,
+        int rc = run_pass(ss, {1, n, br.grid[0], br.grid[1], br.grid[2], br.grid[3], br.ex_nxi, br.ex_nzi,
                                a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, form_bits(ss), ss->fused,
                                ss->tz_step, pa0, pb0}, loop);
         if (!rc && ss->fused && ss->o.use_graph) {   // a replayed graph swaps as the captured loop did

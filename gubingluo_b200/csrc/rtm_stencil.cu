@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_B
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1vz[BZ], s_ic2vz[BZ];
+    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
     const TileRef t = a.tiles[blockIdx.x];   // reconstruction: tiles of the interior + strips only
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
@@ -243,6 +244,7 @@ __global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1z[BZ], s_ic2z[BZ];
+    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
     const TileRef t = a.tiles[blockIdx.x];   // reconstruction: tiles of the interior + strips only
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;

@@ -89,6 +89,9 @@ __device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err)
         if (mbar_done(bar)) break;
     return false;
 }
+// Fixed-grid launches: true for the blocks past the batch's tile list (see StepArgs::counts).
+__device__ __forceinline__ bool tile_beyond(const StepArgs &a) { return a.counts && (int)blockIdx.x >= a.counts[a.list]; }
+
 __device__ __forceinline__ const void *tmap_of(const ShotDev &S, int which)
 {
     return (const char *)S.tmaps + which * RTM_TMAP_BYTES;

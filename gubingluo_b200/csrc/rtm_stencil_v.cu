@@ -36,6 +36,7 @@ __global__ void __launch_bounds__(32 * BZ / U, min_blocks(32 * BZ / U, 80)) k_ve
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1vz[BZ], s_ic2vz[BZ];
+    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
     const TileRef t = a.tiles[blockIdx.x];
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
@@ -158,6 +159,7 @@ __global__ void __launch_bounds__(32 * BZ / U, min_blocks(32 * BZ / U, MODE == 2
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1z[BZ], s_ic2z[BZ];
+    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
     const TileRef t = a.tiles[blockIdx.x];
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;

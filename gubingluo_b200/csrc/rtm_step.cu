@@ -58,6 +58,7 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
     float *svz = svx + TZ * VXW;      // [VZH][BX]  new vz
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
+    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
     const TileRef t = a.tiles[blockIdx.x];
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;

@@ -154,4 +154,9 @@ struct StepArgs {
     int strip_prec, gather_prec, accum_fp64;
     int ring;               // staging-ring slot for fp16/bf16 strips
     int *err;               // device error flag: set non-zero by a kernel whose bounded wait gave up
+    // fixed-grid launches (CUDA-graph replays whose grid covers the largest tile list of the
+    // session): counts[list] is the batch's own tile count, blocks past it return at once;
+    // counts == nullptr: the grid is the tile count
+    const int *counts;
+    int list;
 };
