@@ -104,6 +104,8 @@ def lib() -> C.CDLL:
     L.rtm_session_nrec.argtypes = [vp, C.c_int]
     L.rtm_session_get_pml.argtypes = [vp, C.c_int, vp, vp, vp, vp]
     L.rtm_session_tile_heights.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.rtm_session_prepare.argtypes = [vp, C.c_int, C.c_int]
+    L.rtm_session_batch_size.argtypes = [vp]
     L.rtm_session_stream.argtypes = [vp]
     L.rtm_session_stream.restype = vp
     L.rtm_session_kernel_ms.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int)]
@@ -351,6 +353,14 @@ class Session:
         n = C.c_int(0)
         ms = lib().rtm_session_kernel_ms(self.h, name.encode(), C.byref(n))
         return ms, n.value
+
+    def prepare(self, k0: int, n: int):
+        """Choose the kernel configuration for the batch shape of shots [k0, k0+n) now."""
+        _check(lib().rtm_session_prepare(self.h, k0, n))
+
+    def batch_size(self) -> int:
+        """Shots per launch (batch slots) of the session."""
+        return lib().rtm_session_batch_size(self.h)
 
     def tile_heights(self):
         """Rows per tile in use: {"vel", "vel_recon", "pres"} (tuned per launch shape)."""

@@ -1557,6 +1557,19 @@ static int run_batch(rtm_session *ss, int k0, int n)
 
 int session_batch_size(rtm_session *ss) { return ss ? ss->B : 0; }
 
+// Choose the kernel configuration of the batch shape of shots [k0, k0+n) now (the tuner's
+// trial steps), so that a timed run does not include them.
+int session_prepare(rtm_session *ss, int k0, int n)
+{
+    if (!ss || k0 < 0 || n < 1 || n > ss->B || k0 + n > (int)ss->shots.size())
+        return fail(RTM_ERR_ARG, "bad shot range");
+    CK(cudaSetDevice(ss->dev));
+    int rc = tune_heights(ss, k0, n);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ss->stream));
+    return RTM_OK;
+}
+
 // Modelling only (the reference's mode-0 modelling pass, rtm_model.cu:266-290): record
 // the gathers of shots [k0, k0+n) without saving strips or migrating.
 static int model_range(rtm_session *ss, int k0, int n)
@@ -1768,6 +1781,10 @@ int rtm_session_get_pml(rtm_session *ss, int k, float *ddx, float *ddz, float *d
         if (q.out) CK(cudaMemcpy(q.out, sh.pml + q.off, sizeof(float) * q.n, cudaMemcpyDeviceToHost));
     return RTM_OK;
 }
+
+int rtm_session_prepare(rtm_session *ss, int k0, int n) { return session_prepare(ss, k0, n); }
+
+int rtm_session_batch_size(rtm_session *ss) { return session_batch_size(ss); }
 
 int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres)
 {

@@ -240,6 +240,12 @@ int rtm_session_guard_count(rtm_session *ss);
  * turns that off; RTM_B200_KERNELS=scalar|vector fixes the form; choices persist across
  * processes in RTM_B200_TUNE_CACHE=<file>).  Any pointer may be NULL. */
 int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres);
+/* Run the tuner now for the batch shape of shots [k0, k0+n) (no migration), so that a later
+ * timed rtm_session_run_range of that shape does not include its trial steps. */
+int rtm_session_prepare(rtm_session *ss, int k0, int n);
+/* Shots per launch (batch slots) of the session: options.batch, or as many as device memory
+ * holds. */
+int rtm_session_batch_size(rtm_session *ss);
 /* Number of traces of shot k. */
 int rtm_session_nrec(rtm_session *ss, int k);
 /* cudaStream_t of the session (as void*), for event timing by the caller. */
