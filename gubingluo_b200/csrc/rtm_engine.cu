@@ -872,11 +872,14 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
             const int vhr = ss->bz_vel_recon + RTM_STAGE_ZEXTRA_VEL;
             // whole-step kernel: p of both buffers of each wavefield (placeholders when off)
             const int sw = RTM_BX + 48, sh_ = ss->tz_step + 38;
-            float *a2p = ss->fused ? sl.a2.p : sl.a.p, *b2p = ss->fused ? sl.b2.p : sl.b.p;
+            const WaveDev &A1 = ss->fused ? sl.a2 : sl.a, &B1 = ss->fused ? sl.b2 : sl.b;
+            const int tz = ss->tz_step;
             struct { float *f; int w, h; } m[RTM_TMAP_COUNT] = {
                 {sl.a.p, RTM_STAGE_W, vh}, {sl.a.vx, RTM_STAGE_W, ss->bz_pres}, {sl.a.vz, RTM_BX, ph},
                 {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph},
-                {sl.a.p, RTM_STAGE_W, vhr}, {sl.a.p, sw, sh_}, {a2p, sw, sh_}, {sl.b.p, sw, sh_}, {b2p, sw, sh_}};
+                {sl.a.p, RTM_STAGE_W, vhr}, {sl.a.p, sw, sh_}, {A1.p, sw, sh_}, {sl.b.p, sw, sh_}, {B1.p, sw, sh_},
+                {sl.a.vx, RTM_STAGE_W, tz}, {A1.vx, RTM_STAGE_W, tz}, {sl.b.vx, RTM_STAGE_W, tz}, {B1.vx, RTM_STAGE_W, tz},
+                {sl.a.vz, RTM_BX, tz + 20}, {A1.vz, RTM_BX, tz + 20}, {sl.b.vz, RTM_BX, tz + 20}, {B1.vz, RTM_BX, tz + 20}};
             for (int t = 0; t < RTM_TMAP_COUNT; t++) {
                 CUtensorMap cm;
                 int rc = encode_field_map(&cm, m[t].f, sh.pitch, sh.Z, m[t].w, m[t].h);

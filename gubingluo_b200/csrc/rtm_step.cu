@@ -9,13 +9,20 @@
 // recomputes the new velocities of its tile's halo instead of waiting for its neighbours:
 //
 //   tile      128 columns x TZ rows of pressure cells (x0 a multiple of 4);
-//   staged    the old p of rows z0-19 .. z0+TZ+18, columns x0-24 .. x0+151 (one TMA box);
-//   phase A   new vx of columns x0-12 .. x0+139, rows z0 .. z0+TZ-1 (x-derivatives of the
-//             staged p) into shared memory; the tile's own cells also to HBM;
-//   phase B   new vz of columns x0 .. x0+127, rows z0-10 .. z0+TZ+9 (z-derivatives of the
-//             staged p) into shared memory; the tile's own rows also to HBM;
-//   phase C   new p of the tile from the shared new velocities (with the split PML fields,
-//             source, receivers, strips and imaging of the split pressure kernels).
+//   staged    by the tensor memory accelerator at the block's start, one barrier: the old p
+//             of rows z0-19 .. z0+TZ+18, columns x0-24 .. x0+151; the old vx of rows
+//             z0 .. z0+TZ-1, columns x0-12 .. x0+139; the old vz of rows z0-10 .. z0+TZ+9,
+//             columns x0 .. x0+127 (off the grid: zeros);
+//   phase A   new vx on the staged vx cells (x-derivatives of the staged p), in place in
+//             shared memory; the tile's own cells also to HBM;
+//   phase B   new vz on the staged vz cells (z-derivatives of the staged p), in place; the
+//             tile's own rows also to HBM;
+//   phase C   new p of the tile from the shared new velocities and the staged old p (with the
+//             split PML fields, source, receivers, strips and imaging of the split pressure
+//             kernels).
+// So the per-shot fields cross HBM in bulk copies issued at once, and the only loads of a
+// phase are the models 1/rho and kappa (shared by the shots of a survey window, mostly
+// L2-resident) and, in the receiver pass, the imaging operands.
 //
 // Neighbouring tiles read the old fields while this one writes the new ones, so the fields
 // p, vx, vz have two buffers each (ShotDev a/an, b/bn: before and after the step; the host
@@ -54,8 +61,8 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
     static_assert(TZ % UQ == 0 && VZH % UQ == 0, "two-row tasks");
     extern __shared__ __align__(128) float sm[];
     float *sp = sm;                   // [PH][PW]   old p
-    float *svx = sp + PH * PW;        // [TZ][VXW]  new vx
-    float *svz = svx + TZ * VXW;      // [VZH][BX]  new vz
+    float *svx = sp + PH * PW;        // [TZ][VXW]  old vx, then (updated in place) new vx
+    float *svz = svx + TZ * VXW;      // [VZH][BX]  old vz, then new vz
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
@@ -68,11 +75,16 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
     const float *__restrict__ inv_rho = (MODE >= 2) ? S.inv_rho_b : S.inv_rho_f;
     const float *__restrict__ kappa = (MODE >= 2) ? S.kappa_b : S.kappa_f;
     const PmlOffsets o = pml_offsets(X, Z);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {   // old p (with both halos), old vx (x-halo), old vz (z-halo)
         mbar_init(&s_bar);
-        mbar_expect(&s_bar, PH * PW * sizeof(float));
-        const int which = (MODE == 2) ? RTM_TMAP_STEP_B0 + S.par_b : RTM_TMAP_STEP_A0 + S.par_a;
-        tma_box(sp, tmap_of(S, which), x0 - 24, z0 - 19, &s_bar);
+        mbar_expect(&s_bar, (PH * PW + TZ * VXW + VZH * BX) * sizeof(float));
+        const int par = (MODE == 2) ? S.par_b : S.par_a;
+        const int mp = (MODE == 2) ? RTM_TMAP_STEP_B0 : RTM_TMAP_STEP_A0;
+        const int mx = (MODE == 2) ? RTM_TMAP_STEPVX_B0 : RTM_TMAP_STEPVX_A0;
+        const int mz = (MODE == 2) ? RTM_TMAP_STEPVZ_B0 : RTM_TMAP_STEPVZ_A0;
+        tma_box(sp, tmap_of(S, mp + par), x0 - 24, z0 - 19, &s_bar);
+        tma_box(svx, tmap_of(S, mx + par), x0 - 12, z0, &s_bar);
+        tma_box(svz, tmap_of(S, mz + par), x0, z0 - 10, &s_bar);
     }
     for (int i = threadIdx.x; i < 100; i += kStepThreads) s_tab[i] = a.coef[i];
     __syncthreads();
@@ -100,12 +112,8 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
 #pragma unroll
         for (int u = 0; u < UQ; u++) {
             const unsigned id = (unsigned)(zq + u) * pitch + x;
-            if (colin && zq + u < Z) {
-                ir[u] = ldg4(&inv_rho[id]);
-                ov[u] = ld4(&W.vx[id]);
-            } else {
-                ir[u] = ov[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            ov[u] = lds4(&svx[(UQ * rg + u) * VXW + 4 * q]);   // staged old vx (zero off the grid)
+            ir[u] = (colin && zq + u < Z) ? ldg4(&inv_rho[id]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         const bool own = x >= x0 && x < x0 + BX;
 #pragma unroll
@@ -152,12 +160,8 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
         for (int u = 0; u < UQ; u++) {
             const int z = zq + u;
             const unsigned id = (unsigned)z * pitch + x;
-            if (x < X && z >= 0 && z < Z) {
-                ir[u] = ldg4(&inv_rho[id]);
-                ow[u] = ld4(&W.vz[id]);
-            } else {
-                ir[u] = ow[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            ow[u] = lds4(&svz[(UQ * rg + u) * BX + 4 * q]);   // staged old vz (zero off the grid)
+            ir[u] = (x < X && z >= 0 && z < Z) ? ldg4(&inv_rho[id]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         const float *col = &sp[(UQ * rg) * PW + 24 + 4 * q];   // staged row of grid row zq-9, word of column x
         float dz[UQ][4];
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
             if (z >= Z) return;
             const bool zin = (z >= npml && z < Z - npml);
             kk[u] = ldg4(&kappa[id]);
-            p0[u] = ld4(&W.p[id]);
+            p0[u] = lds4(&sp[(19 + UQ * rg + u) * PW + 24 + 4 * q]);   // staged old p of the cell
             if (MODE != 3 && !fast && (anyxb || !zin)) {
                 s1[u] = ld4(&sxp[id]);
                 s2[u] = ld4(&szp[id]);

@@ -630,8 +630,12 @@ def test_whole_step_kernel_wavefields_and_forward(rtmlib, monkeypatch):
             res[fused] = ss.wavefields(0, g.nxpad, g.nzpad)
         for nsteps in (37, 60):
             res[(fused, nsteps)] = G.forward(s, G.RunOptions(), 1, v, rho, nsteps)
-    for a, b in zip(res["1"], res["0"]):
-        assert np.array_equal(a, b)
+    # the reconstruction writes its region (interior and strips, [npml-10, npml+n+10)); outside
+    # it the second buffer holds older forward values that nothing reads
+    npml = c["npml"]
+    reg = (slice(npml - 10, g.nzpad - npml + 10), slice(npml - 10, g.nxpad - npml + 10))
+    assert np.array_equal(res["1"][0][reg], res["0"][0][reg])
+    assert np.array_equal(res["1"][1], res["0"][1])
     for nsteps in (37, 60):
         for a, b in zip(res[("1", nsteps)], res[("0", nsteps)]):
             assert np.array_equal(a, b), nsteps
