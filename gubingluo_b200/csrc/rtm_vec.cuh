@@ -58,6 +58,17 @@ __device__ __forceinline__ void st_acc4(ACC *p, const ACC (&v)[4])
 // 16-byte word holding the column 12 to the left of the first output column, so a[k] is the
 // value k-12 columns from it.  dx(j) = sum_i c(j, i-1) * (a[F + j + i] - a[G + j - i]) in tap
 // order (velocity from p: F = 12, G = 13; pressure from vx: F = 11, G = 12).
+// Paired lanes (sm_100 packed fp32: one instruction for two lanes, each lane rounded as a
+// scalar operation): s += c * (f - g) per lane, the difference rounded, then a fused
+// multiply-add, as the scalar sums are compiled.
+#ifndef RTM_PACKED_FP32
+#define RTM_PACKED_FP32 1
+#endif
+__device__ __forceinline__ float2 tap2(float2 s, float2 c, float2 f, float2 g)
+{
+    return __ffma2_rn(c, __fadd2_rn(f, make_float2(-g.x, -g.y)), s);
+}
+
 template <int F, int G, typename C>
 __device__ __forceinline__ void dx4(const float *rw, float (&d)[4], C coef)
 {
@@ -67,10 +78,23 @@ __device__ __forceinline__ void dx4(const float *rw, float (&d)[4], C coef)
         const float4 v = lds4(rw + 4 * q);
         a[4 * q] = v.x; a[4 * q + 1] = v.y; a[4 * q + 2] = v.z; a[4 * q + 3] = v.w;
     }
+#if RTM_PACKED_FP32
+#pragma unroll
+    for (int h = 0; h < 2; h++) {   // columns 2h, 2h+1
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 1; i <= R; i++)
+            s = tap2(s, make_float2(coef(2 * h, i - 1), coef(2 * h + 1, i - 1)),
+                     make_float2(a[F + 2 * h + i], a[F + 2 * h + 1 + i]), make_float2(a[G + 2 * h - i], a[G + 2 * h + 1 - i]));
+        d[2 * h] = s.x;
+        d[2 * h + 1] = s.y;
+    }
+#else
 #pragma unroll
     for (int j = 0; j < 4; j++)
         d[j] = tap_sum([&](int i) { return coef(j, i); }, [&](int i) { return a[F + j + i]; },
                        [&](int i) { return a[G + j - i]; });
+#endif
 }
 
 // z-derivative sums of 4 columns x U rows.  `col` points at the 16-byte word of the four
@@ -81,6 +105,27 @@ __device__ __forceinline__ void dx4(const float *rw, float (&d)[4], C coef)
 template <int U, int STRIDE, typename C>
 __device__ __forceinline__ void dz4(const float *col, float (&s)[U][4], C coef)
 {
+#if RTM_PACKED_FP32
+    float2 s2[U][2];
+#pragma unroll
+    for (int u = 0; u < U; u++) s2[u][0] = s2[u][1] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 1; i <= R; i++) {
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const float4 f = lds4(col + (u + i + 9) * STRIDE);
+            const float4 g = lds4(col + (u - i + 10) * STRIDE);
+            s2[u][0] = tap2(s2[u][0], make_float2(coef(u, 0, i - 1), coef(u, 1, i - 1)), make_float2(f.x, f.y),
+                            make_float2(g.x, g.y));
+            s2[u][1] = tap2(s2[u][1], make_float2(coef(u, 2, i - 1), coef(u, 3, i - 1)), make_float2(f.z, f.w),
+                            make_float2(g.z, g.w));
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        s[u][0] = s2[u][0].x; s[u][1] = s2[u][0].y; s[u][2] = s2[u][1].x; s[u][3] = s2[u][1].y;
+    }
+#else
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll
@@ -95,6 +140,7 @@ __device__ __forceinline__ void dz4(const float *col, float (&s)[U][4], C coef)
             for (int j = 0; j < 4; j++) s[u][j] += coef(u, j, i - 1) * (comp(f, j) - comp(g, j));
         }
     }
+#endif
 }
 
 // Resident blocks per SM that leave each of `threads` threads `regs` registers (the launch
