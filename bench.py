@@ -452,13 +452,15 @@ def run_headline(args, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        kern = {k: round(v[0], 4) for k, v in ((k, ss.kernel_ms(k)) for k in KERNEL_FAMILIES) if v[0] > 0}
+        tiles = ss.tile_heights()
         ss.close()
         w = sum(w_of(sh) for sh in arm_shots)
         return {"shots": len(arm_shots), "seconds": round(ms * 1e-3, 3),
                 "shots_per_s": round(len(arm_shots) / (ms * 1e-3), 4),
                 "gcell_updates_per_s": round(w / (ms * 1e-3) * 1e-9, 3),
                 "mean_cell_updates_per_shot": w / len(arm_shots), "batches": st.batches,
-                "kernel_launches": st.kernel_launches}
+                "kernel_launches": st.kernel_launches, "kernel_ms": kern, "tile_rows": tiles}
 
     batched = timed(G.RunOptions(device=local_rank, strip_precision="fp16", gather_precision="fp16",
                                  accum_fp64=True), shots, 4)
