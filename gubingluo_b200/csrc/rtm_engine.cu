@@ -957,6 +957,10 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     a.gather_prec = RTM_PREC_FP32;
     a.accum_fp64 = o.accum_fp64;
     a.err = ss->d_err;
+    {
+        const char *e = std::getenv("RTM_B200_PREFETCH");   // 0: no L2 prefetch of tile operand rows
+        a.prefetch = !(e && *e && std::atoi(e) == 0);
+    }
     ss->last_batch_n = n;
     ss->last_batch_shots.clear();
     for (int j = 0; j < n; j++) ss->last_batch_shots.push_back(k0 + j);

@@ -64,6 +64,12 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_B
         tma_box(sw, tmap_of(S, MODE == 2 ? RTM_TMAP_B_P : (MODE == 3 ? RTM_TMAP_A_P_RECON : RTM_TMAP_A_P)), x0 - 12,
                 z0 - 9, &s_bar);
     }
+    if (a.prefetch) {   // the tile's 1/rho, vx, vz rows into L2
+        const int z1 = min(z0 + BZ, Z);
+        prefetch_rows(inv_rho, 4, z0, z1, x0, pitch, 1);
+        prefetch_rows(W.vx, 4, z0, z1, x0, pitch, 2);
+        prefetch_rows(W.vz, 4, z0, z1, x0, pitch, 3);
+    }
     for (int i = threadIdx.x; i < 100; i += BX) s_tab[i] = a.coef[i];
     for (int i = threadIdx.x; i < BZ; i += BX) {
         const int z = min(z0 + i, Z - 2);
@@ -257,6 +263,21 @@ __global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_
         mbar_expect(&s_bar, (XH * WW + ZH * BX) * sizeof(float));
         tma_box(svx, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VX : RTM_TMAP_A_VX), x0 - 12, z0, &s_bar);
         tma_box(svz, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VZ : RTM_TMAP_A_VZ), x0, z0 - 10, &s_bar);
+    }
+    if (a.prefetch) {   // the tile's kappa and p rows (split fields, imaging operands) into L2
+        const int z1 = min(z0 + BZ, Z);
+        prefetch_rows(kappa, 4, z0, z1, x0, pitch, 1);
+        prefetch_rows(W.p, 4, z0, z1, x0, pitch, 2);
+        if (MODE != 3 && !t.interior) {
+            prefetch_rows(W.sx, 4, z0, z1, x0, pitch, 3);
+            prefetch_rows(W.sz, 4, z0, z1, x0, pitch, 4);
+        }
+        if (MODE == 2) {   // imaging operands of the interior rows
+            const int i0 = max(z0, npml), i1 = min(z1, Z - npml);
+            prefetch_rows(S.a.p, 4, i0, i1, x0, pitch, 5);
+            prefetch_rows(S.g1, (int)sizeof(ACC), i0, i1, x0, pitch, 6);
+            prefetch_rows(S.illum, (int)sizeof(ACC), i0, i1, x0, pitch, 7);
+        }
     }
     for (int i = threadIdx.x; i < 100; i += BX) s_tab[i] = a.coef[i];
     for (int i = threadIdx.x; i < BZ; i += BX) {

@@ -92,6 +92,25 @@ __device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err)
 // Fixed-grid launches: true for the blocks past the batch's tile list (see StepArgs::counts).
 __device__ __forceinline__ bool tile_beyond(const StepArgs &a) { return a.counts && (int)blockIdx.x >= a.counts[a.list]; }
 
+// L2 prefetch of the operand rows of a tile: rows [z0, z1) of columns [x0, x0 + BX) of nf
+// fields (element sizes es), one bulk prefetch per row and field, spread over the block's
+// threads.  The kernels then find their per-cell operands in L2 instead of waiting on DRAM
+// row group by row group.  Rows stop at the row pitch (x0 and the pitch are multiples of 4
+// elements, so every address and size is a multiple of 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+// Rows [z0, z1) of one field, issued by the lanes of warp `w` of the block (wrapped to the
+// block's warps).
+__device__ __forceinline__ void prefetch_rows(const void *field, int es, int z0, int z1, int x0, int pitch, int w)
+{
+    if ((int)(threadIdx.x >> 5) != w % (int)(blockDim.x >> 5)) return;
+    const unsigned bytes = (unsigned)(min(RTM_BX, pitch - x0) * es);
+    for (int z = z0 + (int)(threadIdx.x & 31); z < z1; z += 32)
+        prefetch_l2((const char *)field + ((size_t)z * pitch + x0) * es, bytes);
+}
+
 __device__ __forceinline__ const void *tmap_of(const ShotDev &S, int which)
 {
     return (const char *)S.tmaps + which * RTM_TMAP_BYTES;

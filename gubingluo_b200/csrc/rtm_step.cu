@@ -86,6 +86,10 @@ __global__ void __launch_bounds__(kStepThreads, (FAST && TZ == 16) ? 3 : 2) k_st
         tma_box(svx, tmap_of(S, mx + par), x0 - 12, z0, &s_bar);
         tma_box(svz, tmap_of(S, mz + par), x0, z0 - 10, &s_bar);
     }
+    if (a.prefetch) {   // the models' rows of the tile and its halo into L2
+        prefetch_rows(inv_rho, 4, max(z0 - 10, 0), min(z0 + TZ + 10, Z), x0, pitch, 1);
+        prefetch_rows(kappa, 4, z0, min(z0 + TZ, Z), x0, pitch, 2);
+    }
     for (int i = threadIdx.x; i < 100; i += kStepThreads) s_tab[i] = a.coef[i];
     __syncthreads();
     // every thread waits (bounded); the block goes on only if all saw the tile arrive

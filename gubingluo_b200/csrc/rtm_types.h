@@ -161,4 +161,5 @@ struct StepArgs {
     // counts == nullptr: the grid is the tile count
     const int *counts;
     int list;
+    int prefetch;           // 1: the stencil kernels prefetch their tile's operand rows into L2
 };
