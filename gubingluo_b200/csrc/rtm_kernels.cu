@@ -6,6 +6,7 @@
 
 #include <algorithm>
 
+#include "rtm_strip.cuh"
 #include "rtm_types.h"
 
 #define R RTM_RADIUS
@@ -129,33 +130,7 @@ __global__ void k_strip_save(const ShotDev *shots, int it, int ring, int prec)
 {
     const ShotDev &S = shots[blockIdx.y];
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= S.strip_len) return;
-    const int X = S.X, Z = S.Z, npml = S.npml, nxi = S.nxi, nzi = S.nzi, pitch = S.pitch;
-    const int lr = R * nzi, tb = R * nxi;
-    int k = idx, z, x;
-    const float *f;
-    if (k < 2 * lr || (k >= 2 * lr + 2 * tb && k < 4 * lr + 2 * tb)) {   // left/right strips
-        const bool pstrip = k >= 2 * lr;
-        if (pstrip) k -= 2 * lr + 2 * tb;
-        const int side = k / lr, rem = k - side * lr;
-        z = npml + rem / R;
-        const int c = rem % R;
-        // vx right strip starts at X-npml-1 (vx has X-1 columns), p right strip at X-npml
-        x = side == 0 ? npml - R + c : (pstrip ? X - npml : X - npml - 1) + c;
-        f = pstrip ? S.a.p : S.a.vx;
-    } else {                                                             // top/bottom strips
-        const bool pstrip = k >= 4 * lr + 2 * tb;
-        k -= pstrip ? 4 * lr + 2 * tb : 2 * lr;
-        const int side = k / tb, rem = k - side * tb;
-        const int r = rem / nxi;
-        x = npml + (rem - r * nxi);
-        // vz bottom strip starts at Z-npml-1 (vz has Z-1 rows), p bottom strip at Z-npml
-        z = side == 0 ? npml - R + r : (pstrip ? Z - npml : Z - npml - 1) + r;
-        f = pstrip ? S.a.p : S.a.vz;
-    }
-    const float v = f[(size_t)z * pitch + x];
-    if (prec == RTM_FP32) ((float *)S.strips)[(size_t)it * S.strip_len + idx] = v;
-    else S.strip_stage[(size_t)ring * S.strip_len + idx] = v;
+    if (idx < S.strip_len) strip_save_cell(S, idx, it, ring, prec);
 }
 
 // =====================================================================================

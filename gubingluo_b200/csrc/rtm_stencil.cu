@@ -40,18 +40,17 @@
 // Register budget (measured): 6 blocks per SM (80 registers, no spills) in every mode but the
 // 8-row reconstruction tiles (5, which would spill at 6); with its interior-tile body the
 // reconstruction runs 4% faster at 6 than at 5.
+// The work of one block on tile t (the kernel below, and the persistent pass kernels of
+// rtm_persist.cu); `sw` is the block's dynamic shared memory.
 template <int BZ, int MODE>
-__global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_BLOCKS) : 6) k_vel(const StepArgs a)
+__device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, float *sw)
 {
     constexpr int U = MODE == 3 ? UVR : UV, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int WH = BZ + QNV_MAX - 1;   // staged rows z0-9 .. z0+BZ+QNV_MAX-11 (the box height)
-    extern __shared__ __align__(128) float sw[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1vz[BZ], s_ic2vz[BZ];
-    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
-    const TileRef t = a.tiles[blockIdx.x];   // reconstruction: tiles of the interior + strips only
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
     const int x0 = t.x0, z0 = t.z0;
@@ -235,23 +234,17 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_B
 // PML, source or receiver tests and no split-field loads, in the arithmetic of the general
 // body's interior branch (for the reconstruction: tiles of the interior with no source cell).
 template <int BZ, int MODE, typename ACC>
-__global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_PRES_RECV_BLOCKS)
-                                     : MODE == 3 ? RTM_PRES_RECON_BLOCKS
-                                                 : RTM_PRES_FWD_BLOCKS)
-    k_pres(const StepArgs a, int record)
+__device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const TileRef t, float *sm)
 {
     constexpr int U = MODE == 2 ? UPR : MODE == 3 ? UPC : UP, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
     constexpr int XH = BZ;            // vx rows z0 .. z0+BZ-1, columns x0-12 .. x0+BX+11
     constexpr int ZH = BZ + QNP_MAX - 1;   // vz rows z0-10 .. z0+BZ+QNP_MAX-12 (the box height), columns x0 ..
-    extern __shared__ __align__(128) float sm[];
     float *svx = sm;
     float *svz = sm + XH * WW;   // XH * WW * 4 bytes is a multiple of 128
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float s_tab[100];
     __shared__ float s_c1z[BZ], s_ic2z[BZ];
-    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
-    const TileRef t = a.tiles[blockIdx.x];   // reconstruction: tiles of the interior + strips only
     const ShotDev &S = a.shots[t.shot];
     const int X = S.X, Z = S.Z, pitch = S.pitch, npml = S.npml;
     const int x0 = t.x0, z0 = t.z0;
@@ -474,6 +467,26 @@ __global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_
         one_row(z);
         advance<1, BX>(q, colz, z + 1 - z0, z + 1 < zend);
     }
+}
+
+// The kernels: one block per tile of the launch's list (reconstruction: tiles of the
+// interior and its strips only).
+template <int BZ, int MODE>
+__global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_BLOCKS) : 6) k_vel(const StepArgs a)
+{
+    extern __shared__ __align__(128) float sw[];
+    if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
+    vel_tile<BZ, MODE>(a, a.tiles[blockIdx.x], sw);
+}
+template <int BZ, int MODE, typename ACC>
+__global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_PRES_RECV_BLOCKS)
+                                     : MODE == 3 ? RTM_PRES_RECON_BLOCKS
+                                                 : RTM_PRES_FWD_BLOCKS)
+    k_pres(const StepArgs a, int record)
+{
+    extern __shared__ __align__(128) float sm[];
+    if (tile_beyond(a)) return;
+    pres_tile<BZ, MODE, ACC>(a, record, a.tiles[blockIdx.x], sm);
 }
 
 // =====================================================================================

@@ -1,0 +1,39 @@
+// rtm_strip.cuh — saving one boundary-strip cell after a source-pass step (reference
+// save_d_vxpml / save_d_vzpml / save_d_ppmllr / save_d_ppmltb, kernel.cu:1186-1293), shared
+// by the strip-save kernel (rtm_kernels.cu) and the persistent source pass (rtm_stencil.cu).
+// Strip layout per step: [vx lr 2][nzi][10] [vz tb 2][10][nxi] [p lr 2][nzi][10] [p tb 2][10][nxi].
+#pragma once
+#include "rtm_types.h"
+
+// Cell idx (< S.strip_len) of step it: fp32 strips straight to strips[it]; fp16/bf16 strips
+// to the fp32 staging ring slot `ring` (packed later).
+__device__ __forceinline__ void strip_save_cell(const ShotDev &S, int idx, int it, int ring, int prec)
+{
+    constexpr int R = RTM_RADIUS;
+    const int X = S.X, Z = S.Z, npml = S.npml, nxi = S.nxi, nzi = S.nzi, pitch = S.pitch;
+    const int lr = R * nzi, tb = R * nxi;
+    int k = idx, z, x;
+    const float *f;
+    if (k < 2 * lr || (k >= 2 * lr + 2 * tb && k < 4 * lr + 2 * tb)) {   // left/right strips
+        const bool pstrip = k >= 2 * lr;
+        if (pstrip) k -= 2 * lr + 2 * tb;
+        const int side = k / lr, rem = k - side * lr;
+        z = npml + rem / R;
+        const int c = rem % R;
+        // vx right strip starts at X-npml-1 (vx has X-1 columns), p right strip at X-npml
+        x = side == 0 ? npml - R + c : (pstrip ? X - npml : X - npml - 1) + c;
+        f = pstrip ? S.a.p : S.a.vx;
+    } else {                                                             // top/bottom strips
+        const bool pstrip = k >= 4 * lr + 2 * tb;
+        k -= pstrip ? 4 * lr + 2 * tb : 2 * lr;
+        const int side = k / tb, rem = k - side * tb;
+        const int r = rem / nxi;
+        x = npml + (rem - r * nxi);
+        // vz bottom strip starts at Z-npml-1 (vz has Z-1 rows), p bottom strip at Z-npml
+        z = side == 0 ? npml - R + r : (pstrip ? Z - npml : Z - npml - 1) + r;
+        f = pstrip ? S.a.p : S.a.vz;
+    }
+    const float v = f[(size_t)z * pitch + x];
+    if (prec == RTM_FP32) ((float *)S.strips)[(size_t)it * S.strip_len + idx] = v;
+    else S.strip_stage[(size_t)ring * S.strip_len + idx] = v;
+}

@@ -163,3 +163,23 @@ struct StepArgs {
     int list;
     int prefetch;           // 1: the stencil kernels prefetch their tile's operand rows into L2
 };
+
+// One persistent pass (rtm_stencil.cu, k_pass): every step of the source pass or of the
+// backward pass in one launch.  Blocks take work items from a device queue in the order
+//   source pass, per step it:    velocity tiles, pressure tiles, strip save (one per shot)
+//   backward pass, per step k:   reconstruction velocity tiles, reconstruction pressure
+//                                tiles, receiver velocity tiles, receiver pressure tiles
+// and wait, per shot, until the items an item depends on (all of the shot's items of the
+// phases before it) are done: done[phase][shot] counts them.
+struct PassArgs {
+    StepArgs a;              // shots, wavelet, coefficients, precisions (tiles, it, ring per item)
+    const TileRef *list[4];  // tile lists: source pass {vel, pres}; backward {vel recon, pres recon, vel, pres}
+    int len[4];              // their lengths
+    const int *per_shot;     // tiles per shot of each list: [4][B]
+    int B;                   // stride of per_shot and done
+    int nshots, nsteps, nt;  // shots of the batch; steps of the pass; time samples
+    int save, record, strip_prec;
+    unsigned *queue;         // next item (starts at 0)
+    unsigned *done;          // [4][B] completed items per phase and shot (start at 0)
+    long long wait_ns;       // bound on one wait for other blocks' items (then the error flag, 2)
+};
