@@ -147,6 +147,12 @@ struct rtm_session {
     // current for each wavefield)
     bool fused = false;
     int tz_step = 32;
+    // persistent passes (k_pass, RTM_B200_PERSIST=1): every step of a pass in one launch over a
+    // device work queue with per-shot completion counters; one-column kernels at 32/16/16 rows
+    bool persist = false;
+    long long pass_wait_ns = 2000000000LL;   // bound on one wait (RTM_B200_PASS_WAIT_US)
+    int *d_per_shot = nullptr;               // [6][B]: tiles per shot, source pass lists then backward lists
+    unsigned *d_queue = nullptr, *d_done = nullptr;   // pass queue counter; [4][B] completion counters
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -217,6 +223,8 @@ static int check_kernel_flag(rtm_session *ss)
     CK(cudaMemcpy(&flag, ss->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
         CK(cudaMemset(ss->d_err, 0, sizeof(int)));
+        if (flag == 2)
+            return fail(RTM_ERR_CUDA, "a persistent pass gave up waiting for the work items of other blocks");
         return fail(RTM_ERR_CUDA, "a stencil kernel gave up waiting for its tile (TMA copy did not complete)");
     }
     return RTM_OK;
@@ -435,6 +443,8 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             ss->tune = false;
         }
         if (ss->tz_step != 16 && ss->tz_step != 32) return fail(RTM_ERR_ARG, "RTM_B200_TZ_STEP must be 16 or 32");
+        if ((e = std::getenv("RTM_B200_PERSIST")) && *e) ss->persist = std::atoi(e) != 0 && !ss->fused;
+        if ((e = std::getenv("RTM_B200_PASS_WAIT_US")) && *e) ss->pass_wait_ns = std::atoll(e) * 1000LL;
     }
     size_t per_slot = slot_bytes(s, o, big.pitch, big.Z, big.strip_len, big.nxi, big.nzi, ss->fused);
     size_t fixed = model_bytes + shot_bytes_total + (o.extra_images ? 11 : 4) * ((size_t)s.nx * s.nz * 8 + 256) + (size_t)s.nt * 4 + 4096 +
@@ -460,6 +470,13 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
                 return fail(RTM_ERR_ARG, "RTM_B200_KERNELS must be scalar or vector");
             for (bool &v : ss->vec) v = !std::strcmp(e, "vector");
             ss->forms_fixed = true;
+        }
+        if (ss->persist) {   // the persistent passes run the one-column kernels at the default heights
+            ss->tune = false;
+            ss->bz_vel = 32;
+            ss->bz_vel_recon = 16;
+            ss->bz_pres = 16;
+            for (bool &v : ss->vec) v = false;
         }
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
         if (o.accum_fp64 < 0 || o.accum_fp64 > 2) return fail(RTM_ERR_ARG, "accum_fp64 must be 0, 1 or 2");
@@ -634,7 +651,11 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->d_tiles_pr = (TileRef *)ss->arena.take(sizeof(TileRef) * ss->max_tiles);
     ss->d_fin = ss->arena.take(finalize_shot_size() * B);
     ss->d_counts = (int *)ss->arena.take(4 * sizeof(int));
-    if (!ss->d_counts) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
+    ss->d_per_shot = (int *)ss->arena.take(6 * sizeof(int) * B);
+    ss->d_queue = (unsigned *)ss->arena.take(2 * sizeof(unsigned));
+    ss->d_done = (unsigned *)ss->arena.take(4 * sizeof(unsigned) * B);
+    if (!ss->d_counts || !ss->d_per_shot || !ss->d_queue || !ss->d_done)
+        return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_tiles_r || !ss->d_tiles_pr || !ss->d_fin)
         return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     CK(cudaStreamSynchronize(ss->stream));
@@ -912,6 +933,15 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         return fail(RTM_ERR_ARG, "tile table overflow");
     const int counts[4] = {br.ntiles, br.ntiles_p, br.ntiles_r, br.ntiles_pr};
     CK(cudaMemcpyAsync(ss->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, st));
+    {   // tiles per shot: source pass lists (velocity, pressure), backward lists (reconstruction
+        // velocity and pressure, receiver velocity and pressure)
+        std::vector<int> per(6 * (size_t)ss->B, 0);
+        const std::vector<TileRef> *L[6] = {&tiles, &tiles_p, &tiles_r, &tiles_pr, &tiles, &tiles_p};
+        for (int l = 0; l < 6; l++)
+            for (const TileRef &t : *L[l]) per[(size_t)l * ss->B + t.shot]++;
+        CK(cudaMemcpyAsync(ss->d_per_shot, per.data(), sizeof(int) * per.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));   // the host vector goes out of scope
+    }
     for (int L = 0; L < 4; L++) br.grid[L] = counts[L];
     br.strip_grid = br.max_strip_len;
     for (int j = 0; j < n; j++) {
@@ -1062,6 +1092,55 @@ static int run_pass(rtm_session *ss, std::vector<long> key, F &&body)
     return RTM_OK;
 }
 
+// One persistent launch for a whole pass (dir 0: source pass; 1: backward pass) when the
+// session asks for it and the pass has no part outside it (fp16/bf16 strip packing, the other
+// imaging conditions, snapshots); *ran tells whether it ran.
+static int persistent_pass(rtm_session *ss, BatchRun &br, int dir, int nsteps, bool save, bool record, bool *ran)
+{
+    *ran = false;
+    const rtm_options &o = ss->o;
+    if (!ss->persist || ss->nsnap) return RTM_OK;
+    if (dir == 0 && save && o.strip_precision != RTM_PREC_FP32) return RTM_OK;
+    if (dir == 1 && o.extra_images) return RTM_OK;
+    cudaStream_t st = ss->stream;
+    PassArgs P{};
+    P.a = br.a;
+    P.a.counts = nullptr;
+    P.a.shots = ss->d_shots;
+    if (dir == 0) {
+        P.list[0] = ss->d_tiles, P.len[0] = br.ntiles;
+        P.list[1] = ss->d_tiles_p, P.len[1] = br.ntiles_p;
+        P.per_shot = ss->d_per_shot;
+    } else {
+        P.list[0] = ss->d_tiles_r, P.len[0] = br.ntiles_r;
+        P.list[1] = ss->d_tiles_pr, P.len[1] = br.ntiles_pr;
+        P.list[2] = ss->d_tiles, P.len[2] = br.ntiles;
+        P.list[3] = ss->d_tiles_p, P.len[3] = br.ntiles_p;
+        P.per_shot = ss->d_per_shot + 2 * (size_t)ss->B;
+    }
+    P.B = ss->B;
+    P.nshots = br.n;
+    P.nsteps = dir == 0 ? nsteps : ss->s.nt - 1;
+    P.nt = ss->s.nt;
+    P.save = save;
+    P.record = record;
+    P.strip_prec = o.strip_precision;
+    P.queue = ss->d_queue;
+    P.done = ss->d_done;
+    P.wait_ns = ss->pass_wait_ns;
+    CK(cudaMemsetAsync(ss->d_queue, 0, 2 * sizeof(unsigned), st));
+    CK(cudaMemsetAsync(ss->d_done, 0, 4 * sizeof(unsigned) * ss->B, st));
+    cudaEvent_t e;
+    timing_begin(ss, dir == 0 ? "pass_fwd" : "pass_bwd", 7, &e);
+    const bool ok = launch_pass(dir, P, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, st);
+    timing_end(ss, e);
+    if (!ok) return RTM_OK;
+    ss->launches++;
+    *ran = true;
+    CK(cudaGetLastError());
+    return RTM_OK;
+}
+
 // Source pass (rtm_model.cu:322-346): nsteps forward steps with the source added; strips
 // saved after every step when `save` (one small copy kernel, so the stencil kernels carry no
 // strip logic); the gather recorded when `record` (mode 0 fuses the reference's separate
@@ -1115,7 +1194,14 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
             }
         }
     };
-    if (ntsnap) {   // snapshots read back per pass: no graph
+    bool ran = false;
+    if (int rc = persistent_pass(ss, br, 0, nsteps, save, record, &ran)) {
+        nvtxRangePop();
+        return rc;
+    }
+    if (ran) {
+        // every step ran in the one persistent launch
+    } else if (ntsnap) {   // snapshots read back per pass: no graph
         loop();
         CK(cudaGetLastError());
     } else {
@@ -1269,7 +1355,14 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             }
         }
     };
-    if (ntsnap) {
+    bool ran = false;
+    if (int rc = persistent_pass(ss, br, 1, s.nt - 1, false, false, &ran)) {
+        nvtxRangePop();
+        return rc;
+    }
+    if (ran) {
+        // every step ran in the one persistent launch
+    } else if (ntsnap) {
         loop();
         CK(cudaGetLastError());
     } else {

@@ -11,6 +11,9 @@ void launch_pres(int mode, int bz, const StepArgs &a, int ntiles, int record, cu
 // The same launches with four columns by U rows per thread (rtm_stencil_v.cu): same tile
 // lists, staged boxes and results, 32 * bz / U threads per block.
 void launch_vel4(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s);
+// A whole pass in one persistent launch (rtm_stencil.cu, k_pass): dir 0 the source pass, 1 the
+// backward pass.  Only at the default tile heights (32, 16, 16); returns false otherwise.
+bool launch_pass(int dir, const PassArgs &p, int bz_vel, int bz_vel_recon, int bz_pres, cudaStream_t s);
 void launch_pres4(int mode, int bz, const StepArgs &a, int ntiles, int record, cudaStream_t s);
 // One whole time step (velocities and pressure) of one wavefield (rtm_step.cu): reads the
 // shots' a / b fields, writes an / bn; tz rows per tile (16 or 32), 256 threads per block;

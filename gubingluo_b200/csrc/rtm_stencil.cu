@@ -22,6 +22,7 @@
 // Reference equivalents (gubingluo kernel.cu): forward v :430-500 + :542-713, forward p
 // :501-541 + :714-1185, reconstruction :318-429, strip restore :1294-1400, source :36-47,
 // receivers :48-95, cross-correlation :1401-1416.
+#include <algorithm>
 #include <atomic>
 
 #include <cuda_bf16.h>
@@ -32,6 +33,7 @@
 #include "rtm_types.h"
 
 #include "rtm_stencil_common.cuh"
+#include "rtm_strip.cuh"
 
 // =====================================================================================
 // Velocity update.  MODE 0: forward, full grid; 2: receiver (backward model), full grid;
@@ -490,6 +492,128 @@ __global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_
 }
 
 // =====================================================================================
+// Persistent passes: every step of a pass in one launch (PassArgs).  Blocks claim items in
+// queue order; an item waits only for items earlier in the queue, which blocks that are
+// running have claimed, so the queue always drains.  Each wait is bounded (wait_ns of the
+// global timer, and the error flag of any other block): on giving up, the block sets the
+// error flag to 2 and every block leaves at its next item.  One block per SM slot, 128
+// threads, the tile functions of the kernels above.
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ long long global_ns()
+{
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Thread 0: wait until *c >= target (or give up: error flag 2).  Then order the items' writes
+// before this block's tensor-memory loads (async proxy).
+__device__ __forceinline__ bool wait_done(const unsigned *c, unsigned target, const PassArgs &P)
+{
+    if (ld_acquire(c) < target) {
+        const long long t0 = global_ns();
+        while (ld_acquire(c) < target) {
+            if (global_ns() - t0 > P.wait_ns || *(volatile int *)P.a.err) {
+                atomicCAS(P.a.err, 0, 2);
+                return false;
+            }
+            __nanosleep(100);
+        }
+    }
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    return true;
+}
+
+// DIR 0: source pass (velocity, pressure, strip save per step; mode 0, strips fp32);
+// DIR 1: backward pass (reconstruction velocity and pressure, receiver velocity and pressure
+// with imaging).
+template <int BZV, int BZVR, int BZP, typename ACC, int DIR>
+__global__ void __launch_bounds__(BX, DIR == 0 ? 5 : 4) k_pass(const PassArgs P)
+{
+    extern __shared__ __align__(128) float sm[];
+    __shared__ unsigned s_item;
+    __shared__ int s_ok;
+    const int n = P.nshots;
+    const int ns = (DIR == 0 && P.save) ? n : 0;
+    const int per = DIR == 0 ? P.len[0] + P.len[1] + ns : P.len[0] + P.len[1] + P.len[2] + P.len[3];
+    const unsigned total = (unsigned)per * (unsigned)P.nsteps;
+    const int *cnt = P.per_shot;
+    for (;;) {
+        __syncthreads();   // the previous item's shared memory is free
+        if (threadIdx.x == 0) s_item = *(volatile int *)P.a.err ? total : atomicAdd(P.queue, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= total) return;
+        const int k = (int)(item / per);
+        int r = (int)(item - (unsigned)k * per);
+        StepArgs a = P.a;
+        int ph, s;
+        TileRef t{};
+        if (DIR == 0) {
+            a.it = k;
+            a.ring = k % 32;
+            if (r < P.len[0]) ph = 0, t = P.list[0][r], s = t.shot;
+            else if (r < P.len[0] + P.len[1]) ph = 1, t = P.list[1][r - P.len[0]], s = t.shot;
+            else ph = 2, s = r - P.len[0] - P.len[1];
+        } else {
+            a.it = P.nt - 2 - k;
+            ph = 0;
+            while (r >= P.len[ph]) r -= P.len[ph++];
+            t = P.list[ph][r];
+            s = t.shot;
+        }
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            const unsigned *d = P.done;
+            const int B = P.B;
+            if (DIR == 0) {
+                if (ph == 0) ok = ns ? wait_done(&d[2 * B + s], (unsigned)k, P)
+                                     : wait_done(&d[1 * B + s], (unsigned)(k * cnt[1 * B + s]), P);
+                else if (ph == 1) ok = wait_done(&d[0 * B + s], (unsigned)((k + 1) * cnt[0 * B + s]), P);
+                else ok = wait_done(&d[1 * B + s], (unsigned)((k + 1) * cnt[1 * B + s]), P);
+            } else {
+                // 0 recon vel: after recon pres of step k-1; 1 recon pres: after recon vel of k and
+                // the receiver pressure of k-1 (its imaging read the pressure being replaced);
+                // 2 receiver vel: after receiver pres of k-1; 3 receiver pres: after receiver vel
+                // of k and recon pres of k (its imaging reads that pressure)
+                if (ph == 0) ok = wait_done(&d[1 * B + s], (unsigned)(k * cnt[1 * B + s]), P);
+                else if (ph == 1) ok = wait_done(&d[0 * B + s], (unsigned)((k + 1) * cnt[0 * B + s]), P) &&
+                                       wait_done(&d[3 * B + s], (unsigned)(k * cnt[3 * B + s]), P);
+                else if (ph == 2) ok = wait_done(&d[3 * B + s], (unsigned)(k * cnt[3 * B + s]), P);
+                else ok = wait_done(&d[2 * B + s], (unsigned)((k + 1) * cnt[2 * B + s]), P) &&
+                          wait_done(&d[1 * B + s], (unsigned)((k + 1) * cnt[1 * B + s]), P);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        if (DIR == 0) {
+            if (ph == 0) vel_tile<BZV, 0>(a, t, sm);
+            else if (ph == 1) pres_tile<BZP, 0, float>(a, P.record, t, sm);
+            else {
+                const ShotDev &S = a.shots[s];
+                for (int i = threadIdx.x; i < S.strip_len; i += BX) strip_save_cell(S, i, k, a.ring, P.strip_prec);
+            }
+        } else {
+            if (ph == 0) vel_tile<BZVR, 3>(a, t, sm);
+            else if (ph == 1) pres_tile<BZP, 3, float>(a, 0, t, sm);
+            else if (ph == 2) vel_tile<BZV, 2>(a, t, sm);
+            else pres_tile<BZP, 2, ACC>(a, 0, t, sm);
+        }
+        __syncthreads();   // every thread's writes of the item are done
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&P.done[ph * P.B + s], 1u);
+        }
+    }
+}
+
+// =====================================================================================
 // Host launchers.
 template <int BZ>
 static size_t vel_smem() { return (size_t)(BZ + QNV_MAX - 1) * WW * sizeof(float); }
@@ -555,6 +679,33 @@ static void pres_dispatch(int bz, const StepArgs &a, int ntiles, int record, cud
     else if (bz == 8) pres_launch<8, MODE>(a, ntiles, record, s);
     else if (bz == 64) pres_launch<64, MODE>(a, ntiles, record, s);
     else pres_launch<32, MODE>(a, ntiles, record, s);
+}
+
+// Persistent passes at the default tile heights (32-row forward/receiver velocity tiles,
+// 16-row reconstruction velocity and pressure tiles).  Returns false when the heights differ.
+template <int DIR, typename ACC>
+static void pass_launch_t(const PassArgs &p, int bzv, int bzp, cudaStream_t s)
+{
+    constexpr int BZV = 32, BZVR = 16, BZP = 16;
+    static std::atomic<unsigned long long> done{0};
+    const size_t bytes = std::max(std::max(vel_smem<BZV>(), vel_smem<BZVR>()), pres_smem<BZP>());
+    set_smem_once(done, k_pass<BZV, BZVR, BZP, ACC, DIR>, bytes);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<BZV, BZVR, BZP, ACC, DIR>, BX, bytes);
+    (void)bzv;
+    (void)bzp;
+    k_pass<BZV, BZVR, BZP, ACC, DIR><<<sms * std::max(per_sm, 1), BX, bytes, s>>>(p);
+}
+bool launch_pass(int dir, const PassArgs &p, int bz_vel, int bz_vel_recon, int bz_pres, cudaStream_t s)
+{
+    if (bz_vel != 32 || bz_vel_recon != 16 || bz_pres != 16) return false;
+    if (dir == 0) pass_launch_t<0, float>(p, bz_vel, bz_pres, s);
+    else if (p.a.accum_fp64 == RTM_ACC_FP64) pass_launch_t<1, double>(p, bz_vel, bz_pres, s);
+    else if (p.a.accum_fp64 == RTM_ACC_KAHAN) pass_launch_t<1, KahanAcc>(p, bz_vel, bz_pres, s);
+    else pass_launch_t<1, float>(p, bz_vel, bz_pres, s);
+    return true;
 }
 
 void launch_vel(int mode, int bz, const StepArgs &a, int ntiles, cudaStream_t s)

@@ -639,3 +639,45 @@ def test_whole_step_kernel_wavefields_and_forward(rtmlib, monkeypatch):
     for nsteps in (37, 60):
         for a, b in zip(res[("1", nsteps)], res[("0", nsteps)]):
             assert np.array_equal(a, b), nsteps
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["fp32", "fp64", "kahan"])
+def test_persistent_passes_are_bitwise_identical(rtmlib, monkeypatch, form):
+    """RTM_B200_PERSIST=1: each pass in one persistent launch (device work queue, per-shot
+    completion counters) gives the bits of the per-step launches: gathers and images of the
+    general cases, several shots of uneven windows in one batch."""
+    G = rtmlib
+    opts = dict(fp32=dict(), fp64=dict(accum_fp64=1), kahan=dict(accum_fp64=2))[form]
+    for ci, c in enumerate(GENERAL):
+        v, rho = _random_model(c["nz"], c["nx"], 60 + ci)
+        shots = list(range(1, c["nshot"] + 1))
+        s = cfg_from(G, _survey(c, 0))
+        monkeypatch.setenv("RTM_B200_PERSIST", "0")
+        monkeypatch.setenv("RTM_B200_KERNELS", "scalar")
+        monkeypatch.setenv("RTM_B200_TUNE", "0")
+        want = G.migrate(s, G.RunOptions(**opts), shots, v, rho)
+        monkeypatch.setenv("RTM_B200_PERSIST", "1")
+        got = G.migrate(s, G.RunOptions(**opts), shots, v, rho)
+        for k in ("image1", "image2s", "illum"):
+            assert np.array_equal(got[k], want[k]), (ci, k)
+        for a, b in zip(got["gathers"], want["gathers"]):
+            assert np.array_equal(a, b), ci
+
+
+@pytest.mark.gpu
+def test_persistent_pass_wait_runs_out_cleanly(rtmlib, monkeypatch):
+    """A persistent pass whose waits for other blocks' work items are bounded by 0 us gives up
+    at its first unmet dependency: the call returns an error naming it (no hang), and the next
+    run on the same device succeeds."""
+    G = rtmlib
+    c = GENERAL[1]
+    v, rho = _random_model(c["nz"], c["nx"], 70)
+    s = cfg_from(G, _survey(c, 0))
+    monkeypatch.setenv("RTM_B200_PERSIST", "1")
+    monkeypatch.setenv("RTM_B200_PASS_WAIT_US", "0")
+    with pytest.raises(G.RtmError, match="persistent pass gave up"):
+        G.migrate(s, G.RunOptions(), [1, 2], v, rho)
+    monkeypatch.delenv("RTM_B200_PASS_WAIT_US")
+    out = G.migrate(s, G.RunOptions(), [1, 2], v, rho)
+    assert np.isfinite(out["image1"]).all() and np.abs(out["image1"]).max() > 0
