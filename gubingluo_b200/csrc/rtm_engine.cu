@@ -925,6 +925,17 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         if (o.extra_images)
             for (void *g : sl.gx) CK(cudaMemsetAsync(g, 0, ib, st));
     }
+    {
+        // RTM_B200_TILE_ORDER=position: order each list by tile position and then by shot, so
+        // the shots that share a model window read its rows back to back (the default order,
+        // shot by shot, keeps a shot's neighbouring tiles together instead)
+        const char *e = std::getenv("RTM_B200_TILE_ORDER");
+        if (e && !std::strcmp(e, "position"))
+            for (std::vector<TileRef> *v : {&tiles, &tiles_p, &tiles_r, &tiles_pr})
+                std::stable_sort(v->begin(), v->end(), [](const TileRef &a, const TileRef &b) {
+                    return a.z0 != b.z0 ? a.z0 < b.z0 : a.x0 < b.x0;
+                });
+    }
     br.ntiles = (int)tiles.size();
     br.ntiles_p = (int)tiles_p.size();
     br.ntiles_r = (int)tiles_r.size();
