@@ -733,10 +733,10 @@ struct BatchRun {
     StepArgs a{};
     // whole-step kernel: which buffer holds the current source (pa) and receiver (pb) fields
     int pa = 0, pb = 0;
-    // grid of the launches over each tile list: its tile count, or with use_graph a bound that
-    // depends only on the batch size (n times the most tiles any shot of the session has), so
-    // that one captured graph serves batches of any windows; likewise the strip kernels' and
-    // the other imaging conditions' extents
+    // grid of the launches over each tile list: its tile count, or with use_graph that count
+    // rounded up to four significant bits, so that one captured graph serves batches whose
+    // windows differ a little; likewise the strip kernels' and the other imaging conditions'
+    // extents
     int grid[4] = {0, 0, 0, 0};
     int strip_grid = 0, ex_nxi = 0, ex_nzi = 0;
 };
@@ -959,18 +959,18 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         br.ex_nxi = std::max(br.ex_nxi, ss->shots[k0 + j].nxi);
         br.ex_nzi = std::max(br.ex_nzi, ss->shots[k0 + j].nzi);
     }
-    if (o.use_graph) {   // bounds over every shot of the session
-        int most[4] = {0, 0, 0, 0};
-        for (const ShotState &sh : ss->shots) {
-            std::vector<TileRef> t4[4];
-            std::vector<TileRef> *L[4] = {&t4[0], &t4[1], &t4[2], &t4[3]};
-            shot_tiles(ss, sh, 0, fast, L);
-            for (int l = 0; l < 4; l++) most[l] = std::max(most[l], (int)t4[l].size());
-            br.strip_grid = std::max(br.strip_grid, sh.strip_len);
-            br.ex_nxi = std::max(br.ex_nxi, sh.nxi);
-            br.ex_nzi = std::max(br.ex_nzi, sh.nzi);
-        }
-        for (int l = 0; l < 4; l++) br.grid[l] = n * most[l];
+    if (o.use_graph) {
+        // graph replays launch fixed grids: the counts rounded up to four significant bits
+        // (at most 12.5% of blocks idle), so batches of nearby sizes share one captured graph
+        auto bucket = [](int v) {
+            int e = 0;
+            while ((v >> e) >= 16) e++;
+            return ((v + (1 << e) - 1) >> e) << e;
+        };
+        for (int l = 0; l < 4; l++) br.grid[l] = bucket(counts[l]);
+        br.strip_grid = bucket(br.strip_grid);
+        br.ex_nxi = bucket(br.ex_nxi);
+        br.ex_nzi = bucket(br.ex_nzi);
     }
     for (int j = 0; j < n; j++) {
         const Slot &sl = ss->slots[j];

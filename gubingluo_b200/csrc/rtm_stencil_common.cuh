@@ -55,6 +55,12 @@ __device__ __forceinline__ void mbar_init(unsigned long long *bar)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
+// Before an mbarrier's memory is initialised again (a block that stages one tile after
+// another), the old object is invalidated; every wait on it has completed by then.
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
