@@ -153,6 +153,8 @@ struct rtm_session {
     long long pass_wait_ns = 2000000000LL;   // bound on one wait (RTM_B200_PASS_WAIT_US)
     int *d_per_shot = nullptr;               // [6][B]: tiles per shot, source pass lists then backward lists
     unsigned *d_queue = nullptr, *d_done = nullptr;   // pass queue counter; [4][B] completion counters
+    unsigned *d_trace = nullptr;             // the item each persistent block took last
+    int trace_len = 0;
     void *d_fin = nullptr;
     void *d_tmaps = nullptr;         // B x RTM_TMAP_COUNT tensor maps (rebuilt for every batch)
     int *d_err = nullptr;            // kernel error flag (bounded waits that gave up)
@@ -219,13 +221,22 @@ static int encode_field_map(void *out, float *field, int pitch, int Z, int box_w
 // Read and clear the kernels' error flag (after the stream has been synchronised).
 static int check_kernel_flag(rtm_session *ss)
 {
-    int flag = 0;
-    CK(cudaMemcpy(&flag, ss->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) {
-        CK(cudaMemset(ss->d_err, 0, sizeof(int)));
-        if (flag == 2)
+    int e[8] = {};
+    CK(cudaMemcpy(e, ss->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e[0]) {
+        CK(cudaMemset(ss->d_err, 0, sizeof(e)));
+        if (e[0] == 2)
             return fail(RTM_ERR_CUDA, "a persistent pass gave up waiting for the work items of other blocks");
-        return fail(RTM_ERR_CUDA, "a stencil kernel gave up waiting for its tile (TMA copy did not complete)");
+        char where[200] = "";
+        if (e[1]) {
+            unsigned item = 0;
+            if (ss->persist && e[2] >= 0 && e[2] < ss->trace_len)
+                cudaMemcpy(&item, ss->d_trace + e[2], sizeof(unsigned), cudaMemcpyDeviceToHost);
+            std::snprintf(where, sizeof where, " (block %d, barrier at shared 0x%x, state 0x%08x%08x, persistent item %u)",
+                          e[2], (unsigned)e[3], (unsigned)e[5], (unsigned)e[4], item);
+        }
+        return fail(RTM_ERR_CUDA, std::string("a stencil kernel gave up waiting for its tile (TMA copy did not complete)") +
+                                      where);
     }
     return RTM_OK;
 }
@@ -629,7 +640,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->arena.label = "tables and flags";
     ss->d_shots = (ShotDev *)ss->arena.take(sizeof(ShotDev) * B * (ss->fused ? 4 : 1));
     ss->d_tmaps = ss->arena.take((size_t)B * RTM_TMAP_COUNT * RTM_TMAP_BYTES);
-    ss->d_err = (int *)ss->arena.take(sizeof(int));
+    ss->d_err = (int *)ss->arena.take(8 * sizeof(int));
     ss->d_nonfinite = (int *)ss->arena.take(sizeof(int));
     if (!ss->d_tmaps || !ss->d_err || !ss->d_nonfinite) return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     if (o.verbose && o.tsnap > 0.0f) {
@@ -640,7 +651,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             if (!ss->d_absmax) return fail(RTM_ERR_NOMEM, "device arena exhausted (snapshots)");
         }
     }
-    CK(cudaMemsetAsync(ss->d_err, 0, sizeof(int), ss->stream));
+    CK(cudaMemsetAsync(ss->d_err, 0, 8 * sizeof(int), ss->stream));
     // tile tables sized for the shortest tile height the tuner or the environment may choose
     const int bz_min = 8;
     int tiles_per_shot = ((big.X + RTM_BX - 1) / RTM_BX + 1) * ((big.Z + bz_min - 1) / bz_min + 1);
@@ -654,6 +665,8 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
     ss->d_per_shot = (int *)ss->arena.take(6 * sizeof(int) * B);
     ss->d_queue = (unsigned *)ss->arena.take(2 * sizeof(unsigned));
     ss->d_done = (unsigned *)ss->arena.take(4 * sizeof(unsigned) * B);
+    ss->trace_len = 148 * 16;
+    ss->d_trace = (unsigned *)ss->arena.take(sizeof(unsigned) * ss->trace_len);
     if (!ss->d_counts || !ss->d_per_shot || !ss->d_queue || !ss->d_done)
         return fail(RTM_ERR_NOMEM, "device arena exhausted (tables)");
     if (!ss->d_shots || !ss->d_tiles || !ss->d_tiles_p || !ss->d_tiles_r || !ss->d_tiles_pr || !ss->d_fin)
@@ -1139,6 +1152,8 @@ static int persistent_pass(rtm_session *ss, BatchRun &br, int dir, int nsteps, b
     P.queue = ss->d_queue;
     P.done = ss->d_done;
     P.wait_ns = ss->pass_wait_ns;
+    P.trace = ss->d_trace;
+    P.trace_len = ss->trace_len;
     CK(cudaMemsetAsync(ss->d_queue, 0, 2 * sizeof(unsigned), st));
     CK(cudaMemsetAsync(ss->d_done, 0, 4 * sizeof(unsigned) * ss->B, st));
     cudaEvent_t e;

@@ -553,6 +553,7 @@ __global__ void __launch_bounds__(BX, DIR == 0 ? 5 : 4) k_pass(const PassArgs P)
         __syncthreads();
         const unsigned item = s_item;
         if (item >= total) return;
+        if (threadIdx.x == 0 && (int)blockIdx.x < P.trace_len) P.trace[blockIdx.x] = item;
         const int k = (int)(item / per);
         int r = (int)(item - (unsigned)k * per);
         StepArgs a = P.a;

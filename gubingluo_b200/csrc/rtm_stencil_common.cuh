@@ -90,6 +90,16 @@ __device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err)
 {
     for (long i = 0; i < kWaitLimit; i++)
         if (mbar_done(bar)) return true;
+    // the first block to give up records where: its index, the barrier's shared address and
+    // its 64-bit state word (err[1..5]; the host adds them to the error message)
+    if (atomicCAS(err + 1, 0, 1) == 0) {
+        unsigned long long w;
+        asm volatile("ld.shared.b64 %0, [%1];\n" : "=l"(w) : "r"(smem_u32(bar)) : "memory");
+        err[2] = (int)blockIdx.x;
+        err[3] = (int)smem_u32(bar);
+        err[4] = (int)(unsigned)w;
+        err[5] = (int)(unsigned)(w >> 32);
+    }
     atomicExch(err, 1);
     for (long i = 0; i < kWaitLimit; i++)
         if (mbar_done(bar)) break;

@@ -182,4 +182,6 @@ struct PassArgs {
     unsigned *queue;         // next item (starts at 0)
     unsigned *done;          // [4][B] completed items per phase and shot (start at 0)
     long long wait_ns;       // bound on one wait for other blocks' items (then the error flag, 2)
+    unsigned *trace;         // [trace_len] the item each block took last (for error reports)
+    int trace_len;
 };
