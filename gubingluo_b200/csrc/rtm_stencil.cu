@@ -43,10 +43,10 @@
 // 8-row reconstruction tiles (5, which would spill at 6); with its interior-tile body the
 // reconstruction runs 4% faster at 6 than at 5.
 // The work of one block on tile t (the kernels below, and the persistent pass kernel);
-// `sw` is the block's dynamic shared memory; `reinit`: the block has staged a tile with this
-// function before (its mbarrier is invalidated and initialised again).
+// `sw` is the block's dynamic shared memory; `use`: how many tiles the block has staged with
+// this function before (the first use initialises the mbarrier, use n waits for its phase n).
 template <int BZ, int MODE>
-__device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, float *sw, bool reinit = false)
+__device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, float *sw, unsigned use = 0)
 {
     constexpr int U = MODE == 3 ? UVR : UV, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
@@ -61,8 +61,7 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
     const float *__restrict__ inv_rho = (MODE >= 2) ? S.inv_rho_b : S.inv_rho_f;
     const PmlOffsets o = pml_offsets(X, Z);
     if (threadIdx.x == 0) {   // p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139
-        if (reinit) mbar_inval(&s_bar);   // a persistent block's earlier tile used it
-        mbar_init(&s_bar);
+        if (use == 0) mbar_init(&s_bar);   // a persistent block keeps it between its tiles
         mbar_expect(&s_bar, WH * WW * sizeof(float));
         tma_box(sw, tmap_of(S, MODE == 2 ? RTM_TMAP_B_P : (MODE == 3 ? RTM_TMAP_A_P_RECON : RTM_TMAP_A_P)), x0 - 12,
                 z0 - 9, &s_bar);
@@ -116,7 +115,7 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
     };
     if (x < X && z0 + U <= zend) load_group(z0, cir, cov, cow);
     __syncthreads();
-    if (!tile_wait(&s_bar, a.err) || x >= X) return;   // no barrier below
+    if (!tile_wait(&s_bar, a.err, use & 1u) || x >= X) return;   // no barrier below
 
     const float *col = &sw[tx + 12];   // staged column x: col[r*WW] = p[z0-9+r][x]
     float q[QN];                        // q[k] = p[z-9+k][x] at the current row z
@@ -238,7 +237,7 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
 // PML, source or receiver tests and no split-field loads, in the arithmetic of the general
 // body's interior branch (for the reconstruction: tiles of the interior with no source cell).
 template <int BZ, int MODE, typename ACC>
-__device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const TileRef t, float *sm, bool reinit = false)
+__device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const TileRef t, float *sm, unsigned use = 0)
 {
     constexpr int U = MODE == 2 ? UPR : MODE == 3 ? UPC : UP, QN = 2 * R + U - 1;
     static_assert(BZ % U == 0, "interior tiles take whole row groups");
@@ -256,8 +255,7 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
     const float *__restrict__ kappa = (MODE >= 2) ? S.kappa_b : S.kappa_f;
     const PmlOffsets o = pml_offsets(X, Z);
     if (threadIdx.x == 0) {   // vx rows z0 .. z0+BZ-1 (columns x0-12 ..), vz rows z0-10 .. z0+BZ+11
-        if (reinit) mbar_inval(&s_bar);   // a persistent block's earlier tile used it
-        mbar_init(&s_bar);
+        if (use == 0) mbar_init(&s_bar);   // a persistent block keeps it between its tiles
         mbar_expect(&s_bar, (XH * WW + ZH * BX) * sizeof(float));
         tma_box(svx, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VX : RTM_TMAP_A_VX), x0 - 12, z0, &s_bar);
         tma_box(svz, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VZ : RTM_TMAP_A_VZ), x0, z0 - 10, &s_bar);
@@ -336,7 +334,7 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
     };
     if (x < X && z0 + U <= zend) load_group(z0, ckk, cp0, cs1, cs2, cps, cg1, cil);
     __syncthreads();
-    if (!tile_wait(&s_bar, a.err) || x >= X) return;
+    if (!tile_wait(&s_bar, a.err, use & 1u) || x >= X) return;
 
     const float *colx = &svx[tx + 12];   // colx[r*WW] = vx[z0+r][x]
     const float *colz = &svz[tx];        // colz[r*BX] = vz[z0-10+r][x]
@@ -546,7 +544,7 @@ __global__ void __launch_bounds__(BX, DIR == 0 ? 5 : 4) k_pass(const PassArgs P)
     const int per = DIR == 0 ? P.len[0] + P.len[1] + ns : P.len[0] + P.len[1] + P.len[2] + P.len[3];
     const unsigned total = (unsigned)per * (unsigned)P.nsteps;
     const int *cnt = P.per_shot;
-    unsigned used = 0;   // bit ph: this block has run the tile function of phase ph (its mbarrier)
+    unsigned uses[4] = {0, 0, 0, 0};   // tiles this block has staged with each phase's function
     for (;;) {
         __syncthreads();   // the previous item's shared memory is free
         if (threadIdx.x == 0) s_item = *(volatile int *)P.a.err ? total : atomicAdd(P.queue, 1u);
@@ -597,20 +595,22 @@ __global__ void __launch_bounds__(BX, DIR == 0 ? 5 : 4) k_pass(const PassArgs P)
         }
         __syncthreads();
         if (!s_ok) return;
-        const bool reinit = (used >> ph) & 1u;
-        used |= 1u << ph;
+        unsigned use = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (q == ph) use = uses[q]++;
         if (DIR == 0) {
-            if (ph == 0) vel_tile<BZV, 0>(a, t, sm, reinit);
-            else if (ph == 1) pres_tile<BZP, 0, float>(a, P.record, t, sm, reinit);
+            if (ph == 0) vel_tile<BZV, 0>(a, t, sm, use);
+            else if (ph == 1) pres_tile<BZP, 0, float>(a, P.record, t, sm, use);
             else {
                 const ShotDev &S = a.shots[s];
                 for (int i = threadIdx.x; i < S.strip_len; i += BX) strip_save_cell(S, i, k, a.ring, P.strip_prec);
             }
         } else {
-            if (ph == 0) vel_tile<BZVR, 3>(a, t, sm, reinit);
-            else if (ph == 1) pres_tile<BZP, 3, float>(a, 0, t, sm, reinit);
-            else if (ph == 2) vel_tile<BZV, 2>(a, t, sm, reinit);
-            else pres_tile<BZP, 2, ACC>(a, 0, t, sm, reinit);
+            if (ph == 0) vel_tile<BZVR, 3>(a, t, sm, use);
+            else if (ph == 1) pres_tile<BZP, 3, float>(a, 0, t, sm, use);
+            else if (ph == 2) vel_tile<BZV, 2>(a, t, sm, use);
+            else pres_tile<BZP, 2, ACC>(a, 0, t, sm, use);
         }
         __syncthreads();   // every thread's writes of the item are done
         if (threadIdx.x == 0) {

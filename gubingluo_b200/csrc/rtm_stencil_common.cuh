@@ -74,22 +74,23 @@ __device__ __forceinline__ void tma_box(float *dst, const void *tmap, int x, int
         "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
-__device__ __forceinline__ bool mbar_done(unsigned long long *bar)
+// True once the barrier's phase of the given parity (0: the first phase after init) is done.
+__device__ __forceinline__ bool mbar_done(unsigned long long *bar, unsigned parity = 0)
 {
     unsigned ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar))
+        : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     return ok != 0;
 }
 // Wait for the tile; on giving up, flag the error, wait once more (bounded) for the copies
 // still in flight and report false, so that the block returns without computing.
-__device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err)
+__device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err, unsigned parity = 0)
 {
     for (long i = 0; i < kWaitLimit; i++)
-        if (mbar_done(bar)) return true;
+        if (mbar_done(bar, parity)) return true;
     // the first block to give up records where: its index, the barrier's shared address and
     // its 64-bit state word (err[1..5]; the host adds them to the error message)
     if (atomicCAS(err + 1, 0, 1) == 0) {
@@ -102,7 +103,7 @@ __device__ __forceinline__ bool tile_wait(unsigned long long *bar, int *err)
     }
     atomicExch(err, 1);
     for (long i = 0; i < kWaitLimit; i++)
-        if (mbar_done(bar)) break;
+        if (mbar_done(bar, parity)) break;
     return false;
 }
 // Fixed-grid launches: true for the blocks past the batch's tile list (see StepArgs::counts).
