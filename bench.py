@@ -185,10 +185,10 @@ def ncu_traffic_per_unit(kernel: str, X: int, Z: int):
 # ------------------------------------------------------------------------------------------
 # kernel families timed by the session (split kernels; whole-step kernel)
 KERNEL_FAMILIES = ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv", "step_fwd", "step_recon",
-                   "step_recv")
+                   "step_recv", "pass_fwd", "pass_bwd")
 
 
-def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int) -> float:
+def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int, nt: int = 1) -> float:
     """Algorithmic DRAM bytes of one launch of `kind` for one shot: every array the kernel
     must read or write, once (4-byte fields; PML split fields excluded as thin bands).
       vel_fwd, vel_recv:   read p, 1/rho; read+write vx, vz            24 B per padded cell
@@ -199,7 +199,8 @@ def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum
       step_fwd, step_recv (whole step): read p, vx, vz, 1/rho, kappa; write p, vx, vz   32 B per padded cell
       step_recon: the same on the interior, with both strip sets       32 B per interior cell
     plus the boundary strips the reconstruction kernels read (the forward strips are written
-    by a separate copy kernel)."""
+    by a separate copy kernel).  pass_fwd / pass_bwd (persistent passes, one launch per pass of
+    nt steps): the per-step kernels' bytes times the steps, with the strip saves."""
     cells, inner = X * Z, nxi * nzi
     strips = 80 * (nxi + nzi)   # vx+vz or p strips of one step, fp32
     table = {
@@ -214,6 +215,9 @@ def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum
         "step_recon": 32 * inner + 2 * strips,
         "step_recv": 32 * cells + (4 + 4 * accum_bytes) * inner + 4 * nrec,
     }
+    # persistent passes (one launch per pass): the per-step kernels' bytes times the steps
+    table["pass_fwd"] = nt * (table["vel_fwd"] + table["pres_fwd"] + 8 * 40 * (nxi + nzi))
+    table["pass_bwd"] = (nt - 1) * (table["vel_recon"] + table["pres_recon"] + table["vel_recv"] + table["pres_recv"])
     return table[kind]
 
 
@@ -377,7 +381,7 @@ def run_ours(args, rank, world, local_rank):
     # algorithmic bytes of the first launch of a timed step: each shot's own window
     first = step_shots[W * B:W * B + nshots_launch]
     bytes_launch = sum(kernel_bytes(dom, geos[sh].nxpad, geos[sh].nzpad, geos[sh].nxlength, s.nz, geos[sh].nrec,
-                                    accum_bytes) for sh in first)
+                                    accum_bytes, s.nt) for sh in first)
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_hbm_peak()
     per_cell = ncu_traffic_per_unit(dom, X, Z)
