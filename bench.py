@@ -103,6 +103,8 @@ def parse():
     ap.add_argument("--headline-only", action="store_true", help="run only the configuration-4 comparison")
     ap.add_argument("--headline-sample", type=int, default=8,
                     help="plain per-shot arm: every k-th shot of the 256 (default 8: 32 shots)")
+    ap.add_argument("--headline-arms", default="batched,plain,nograph",
+                    help="which arms of the configuration-4 comparison to run (comma-separated)")
     return ap.parse_args()
 
 
@@ -466,14 +468,17 @@ def run_headline(args, local_rank):
                 "mean_cell_updates_per_shot": w / len(arm_shots), "batches": st.batches,
                 "kernel_launches": st.kernel_launches, "kernel_ms": kern, "tile_rows": tiles}
 
+    arms = set(args.headline_arms.split(","))
+    empty = {"shots": 0, "shots_per_s": None, "gcell_updates_per_s": None}
     batched = timed(G.RunOptions(device=local_rank, strip_precision="fp16", gather_precision="fp16",
-                                 accum_fp64=True), shots, 4)
+                                 accum_fp64=True), shots, 4) if "batched" in arms else empty
     sample = shots[args.headline_sample // 2::args.headline_sample]
-    plain = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), sample, 1)
+    plain = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), sample, 1) if "plain" in arms else empty
     nog = sample[:8]
-    plain_nograph = timed(G.RunOptions(device=local_rank, batch=1), nog, 1)
+    plain_nograph = timed(G.RunOptions(device=local_rank, batch=1), nog, 1) if "nograph" in arms else empty
     # the graph arm on the same 8 shots, for the launch-gap comparison
-    plain_graph8 = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), nog, 1)
+    plain_graph8 = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), nog, 1) if "nograph" in arms \
+        else empty
     ap = meta["apertures"]
     return {"workload": ("config 4: 3201x801 grid (10 m), 40-cell PML, nt=%d, dt=0.8 ms, 20 Hz Ricker, 256 shots, "
                          "apertures drawn from %d-%d columns (layout-1 windows cut at the model's edges), "
@@ -486,7 +491,8 @@ def run_headline(args, local_rank):
             "plain_fp32_per_shot_no_graph": {**plain_nograph, "form": "fp32, one shot per launch, direct launches",
                                              "sample": f"the first {len(nog)} shots of that sample"},
             "plain_fp32_per_shot_graph_same_8": plain_graph8,
-            "ratio": round(batched["gcell_updates_per_s"] / plain["gcell_updates_per_s"], 3),
+            "ratio": (round(batched["gcell_updates_per_s"] / plain["gcell_updates_per_s"], 3)
+                      if batched["shots"] and plain["shots"] else None),
             "ratio_basis": "Gcell-updates/s (shots/s at equal work per shot)",
             "target": 3.0, "setup_seconds_data_modelling": round(t_data, 2)}
 
