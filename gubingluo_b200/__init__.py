@@ -215,7 +215,7 @@ class RunOptions:
     gather_precision: str = "fp32"
     accum_fp64: int = 0     # 0 fp32, 1 (or True) fp64, 2 compensated fp32 pairs; 1 and 2 stack in fp64
     batch: int = 0
-    use_graph: bool = False
+    use_graph: int = 0      # 1: each pass as a CUDA graph per launch shape; 2: with rounded fixed grids
     verbose: bool = False
     extra_images: int = 0   # 1: image3/4/5 and imagetrue, indexing corrected; 2: the reference's
     tsnap: float = 0.0      # with verbose: print max |p| per shot every tsnap seconds

@@ -758,7 +758,7 @@ struct BatchRun {
 // device tile counts that the blocks past the batch's tiles check.
 static int list_grid(rtm_session *ss, BatchRun &br, StepArgs &a, int L)
 {
-    a.counts = ss->o.use_graph ? ss->d_counts : nullptr;
+    a.counts = ss->o.use_graph == 2 ? ss->d_counts : nullptr;
     a.list = L;
     return br.grid[L];
 }
@@ -972,9 +972,10 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         br.ex_nxi = std::max(br.ex_nxi, ss->shots[k0 + j].nxi);
         br.ex_nzi = std::max(br.ex_nzi, ss->shots[k0 + j].nzi);
     }
-    if (o.use_graph) {
-        // graph replays launch fixed grids: the counts rounded up to four significant bits
-        // (at most 12.5% of blocks idle), so batches of nearby sizes share one captured graph
+    if (o.use_graph == 2) {
+        // use_graph 2: graph replays launch fixed grids, the counts rounded up to four
+        // significant bits (at most 12.5% of blocks idle), so batches of nearby sizes share one
+        // captured graph (use_graph 1: exact grids, one graph per launch shape)
         auto bucket = [](int v) {
             int e = 0;
             while ((v >> e) >= 16) e++;
@@ -1012,8 +1013,11 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     a.accum_fp64 = o.accum_fp64;
     a.err = ss->d_err;
     {
-        const char *e = std::getenv("RTM_B200_PREFETCH");   // 0: no L2 prefetch of tile operand rows
-        a.prefetch = !(e && *e && std::atoi(e) == 0);
+        // L2 prefetch of the tiles' operand rows: on for batches of 4 shots or more (measured:
+        // +4% at 64 shots per launch, -6% at one shot per launch, where few blocks run and the
+        // extra instructions are not hidden); RTM_B200_PREFETCH=0 / 1 forces it
+        const char *e = std::getenv("RTM_B200_PREFETCH");
+        a.prefetch = (e && *e) ? std::atoi(e) != 0 : n >= 4;
     }
     ss->last_batch_n = n;
     ss->last_batch_shots.clear();
@@ -1091,7 +1095,7 @@ static int run_pass(rtm_session *ss, std::vector<long> key, F &&body)
     }
     auto it = ss->graphs.find(key);
     if (it == ss->graphs.end()) {
-        if (ss->graphs.size() >= 16) {   // bound the cache: shapes vary with uneven apertures
+        if (ss->graphs.size() >= 32) {   // bound the cache: shapes vary with uneven apertures
             for (auto &kv : ss->graphs) cudaGraphExecDestroy(kv.second.exec);
             ss->graphs.clear();
         }

@@ -82,8 +82,11 @@ typedef struct rtm_options {
     int use_graph;           /* 1: each pass's time loop (source pass; backward pass) runs as one
                                 CUDA graph, captured the first time a launch shape (shots per
                                 batch, tile counts) occurs and replayed for later batches of that
-                                shape; results are bit-identical to direct launches.  Not used with
-                                tsnap snapshots, and per-kernel timing is not sampled. */
+                                shape; 2: the same with grids rounded up to four significant bits
+                                (blocks past the batch's tiles return), so batches of nearby
+                                shapes share a graph.  Results are bit-identical to direct
+                                launches.  Not used with tsnap snapshots, and per-kernel timing is
+                                not sampled. */
     int verbose;             /* print per-batch progress like the reference */
     int extra_images;        /* the reference's other imaging conditions (kernel.cu:1417-1555):
                                 0 off; 1 wavefield decomposition, Poynting-angle and energy-norm

@@ -475,12 +475,13 @@ def test_tile_heights_do_not_change_the_bits(rtmlib, monkeypatch):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("strips", ["fp32", "fp16"])
-def test_graph_replay_is_bitwise_identical(rtmlib, monkeypatch, strips):
-    """use_graph: each pass's time loop captured once per launch shape and replayed gives the
-    gathers and images of direct launches bit for bit.  One shot per launch over shots of
-    three window widths (layout 1, offsetmax cut at the model's edges), so that graphs are
-    both captured and replayed, with packed strips too."""
+@pytest.mark.parametrize("strips,graph", [("fp32", 1), ("fp16", 1), ("fp32", 2), ("fp16", 2)])
+def test_graph_replay_is_bitwise_identical(rtmlib, monkeypatch, strips, graph):
+    """use_graph: each pass's time loop captured once per launch shape (1) or per rounded
+    grid (2, blocks past the batch's tiles return) and replayed gives the gathers and images of
+    direct launches bit for bit.  One shot per launch over shots of three window widths
+    (layout 1, offsetmax cut at the model's edges), so that graphs are both captured and
+    replayed, with packed strips too."""
     G = rtmlib
     monkeypatch.setenv("RTM_B200_TUNE", "0")   # tile-height trials would add launches to the first run only
     c = GENERAL[2]
@@ -491,7 +492,7 @@ def test_graph_replay_is_bitwise_identical(rtmlib, monkeypatch, strips):
     assert len(widths) > 1
     base = dict(batch=1, strip_precision=strips)
     want = G.migrate(s, G.RunOptions(**base), shots, v, rho)
-    got = G.migrate(s, G.RunOptions(use_graph=True, **base), shots, v, rho)
+    got = G.migrate(s, G.RunOptions(use_graph=graph, **base), shots, v, rho)
     for k in ("image1", "image2s", "illum"):
         assert np.array_equal(got[k], want[k]), k
     for a, b in zip(got["gathers"], want["gathers"]):
@@ -592,7 +593,7 @@ def test_whole_step_kernel_is_bitwise_identical(rtmlib, monkeypatch, form):
     passes replayed as CUDA graphs."""
     G = rtmlib
     opts = dict(fp32=dict(), fp64=dict(accum_fp64=1, extra_images=1),
-                fp16=dict(strip_precision="fp16", gather_precision="fp16", use_graph=True),
+                fp16=dict(strip_precision="fp16", gather_precision="fp16", use_graph=2),
                 kahan=dict(accum_fp64=2, batch=1))[form]
     for ci, c in enumerate(GENERAL):
         v, rho = _random_model(c["nz"], c["nx"], 40 + ci)
