@@ -103,7 +103,7 @@ def parse():
     ap.add_argument("--headline-only", action="store_true", help="run only the configuration-4 comparison")
     ap.add_argument("--headline-sample", type=int, default=8,
                     help="plain per-shot arm: every k-th shot of the 256 (default 8: 32 shots)")
-    ap.add_argument("--headline-arms", default="batched,plain,nograph",
+    ap.add_argument("--headline-arms", default="batched,plain,graph",
                     help="which arms of the configuration-4 comparison to run (comma-separated)")
     return ap.parse_args()
 
@@ -406,14 +406,16 @@ def run_headline(args, local_rank):
 
       batched: all 256 shots in one session, as many per launch as device memory holds,
                fp16 boundary strips and gathers, fp64 image accumulation;
-      plain per-shot: plain FP32 (strips, gathers, accumulators), one shot per launch with
-               each pass's time loop replayed as a CUDA graph, on every k-th shot of the
-               survey (--headline-sample; the apertures are drawn independently of the shot
-               number, so the sample has the survey's spread); also timed without the graph.
+      plain per-shot: plain FP32 (strips, gathers, accumulators), one shot per launch, on
+               every k-th shot of the survey (--headline-sample; the apertures are drawn
+               independently of the shot number, so the sample has the survey's spread),
+               timed with direct launches and with each pass's time loop replayed as a CUDA
+               graph.
 
     Both are timed with CUDA events on the session stream, gathers resident.  The ratio is
-    taken at equal work per shot: Gcell-updates/s of the batched arm over that of the
-    per-shot arm (= shots/s over shots/s when both arms' shots have the same mean size).
+    taken at equal work per shot: Gcell-updates/s of the batched arm over that of the faster
+    per-shot arm, direct launches or graph replays (= shots/s over shots/s when both arms'
+    shots have the same mean size).
     The image error of both forms against the FP64 oracle is tested in
     tests/test_gpu_configs.py (narrowest and widest aperture, full nt)."""
     import torch
@@ -473,12 +475,14 @@ def run_headline(args, local_rank):
     batched = timed(G.RunOptions(device=local_rank, strip_precision="fp16", gather_precision="fp16",
                                  accum_fp64=True), shots, 4) if "batched" in arms else empty
     sample = shots[args.headline_sample // 2::args.headline_sample]
-    plain = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), sample, 1) if "plain" in arms else empty
-    nog = sample[:8]
-    plain_nograph = timed(G.RunOptions(device=local_rank, batch=1), nog, 1) if "nograph" in arms else empty
-    # the graph arm on the same 8 shots, for the launch-gap comparison
-    plain_graph8 = timed(G.RunOptions(device=local_rank, batch=1, use_graph=True), nog, 1) if "nograph" in arms \
-        else empty
+    # plain FP32, one shot per launch: direct launches, and each pass replayed as a CUDA graph
+    # (rounded grids, so that shots of nearby windows share a graph; every shot here has its
+    # own window, and a graph per exact shape would be captured once per shot)
+    plain = timed(G.RunOptions(device=local_rank, batch=1), sample, 1) if "plain" in arms else empty
+    plain_graph = timed(G.RunOptions(device=local_rank, batch=1, use_graph=2), sample, 1) \
+        if "graph" in arms else empty
+    best = max((a for a in (plain, plain_graph) if a["shots"]), key=lambda a: a["gcell_updates_per_s"],
+               default=None)
     ap = meta["apertures"]
     return {"workload": ("config 4: 3201x801 grid (10 m), 40-cell PML, nt=%d, dt=0.8 ms, 20 Hz Ricker, 256 shots, "
                          "apertures drawn from %d-%d columns (layout-1 windows cut at the model's edges), "
@@ -486,13 +490,14 @@ def run_headline(args, local_rank):
                          % (s.nt, min(ap.values()), max(ap.values()))),
             "batched_mixed": {**batched, "form": "fp16 strips + fp16 gathers + fp64 images, all 256 shots, "
                                                    "as many per launch as fit"},
-            "plain_fp32_per_shot": {**plain, "form": "fp32, one shot per launch, CUDA graph per pass",
+            "plain_fp32_per_shot": {**plain, "form": "fp32, one shot per launch, direct launches",
                                     "sample": f"every {args.headline_sample}th shot ({len(sample)} shots)"},
-            "plain_fp32_per_shot_no_graph": {**plain_nograph, "form": "fp32, one shot per launch, direct launches",
-                                             "sample": f"the first {len(nog)} shots of that sample"},
-            "plain_fp32_per_shot_graph_same_8": plain_graph8,
-            "ratio": (round(batched["gcell_updates_per_s"] / plain["gcell_updates_per_s"], 3)
-                      if batched["shots"] and plain["shots"] else None),
+            "plain_fp32_per_shot_graph": {**plain_graph, "form": "fp32, one shot per launch, each pass replayed as "
+                                                               "a CUDA graph (rounded grids)",
+                                          "sample": "the same shots"},
+            "ratio": (round(batched["gcell_updates_per_s"] / best["gcell_updates_per_s"], 3)
+                      if batched["shots"] and best else None),
+            "ratio_denominator": "the faster of the two plain per-shot arms",
             "ratio_basis": "Gcell-updates/s (shots/s at equal work per shot)",
             "target": 3.0, "setup_seconds_data_modelling": round(t_data, 2)}
 
