@@ -192,30 +192,34 @@ KERNEL_FAMILIES = ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv",
 
 def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int, nt: int = 1) -> float:
     """Algorithmic DRAM bytes of one launch of `kind` for one shot: every array the kernel
-    must read or write, once (4-byte fields; PML split fields excluded as thin bands).
+    must read or write, once (4-byte fields).
       vel_fwd, vel_recv:   read p, 1/rho; read+write vx, vz            24 B per padded cell
       pres_fwd, pres_recv: read vx, vz, kappa; read+write p            20 B per padded cell
+                           + in the PML band (padded minus interior cells) the split parts
+                           sx, sz read and written, the old p not read: +12 B per band cell
       vel_recon:  read ps, 1/rho; read+write vxs, vzs on the interior  24 B per interior cell
       pres_recon: read vxs, vzs, kappa; read+write ps on the interior  20 B per interior cell
       pres_recv adds the imaging: read ps, read+write g1 and illum     4 + 4*accum B per interior cell
       step_fwd, step_recv (whole step): read p, vx, vz, 1/rho, kappa; write p, vx, vz   32 B per padded cell
+                           + sx, sz read and written in the band       +16 B per band cell
       step_recon: the same on the interior, with both strip sets       32 B per interior cell
     plus the boundary strips the reconstruction kernels read (the forward strips are written
     by a separate copy kernel).  pass_fwd / pass_bwd (persistent passes, one launch per pass of
     nt steps): the per-step kernels' bytes times the steps, with the strip saves."""
     cells, inner = X * Z, nxi * nzi
+    band = cells - inner
     strips = 80 * (nxi + nzi)   # vx+vz or p strips of one step, fp32
     table = {
         "vel_fwd": 24 * cells,
-        "pres_fwd": 20 * cells,
+        "pres_fwd": 20 * cells + 12 * band,
         "vel_recon": 24 * inner + strips,
         "pres_recon": 20 * inner + strips,
         "vel_recv": 24 * cells,
-        "pres_recv": 20 * cells + (4 + 4 * accum_bytes) * inner + 4 * nrec,
+        "pres_recv": 20 * cells + 12 * band + (4 + 4 * accum_bytes) * inner + 4 * nrec,
         # whole-step kernel: read p, vx, vz, 1/rho, kappa; write p, vx, vz once per cell
-        "step_fwd": 32 * cells,
+        "step_fwd": 32 * cells + 16 * band,
         "step_recon": 32 * inner + 2 * strips,
-        "step_recv": 32 * cells + (4 + 4 * accum_bytes) * inner + 4 * nrec,
+        "step_recv": 32 * cells + 16 * band + (4 + 4 * accum_bytes) * inner + 4 * nrec,
     }
     # persistent passes (one launch per pass): the per-step kernels' bytes times the steps
     table["pass_fwd"] = nt * (table["vel_fwd"] + table["pres_fwd"] + 8 * 40 * (nxi + nzi))
@@ -393,7 +397,11 @@ def run_ours(args, rank, world, local_rank):
                                                                               for sh in first)),
                 "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 4),
                 "launches_sampled": sampled[dom][1],
-                "kernel_ms": {k: round(v[0], 4) for k, v in sampled.items()}}
+                "kernel_ms": {k: round(v[0], 4) for k, v in sampled.items()},
+                # every family's algorithmic bytes per launch / its mean event time, of the same peak
+                "kernel_frac": {k: round(sum(kernel_bytes(k, geos[sh].nxpad, geos[sh].nzpad, geos[sh].nxlength, s.nz,
+                                                          geos[sh].nrec, accum_bytes, s.nt) for sh in first)
+                                         / (v[0] * 1e-3) / 1e9 / peak, 4) for k, v in sampled.items()}}
     return dict(value=value, gcell=gcell, ms_total=ms_total, launches=launches, e2e=e2e, roofline=roofline, tiles=tiles,
                 clocks=clock_info, shots_done=shots_done, t_data=t_data, X=X, Z=Z, nxi=nxi, nzi=nzi, nrec=nrec,
                 w_shot=w_timed / (K * B), s=s, shots_per_launch=nshots_launch, meta=meta, all_shots=all_shots)
@@ -448,10 +456,8 @@ def run_headline(args, local_rank):
         for k, sh in enumerate(arm_shots):
             ss.set_gather(k, gathers[sh])
         stream = torch.cuda.ExternalStream(ss.stream())
-        # the tuner's trials for the batch shapes of the timed run, then a short warm-up
-        B = ss.batch_size()
-        for k0 in range(0, len(arm_shots), B):
-            ss.prepare(k0, min(B, len(arm_shots) - k0))
+        # the tuner's trials for the launch shapes of the timed run, then a short warm-up
+        ss.prepare(0, len(arm_shots))
         ss.run_range(0, warm)
         ss.reset_images()
         torch.cuda.synchronize()

@@ -103,7 +103,7 @@ def lib() -> C.CDLL:
     L.rtm_session_reset_images.argtypes = [vp]
     L.rtm_session_nrec.argtypes = [vp, C.c_int]
     L.rtm_session_get_pml.argtypes = [vp, C.c_int, vp, vp, vp, vp]
-    L.rtm_session_tile_heights.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.rtm_session_tile_heights.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
     L.rtm_session_prepare.argtypes = [vp, C.c_int, C.c_int]
     L.rtm_session_batch_size.argtypes = [vp]
     L.rtm_session_stream.argtypes = [vp]
@@ -355,7 +355,7 @@ class Session:
         return ms, n.value
 
     def prepare(self, k0: int, n: int):
-        """Choose the kernel configuration for the batch shape of shots [k0, k0+n) now."""
+        """Choose the kernel configuration of every launch shape of run_range(k0, n) now."""
         _check(lib().rtm_session_prepare(self.h, k0, n))
 
     def batch_size(self) -> int:
@@ -363,10 +363,11 @@ class Session:
         return lib().rtm_session_batch_size(self.h)
 
     def tile_heights(self):
-        """Rows per tile in use: {"vel", "vel_recon", "pres"} (tuned per launch shape)."""
-        v = [C.c_int(0) for _ in range(3)]
+        """Rows per tile in use: {"vel", "vel_recon", "pres", "pres_recon"} (tuned per launch
+        shape)."""
+        v = [C.c_int(0) for _ in range(4)]
         _check(lib().rtm_session_tile_heights(self.h, *[C.byref(x) for x in v]))
-        return dict(zip(("vel", "vel_recon", "pres"), [x.value for x in v]))
+        return dict(zip(("vel", "vel_recon", "pres", "pres_recon"), [x.value for x in v]))
 
     def pml_profiles(self, k: int, X: int, Z: int):
         """Shot k's device PML damping profiles (ddx [X], ddz [Z], ddxvx [X-1], ddzvz [Z-1])."""

@@ -15,7 +15,7 @@
 #include "rtm_internal.h"
 
 namespace rtm {
-int session_batch_size(rtm_session *ss);
+int session_wave_size(const rtm_session *ss, int remaining);
 int session_run_range(rtm_session *ss, int k0, int n);
 }  // namespace rtm
 
@@ -49,7 +49,6 @@ static void drive(const char *who, rtm_session *ss, const rtm_survey &s, const r
     const size_t nimg = (size_t)nx * nz;
     char path[512];
     int rc;
-    const int B = session_batch_size(ss);
     std::vector<float> tmp(nimg);
     std::vector<float> xi[7];   // image3s .. image5m, imagetrue (zero unless extra_images)
     for (auto &v : xi) v.assign(nimg, 0.0f);
@@ -77,8 +76,8 @@ static void drive(const char *who, rtm_session *ss, const rtm_survey &s, const r
     FILE *log = nullptr;
     if (const char *lp = std::getenv("RTM_B200_LOG"))
         if (*lp) log = std::fopen(lp, "a");
-    for (size_t k0 = start; k0 < shots.size(); k0 += B) {
-        int n = (int)std::min<size_t>(B, shots.size() - k0);
+    for (size_t k0 = start; k0 < shots.size();) {
+        const int n = session_wave_size(ss, (int)(shots.size() - k0));
         auto t0 = std::chrono::steady_clock::now();
         rc = session_run_range(ss, (int)k0, n);
         if (rc) {
@@ -130,6 +129,7 @@ static void drive(const char *who, rtm_session *ss, const rtm_survey &s, const r
                 if (write_image_su(path, t.img, nz, nx, dx)) std::printf("The file %s open failed !\n", path);
             }
         }
+        k0 += n;
     }
     if (log) std::fclose(log);
     rtm_session_get_images(ss, image1, image2s, image2m, illum);   // rtm_model.cu:575-585

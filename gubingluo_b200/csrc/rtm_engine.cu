@@ -131,8 +131,9 @@ struct rtm_session {
     TileRef *d_tiles_r = nullptr;    // velocity tiles of the reconstruction region (interior + strips)
     TileRef *d_tiles_pr = nullptr;   // pressure tiles of the reconstruction region
     // rows per tile (measured): 32 for the forward and receiver velocity kernels, 16 for the
-    // velocity reconstruction and the pressure kernels
-    int bz_vel = 32, bz_vel_recon = 16, bz_pres = 16;
+    // velocity reconstruction and the pressure kernels (forward and receiver pressure share
+    // one tile list; the pressure reconstruction has its own)
+    int bz_vel = 32, bz_vel_recon = 16, bz_pres = 16, bz_pres_recon = 16;
     // kernel form per family (forward/receiver velocity, reconstruction velocity, forward/receiver
     // pressure, reconstruction pressure): four columns by U rows per thread (rtm_stencil_v.cu)
     // or one column per thread (rtm_stencil.cu); the results are the same bits.  Chosen by the
@@ -470,9 +471,11 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
         e = std::getenv("RTM_B200_BZ_VEL_RECON");
         if (e && *e) ss->bz_vel_recon = std::atoi(e);
         e = std::getenv("RTM_B200_BZ_PRES");
-        if (e && *e) ss->bz_pres = std::atoi(e);
+        if (e && *e) ss->bz_pres = ss->bz_pres_recon = std::atoi(e);
+        e = std::getenv("RTM_B200_BZ_PRES_RECON");
+        if (e && *e) ss->bz_pres_recon = std::atoi(e);
         // tile heights set by hand turn the tuner off; so does RTM_B200_TUNE=0
-        for (const char *v : {"RTM_B200_BZ_VEL", "RTM_B200_BZ_VEL_RECON", "RTM_B200_BZ_PRES"})
+        for (const char *v : {"RTM_B200_BZ_VEL", "RTM_B200_BZ_VEL_RECON", "RTM_B200_BZ_PRES", "RTM_B200_BZ_PRES_RECON"})
             if ((e = std::getenv(v)) && *e) ss->tune = false;
         if ((e = std::getenv("RTM_B200_TUNE")) && *e && std::atoi(e) == 0) ss->tune = false;
         e = std::getenv("RTM_B200_KERNELS");
@@ -486,12 +489,12 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             ss->tune = false;
             ss->bz_vel = 32;
             ss->bz_vel_recon = 16;
-            ss->bz_pres = 16;
+            ss->bz_pres = ss->bz_pres_recon = 16;
             for (bool &v : ss->vec) v = false;
         }
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
         if (o.accum_fp64 < 0 || o.accum_fp64 > 2) return fail(RTM_ERR_ARG, "accum_fp64 must be 0, 1 or 2");
-        for (int bz : {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres})
+        for (int bz : {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->bz_pres_recon})
             if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
     }
     B = std::max(B, 1);
@@ -805,8 +808,11 @@ static void shot_tiles(const rtm_session *ss, const ShotState &sh, int j, bool f
     const rtm_survey &s = ss->s;
     std::vector<TileRef> &tiles = *L[0], &tiles_p = *L[1], &tiles_r = *L[2], &tiles_pr = *L[3];
     // whole-grid tiles, and the reconstruction's tiles: it writes only the interior and the
-    // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10)
-    const int xr0 = (s.npml - RTM_RADIUS) & ~3, xr1 = sh.X - s.npml + RTM_RADIUS;
+    // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10).  The
+    // reconstruction's tile columns start on a 32-column (128-byte) boundary, so that every
+    // warp's row access covers whole 128-byte lines (the kernels mask the cells outside the
+    // region)
+    const int xr0 = (s.npml - RTM_RADIUS) & ~31, xr1 = sh.X - s.npml + RTM_RADIUS;
     const int zr0 = s.npml - RTM_RADIUS, zr1 = sh.Z - s.npml + RTM_RADIUS;
     // velocity tiles: interior when every column lies in [npml, X-npml-1) and every row in
     // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies
@@ -852,9 +858,9 @@ static void shot_tiles(const rtm_session *ss, const ShotState &sh, int j, bool f
     if (!ss->fused) add_tiles(tiles_r, ss->bz_vel_recon, xr0, xr1, zr0, zr1);
     // reconstruction pressure tiles: interior when inside the pressure interior with no
     // source cell
-    for (int z0 = zr0; z0 < (ss->fused ? zr0 : zr1); z0 += ss->bz_pres)
+    for (int z0 = zr0; z0 < (ss->fused ? zr0 : zr1); z0 += ss->bz_pres_recon)
         for (int x0 = xr0; x0 < xr1; x0 += RTM_BX) {
-            const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres;
+            const int x1 = x0 + RTM_BX, z1 = z0 + ss->bz_pres_recon;
             const bool inside = x0 >= s.npml && x1 <= sh.X - s.npml && z0 >= s.npml && z1 <= sh.Z - s.npml;
             const bool src = x0 < sh.sbx0 + sh.sbnx && sh.sbx0 < x1 && z0 < sh.sbz0 + sh.sbnz && sh.sbz0 < z1;
             tiles_pr.push_back({j, x0, z0, (fast && inside && !src) ? 1 : 0});
@@ -903,7 +909,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         // tensor maps of the fields the stencil kernels stage, for this shot's row pitch
         {
             const int vh = ss->bz_vel + RTM_STAGE_ZEXTRA_VEL, ph = ss->bz_pres + RTM_STAGE_ZEXTRA_PRES;
-            const int vhr = ss->bz_vel_recon + RTM_STAGE_ZEXTRA_VEL;
+            const int vhr = ss->bz_vel_recon + RTM_STAGE_ZEXTRA_VEL, phr = ss->bz_pres_recon + RTM_STAGE_ZEXTRA_PRES;
             // whole-step kernel: p of both buffers of each wavefield (placeholders when off)
             const int sw = RTM_BX + 48, sh_ = ss->tz_step + 38;
             const WaveDev &A1 = ss->fused ? sl.a2 : sl.a, &B1 = ss->fused ? sl.b2 : sl.b;
@@ -913,7 +919,8 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
                 {sl.b.p, RTM_STAGE_W, vh}, {sl.b.vx, RTM_STAGE_W, ss->bz_pres}, {sl.b.vz, RTM_BX, ph},
                 {sl.a.p, RTM_STAGE_W, vhr}, {sl.a.p, sw, sh_}, {A1.p, sw, sh_}, {sl.b.p, sw, sh_}, {B1.p, sw, sh_},
                 {sl.a.vx, RTM_STAGE_W, tz}, {A1.vx, RTM_STAGE_W, tz}, {sl.b.vx, RTM_STAGE_W, tz}, {B1.vx, RTM_STAGE_W, tz},
-                {sl.a.vz, RTM_BX, tz + 20}, {A1.vz, RTM_BX, tz + 20}, {sl.b.vz, RTM_BX, tz + 20}, {B1.vz, RTM_BX, tz + 20}};
+                {sl.a.vz, RTM_BX, tz + 20}, {A1.vz, RTM_BX, tz + 20}, {sl.b.vz, RTM_BX, tz + 20}, {B1.vz, RTM_BX, tz + 20},
+                {sl.a.vx, RTM_STAGE_W, ss->bz_pres_recon}, {sl.a.vz, RTM_BX, phr}};
             for (int t = 0; t < RTM_TMAP_COUNT; t++) {
                 CUtensorMap cm;
                 int rc = encode_field_map(&cm, m[t].f, sh.pitch, sh.Z, m[t].w, m[t].h);
@@ -1162,7 +1169,7 @@ static int persistent_pass(rtm_session *ss, BatchRun &br, int dir, int nsteps, b
     CK(cudaMemsetAsync(ss->d_done, 0, 4 * sizeof(unsigned) * ss->B, st));
     cudaEvent_t e;
     timing_begin(ss, dir == 0 ? "pass_fwd" : "pass_bwd", 7, &e);
-    const bool ok = launch_pass(dir, P, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, st);
+    const bool ok = ss->bz_pres_recon == ss->bz_pres && launch_pass(dir, P, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, st);
     timing_end(ss, e);
     if (!ok) return RTM_OK;
     ss->launches++;
@@ -1368,7 +1375,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             timing_end(ss, e);
             timing_begin(ss, "pres_recon", it, &e);
             a.tiles = ss->d_tiles_pr;
-            pres_step(ss, RTM_WAVE_RECON, ss->bz_pres, a, list_grid(ss, br, a, 3), 0);
+            pres_step(ss, RTM_WAVE_RECON, ss->bz_pres_recon, a, list_grid(ss, br, a, 3), 0);
             timing_end(ss, e);
             timing_begin(ss, "vel_recv", it, &e);
             a.tiles = ss->d_tiles;
@@ -1398,8 +1405,8 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     } else {
         const int pa0 = br.pa, pb0 = br.pb;
         int rc = run_pass(ss, {1, n, br.grid[0], br.grid[1], br.grid[2], br.grid[3], br.ex_nxi, br.ex_nzi,
-                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, form_bits(ss), ss->fused,
-                               ss->tz_step, pa0, pb0}, loop);
+                               a.gather_prec, ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->bz_pres_recon,
+                               form_bits(ss), ss->fused, ss->tz_step, pa0, pb0}, loop);
         if (!rc && ss->fused && ss->o.use_graph) {   // a replayed graph swaps as the captured loop did
             br.pa = pa0 ^ ((s.nt - 1) & 1);
             br.pb = pb0 ^ ((s.nt - 1) & 1);
@@ -1446,17 +1453,17 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
 // the kernel.  Before the first batch of a launch shape, every (height, form) is timed on that
 // batch's own buffers: two untimed and four timed source-pass steps (velocity and pressure)
 // and backward steps (reconstruction and receiver pass) with CUDA events per kernel, no strips
-// saved.  Forward/receiver velocity and reconstruction velocity each keep their fastest pair;
-// the pressure kernels share one height (one tile list), and the forward/receiver and the
-// reconstruction pressure take their faster form at it.  The batch is set up again afterwards,
-// so the trial steps leave nothing behind; heights and forms do not change the results (tested
+// saved.  Forward/receiver velocity, reconstruction velocity and reconstruction pressure each
+// keep their fastest pair; the forward and receiver pressure kernels share one height (one
+// tile list), each taking its faster form at it.  The batch is set up again afterwards, so
+// the trial steps leave nothing behind; heights and forms do not change the results (tested
 // bit for bit).  Choices are kept per process by launch shape and, with
-// RTM_B200_TUNE_CACHE=<file>, in that file ("key vel vel_recon pres forms" lines, forms a
-// bit set of vel, vel_recon, pres, pres_recon) across processes.  The whole-step kernel's tile
+// RTM_B200_TUNE_CACHE=<file>, in that file ("key vel vel_recon pres pres_recon forms" lines,
+// forms a bit set of vel, vel_recon, pres, pres_recon) across processes.  The whole-step kernel's tile
 // height is chosen the same way (tune_step_height).
 namespace {
 std::mutex g_tune_mu;
-std::map<std::string, std::array<int, 4>> g_tune;
+std::map<std::string, std::array<int, 5>> g_tune;
 bool g_tune_loaded = false;
 }  // namespace
 
@@ -1474,7 +1481,7 @@ static std::string tune_key(rtm_session *ss, int k0, int n)
 
 // The whole-step kernel's tile height (16 or 32 rows), timed the same way: source-pass,
 // reconstruction and receiver steps, each kind's fast and general launches together.  The
-// choice is recorded as "key tz tz tz 0".
+// choice is recorded as "key tz tz tz tz 0".
 static int tune_step_height(rtm_session *ss, int k0, int n, const std::string &key, const char *path)
 {
     const int cand[2] = {16, 32};
@@ -1528,10 +1535,10 @@ static int tune_step_height(rtm_session *ss, int k0, int n, const std::string &k
         std::printf("rtm_b200: step tile height for %s: %d (ms per 4 steps: 16 rows %.3f, 32 rows %.3f)\n", key.c_str(),
                     tz, ms[0], ms[1]);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tune[key] = {tz, tz, tz, 0};
+    g_tune[key] = {tz, tz, tz, tz, 0};
     if (path && *path)
         if (FILE *f = std::fopen(path, "a")) {
-            std::fprintf(f, "%s %d %d %d 0\n", key.c_str(), tz, tz, tz);
+            std::fprintf(f, "%s %d %d %d %d 0\n", key.c_str(), tz, tz, tz, tz);
             std::fclose(f);
         }
     return RTM_OK;
@@ -1548,9 +1555,9 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             g_tune_loaded = true;
             if (FILE *f = std::fopen(path, "r")) {
                 char k[200];
-                int v[4];
-                while (std::fscanf(f, "%199s %d %d %d %d", k, &v[0], &v[1], &v[2], &v[3]) == 5)
-                    g_tune[k] = {v[0], v[1], v[2], v[3]};
+                int v[5];
+                while (std::fscanf(f, "%199s %d %d %d %d %d", k, &v[0], &v[1], &v[2], &v[3], &v[4]) == 6)
+                    g_tune[k] = {v[0], v[1], v[2], v[3], v[4]};
                 std::fclose(f);
             }
         }
@@ -1563,7 +1570,8 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             ss->bz_vel = it->second[0];
             ss->bz_vel_recon = it->second[1];
             ss->bz_pres = it->second[2];
-            for (int f = 0; f < 4; f++) ss->vec[f] = (it->second[3] >> f) & 1;
+            ss->bz_pres_recon = it->second[3];
+            for (int f = 0; f < 4; f++) ss->vec[f] = (it->second[4] >> f) & 1;
             return RTM_OK;
         }
     }
@@ -1584,7 +1592,7 @@ static int tune_heights(rtm_session *ss, int k0, int n)
     int rc = RTM_OK;
     const int steps = 6, warm = 2;
     for (int c = 0; c < nc && rc == RTM_OK; c++) {
-        ss->bz_vel = ss->bz_vel_recon = ss->bz_pres = cand[c].first;
+        ss->bz_vel = ss->bz_vel_recon = ss->bz_pres = ss->bz_pres_recon = cand[c].first;
         for (bool &v : ss->vec) v = cand[c].second != 0;
         BatchRun br;
         if ((rc = batch_setup(ss, k0, n, br))) break;
@@ -1598,7 +1606,8 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             rec(0, 0); a.tiles = ss->d_tiles; vel_step(ss, RTM_WAVE_FWD, ss->bz_vel, a, br.ntiles); rec(0, 1);
             rec(1, 0); a.tiles = ss->d_tiles_p; pres_step(ss, RTM_WAVE_FWD, ss->bz_pres, a, br.ntiles_p, 0); rec(1, 1);
             rec(2, 0); a.tiles = ss->d_tiles_r; vel_step(ss, RTM_WAVE_RECON, ss->bz_vel_recon, a, br.ntiles_r); rec(2, 1);
-            rec(3, 0); a.tiles = ss->d_tiles_pr; pres_step(ss, RTM_WAVE_RECON, ss->bz_pres, a, br.ntiles_pr, 0); rec(3, 1);
+            rec(3, 0); a.tiles = ss->d_tiles_pr; pres_step(ss, RTM_WAVE_RECON, ss->bz_pres_recon, a, br.ntiles_pr, 0);
+            rec(3, 1);
             rec(4, 0); a.tiles = ss->d_tiles; vel_step(ss, RTM_WAVE_RECEIVER, ss->bz_vel, a, br.ntiles); rec(4, 1);
             rec(5, 0); a.tiles = ss->d_tiles_p; pres_step(ss, RTM_WAVE_RECEIVER, ss->bz_pres, a, br.ntiles_p, 0); rec(5, 1);
         }
@@ -1619,8 +1628,8 @@ static int tune_heights(rtm_session *ss, int k0, int n)
             for (auto &e : b) cudaEventDestroy(e);
     if (rc) return rc;
     if ((rc = check_kernel_flag(ss))) return rc;
-    // velocity families: the fastest (height, form) each; pressure families share a height,
-    // each taking its faster form at that height
+    // the fastest (height, form) of each family, the forward and receiver kernels of a field
+    // together (they share a tile list and a form)
     auto argmin = [&](auto cost) {
         int bi = 0;
         for (int c = 1; c < nc; c++)
@@ -1629,30 +1638,21 @@ static int tune_heights(rtm_session *ss, int k0, int n)
     };
     const int cv = argmin([&](int c) { return ms[c][0] + ms[c][4]; });
     const int cr = argmin([&](int c) { return ms[c][2]; });
-    int best_bz = 0, fp = 0, fpr = 0;
-    double best = 1e300;
-    for (int bz : {8, 16, 32}) {
-        double pf = 1e300, pr = 1e300;
-        int f1 = 0, f2 = 0;
-        for (int c = 0; c < nc; c++)
-            if (cand[c].first == bz) {
-                if (ms[c][1] + ms[c][5] < pf) pf = ms[c][1] + ms[c][5], f1 = cand[c].second;
-                if (ms[c][3] < pr) pr = ms[c][3], f2 = cand[c].second;
-            }
-        if (pf + pr < best) best = pf + pr, best_bz = bz, fp = f1, fpr = f2;
-    }
+    const int cp = argmin([&](int c) { return ms[c][1] + ms[c][5]; });
+    const int cpr = argmin([&](int c) { return ms[c][3]; });
     ss->bz_vel = cand[cv].first;
     ss->bz_vel_recon = cand[cr].first;
-    ss->bz_pres = best_bz;
+    ss->bz_pres = cand[cp].first;
+    ss->bz_pres_recon = cand[cpr].first;
     ss->vec[0] = cand[cv].second;
     ss->vec[1] = cand[cr].second;
-    ss->vec[2] = fp;
-    ss->vec[3] = fpr;
-    const std::array<int, 4> pick = {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, form_bits(ss)};
+    ss->vec[2] = cand[cp].second;
+    ss->vec[3] = cand[cpr].second;
+    const std::array<int, 5> pick = {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->bz_pres_recon, form_bits(ss)};
     if (ss->o.verbose) {
-        std::printf("rtm_b200: tiles for %s: vel %d%s, vel_recon %d%s, pres %d%s/%s (ms per 4 steps:", key.c_str(),
-                    pick[0], ss->vec[0] ? "v" : "s", pick[1], ss->vec[1] ? "v" : "s", pick[2], ss->vec[2] ? "v" : "s",
-                    ss->vec[3] ? "v" : "s");
+        std::printf("rtm_b200: tiles for %s: vel %d%s, vel_recon %d%s, pres %d%s, pres_recon %d%s (ms per 4 steps:",
+                    key.c_str(), pick[0], ss->vec[0] ? "v" : "s", pick[1], ss->vec[1] ? "v" : "s", pick[2],
+                    ss->vec[2] ? "v" : "s", pick[3], ss->vec[3] ? "v" : "s");
         for (int c = 0; c < nc; c++)
             for (int k = 0; k < 6; k++)
                 std::printf(" %s@%d%s=%.3f", names[k], cand[c].first, cand[c].second ? "v" : "s", ms[c][k]);
@@ -1662,7 +1662,7 @@ static int tune_heights(rtm_session *ss, int k0, int n)
     g_tune[key] = pick;
     if (path && *path)
         if (FILE *f = std::fopen(path, "a")) {
-            std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), pick[0], pick[1], pick[2], pick[3]);
+            std::fprintf(f, "%s %d %d %d %d %d\n", key.c_str(), pick[0], pick[1], pick[2], pick[3], pick[4]);
             std::fclose(f);
         }
     return RTM_OK;
@@ -1687,15 +1687,27 @@ static int run_batch(rtm_session *ss, int k0, int n)
 
 int session_batch_size(rtm_session *ss) { return ss ? ss->B : 0; }
 
-// Choose the kernel configuration of the batch shape of shots [k0, k0+n) now (the tuner's
-// trial steps), so that a timed run does not include them.
+// Shots in the next launch of a run over `remaining` shots: the run is split into
+// ceil(remaining / B) launches of equal size (to within one shot), so that no launch is a
+// small remainder that leaves most of the SMs idle for a whole pass (256 shots with room for
+// 246: two launches of 128, not 246 and 10).
+int session_wave_size(const rtm_session *ss, int remaining)
+{
+    const int waves = (remaining + ss->B - 1) / ss->B;
+    return (remaining + waves - 1) / waves;
+}
+
+// Choose the kernel configuration of every launch shape of a run over shots [k0, k0+n) now
+// (the tuner's trial steps), so that a timed run does not include them.
 int session_prepare(rtm_session *ss, int k0, int n)
 {
-    if (!ss || k0 < 0 || n < 1 || n > ss->B || k0 + n > (int)ss->shots.size())
-        return fail(RTM_ERR_ARG, "bad shot range");
+    if (!ss || k0 < 0 || n < 1 || k0 + n > (int)ss->shots.size()) return fail(RTM_ERR_ARG, "bad shot range");
     CK(cudaSetDevice(ss->dev));
-    int rc = tune_heights(ss, k0, n);
-    if (rc) return rc;
+    for (int b0 = k0; b0 < k0 + n;) {
+        const int m = session_wave_size(ss, k0 + n - b0);
+        if (int rc = tune_heights(ss, b0, m)) return rc;
+        b0 += m;
+    }
     CK(cudaStreamSynchronize(ss->stream));
     return RTM_OK;
 }
@@ -1811,8 +1823,8 @@ int rtm_session_run(rtm_session *ss, rtm_stats *stats)
     auto t0 = std::chrono::steady_clock::now();
     int nb = 0;
     double cells = 0;
-    for (int k0 = 0; k0 < (int)ss->shots.size(); k0 += ss->B) {
-        int n = std::min(ss->B, (int)ss->shots.size() - k0);
+    for (int k0 = 0; k0 < (int)ss->shots.size();) {
+        const int n = session_wave_size(ss, (int)ss->shots.size() - k0);
         int rc = run_batch(ss, k0, n);
         if (rc) return rc;
         nb++;
@@ -1822,6 +1834,7 @@ int rtm_session_run(rtm_session *ss, rtm_stats *stats)
         }
         if (ss->o.verbose)
             std::printf("rtm_b200: batch of %d shots done (%d/%zu)\n", n, k0 + n, ss->shots.size());
+        k0 += n;
     }
     auto t1 = std::chrono::steady_clock::now();
     if (stats) {
@@ -1844,8 +1857,8 @@ int rtm_session_run_range(rtm_session *ss, int k0, int n, rtm_stats *stats)
     auto t0 = std::chrono::steady_clock::now();
     int nb = 0;
     double cells = 0;
-    for (int b0 = k0; b0 < k0 + n; b0 += ss->B) {
-        int m = std::min(ss->B, k0 + n - b0);
+    for (int b0 = k0; b0 < k0 + n;) {
+        const int m = session_wave_size(ss, k0 + n - b0);
         int rc = run_batch(ss, b0, m);
         if (rc) return rc;
         nb++;
@@ -1853,6 +1866,7 @@ int rtm_session_run_range(rtm_session *ss, int k0, int n, rtm_stats *stats)
             const ShotState &sh = ss->shots[b0 + j];
             cells += (double)ss->s.nt * (2.0 * sh.X * sh.Z + (double)sh.nxi * sh.nzi);
         }
+        b0 += m;
     }
     if (stats) {
         stats->seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1869,10 +1883,11 @@ int rtm_session_model(rtm_session *ss)
     if (!ss) return fail(RTM_ERR_ARG, "null session");
     if (ss->s.mode != 0) return fail(RTM_ERR_ARG, "modelling needs a mode-0 session");
     CK(cudaSetDevice(ss->dev));
-    for (int k0 = 0; k0 < (int)ss->shots.size(); k0 += ss->B) {
-        int n = std::min(ss->B, (int)ss->shots.size() - k0);
+    for (int k0 = 0; k0 < (int)ss->shots.size();) {
+        const int n = session_wave_size(ss, (int)ss->shots.size() - k0);
         int rc = model_range(ss, k0, n);
         if (rc) return rc;
+        k0 += n;
     }
     return RTM_OK;
 }
@@ -1916,12 +1931,13 @@ int rtm_session_prepare(rtm_session *ss, int k0, int n) { return session_prepare
 
 int rtm_session_batch_size(rtm_session *ss) { return session_batch_size(ss); }
 
-int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres)
+int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres, int *bz_pres_recon)
 {
     if (!ss) return fail(RTM_ERR_ARG, "null session");
     if (bz_vel) *bz_vel = ss->fused ? ss->tz_step : ss->bz_vel;
     if (bz_vel_recon) *bz_vel_recon = ss->fused ? ss->tz_step : ss->bz_vel_recon;
     if (bz_pres) *bz_pres = ss->fused ? ss->tz_step : ss->bz_pres;
+    if (bz_pres_recon) *bz_pres_recon = ss->fused ? ss->tz_step : ss->bz_pres_recon;
     return RTM_OK;
 }
 

@@ -257,8 +257,10 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
     if (threadIdx.x == 0) {   // vx rows z0 .. z0+BZ-1 (columns x0-12 ..), vz rows z0-10 .. z0+BZ+11
         if (use == 0) mbar_init(&s_bar);   // a persistent block keeps it between its tiles
         mbar_expect(&s_bar, (XH * WW + ZH * BX) * sizeof(float));
-        tma_box(svx, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VX : RTM_TMAP_A_VX), x0 - 12, z0, &s_bar);
-        tma_box(svz, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VZ : RTM_TMAP_A_VZ), x0, z0 - 10, &s_bar);
+        const int mvx = MODE == 2 ? RTM_TMAP_B_VX : MODE == 3 ? RTM_TMAP_A_VX_RECON : RTM_TMAP_A_VX;
+        const int mvz = MODE == 2 ? RTM_TMAP_B_VZ : MODE == 3 ? RTM_TMAP_A_VZ_RECON : RTM_TMAP_A_VZ;
+        tma_box(svx, tmap_of(S, mvx), x0 - 12, z0, &s_bar);
+        tma_box(svz, tmap_of(S, mvz), x0, z0 - 10, &s_bar);
     }
     if (a.prefetch) {   // the tile's kappa and p rows (split fields, imaging operands) into L2
         const int z1 = min(z0 + BZ, Z);

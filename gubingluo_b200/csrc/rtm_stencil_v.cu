@@ -170,8 +170,10 @@ __global__ void __launch_bounds__(32 * BZ / U, min_blocks(32 * BZ / U, MODE == 2
     if (threadIdx.x == 0) {
         mbar_init(&s_bar);
         mbar_expect(&s_bar, (XH * WW + ZH * BX) * sizeof(float));
-        tma_box(svx, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VX : RTM_TMAP_A_VX), x0 - 12, z0, &s_bar);
-        tma_box(svz, tmap_of(S, MODE == 2 ? RTM_TMAP_B_VZ : RTM_TMAP_A_VZ), x0, z0 - 10, &s_bar);
+        const int mvx = MODE == 2 ? RTM_TMAP_B_VX : MODE == 3 ? RTM_TMAP_A_VX_RECON : RTM_TMAP_A_VX;
+        const int mvz = MODE == 2 ? RTM_TMAP_B_VZ : MODE == 3 ? RTM_TMAP_A_VZ_RECON : RTM_TMAP_A_VZ;
+        tma_box(svx, tmap_of(S, mvx), x0 - 12, z0, &s_bar);
+        tma_box(svz, tmap_of(S, mvz), x0, z0 - 10, &s_bar);
     }
     for (int i = threadIdx.x; i < 100; i += blockDim.x) s_tab[i] = a.coef[i];
     for (int i = threadIdx.x; i < BZ; i += blockDim.x) {

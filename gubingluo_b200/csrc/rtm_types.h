@@ -125,14 +125,17 @@ enum RtmAccum { RTM_ACC_FP32 = 0, RTM_ACC_FP64 = 1, RTM_ACC_KAHAN = 2 };
 // stencil kernel loads (velocity: p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139;
 // pressure: vx rows z0 .. z0+BZ-1 with the same columns, vz rows z0-10 .. z0+BZ+11,
 // columns x0 .. x0+127).
-// (A_P_RECON: the source pressure again, in the boxes of the reconstruction's own tile height)
+// (A_P_RECON: the source pressure again, in the boxes of the velocity reconstruction's own tile
+// height; A_VX_RECON / A_VZ_RECON: the source velocities in the boxes of the pressure
+// reconstruction's own tile height)
 // (whole-step kernel, per wavefield (A, B) and buffer (0, 1): STEP_*: p in the box of rows
 // z0-19 .. z0+TZ+18, columns x0-24 .. x0+151; STEPVX_*: vx, rows z0 .. z0+TZ-1, columns
 // x0-12 .. x0+139; STEPVZ_*: vz, rows z0-10 .. z0+TZ+9, columns x0 .. x0+127)
 enum RtmTmap { RTM_TMAP_A_P = 0, RTM_TMAP_A_VX, RTM_TMAP_A_VZ, RTM_TMAP_B_P, RTM_TMAP_B_VX, RTM_TMAP_B_VZ,
                RTM_TMAP_A_P_RECON, RTM_TMAP_STEP_A0, RTM_TMAP_STEP_A1, RTM_TMAP_STEP_B0, RTM_TMAP_STEP_B1,
                RTM_TMAP_STEPVX_A0, RTM_TMAP_STEPVX_A1, RTM_TMAP_STEPVX_B0, RTM_TMAP_STEPVX_B1,
-               RTM_TMAP_STEPVZ_A0, RTM_TMAP_STEPVZ_A1, RTM_TMAP_STEPVZ_B0, RTM_TMAP_STEPVZ_B1, RTM_TMAP_COUNT };
+               RTM_TMAP_STEPVZ_A0, RTM_TMAP_STEPVZ_A1, RTM_TMAP_STEPVZ_B0, RTM_TMAP_STEPVZ_B1,
+               RTM_TMAP_A_VX_RECON, RTM_TMAP_A_VZ_RECON, RTM_TMAP_COUNT };
 #define RTM_TMAP_BYTES 128
 
 // One block's work: the tile of `shot` whose top-left cell is (x0, z0).  x0 is a multiple of

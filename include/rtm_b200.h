@@ -187,7 +187,8 @@ int rtm_session_set_gather_raw(rtm_session *ss, int k, const float *seisobs, int
 /* Migrate every shot of the session; images accumulate on the device.  Inputs must be
  * resident (rtm_session_set_gather for mode 1). */
 int rtm_session_run(rtm_session *ss, rtm_stats *stats);
-/* Migrate shots [k0, k0+n) only (batches of the session's batch size); images accumulate. */
+/* Migrate shots [k0, k0+n) only; images accumulate.  A run (this or rtm_session_run) goes
+ * in ceil(n / batch size) launches of equal size, to within one shot. */
 int rtm_session_run_range(rtm_session *ss, int k0, int n, rtm_stats *stats);
 /* Mode 0 only: model every shot's gather (forward pass with receiver sampling; no
  * migration), the reference's modelling pass (rtm_model.cu:266-290). */
@@ -237,14 +238,16 @@ unsigned long long rtm_session_config_hash(rtm_session *ss);
  * number of guard bands of the session (0 when the mode is off). */
 int rtm_session_guard_count(rtm_session *ss);
 /* Rows per stencil tile in use: forward and receiver velocity, reconstruction velocity,
- * pressure (with the whole-step kernel, its tile height in all three).  Chosen, with the kernel
- * form of each family, per launch shape by timing 8-, 16- and 32-row tiles in both forms before
- * the first batch of that shape (RTM_B200_TUNE=0, or RTM_B200_BZ_VEL / _VEL_RECON / _PRES set,
- * turns that off; RTM_B200_KERNELS=scalar|vector fixes the form; choices persist across
- * processes in RTM_B200_TUNE_CACHE=<file>).  Any pointer may be NULL. */
-int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres);
-/* Run the tuner now for the batch shape of shots [k0, k0+n) (no migration), so that a later
- * timed rtm_session_run_range of that shape does not include its trial steps. */
+ * forward and receiver pressure, reconstruction pressure (with the whole-step kernel, its tile
+ * height in all four).  Chosen, with the kernel form of each family, per launch shape by timing
+ * 8-, 16- and 32-row tiles in both forms before the first batch of that shape
+ * (RTM_B200_TUNE=0, or RTM_B200_BZ_VEL / _VEL_RECON / _PRES / _PRES_RECON set, turns that off;
+ * RTM_B200_BZ_PRES sets both pressure heights unless _PRES_RECON is given;
+ * RTM_B200_KERNELS=scalar|vector fixes the form; choices persist across processes in
+ * RTM_B200_TUNE_CACHE=<file>).  Any pointer may be NULL. */
+int rtm_session_tile_heights(rtm_session *ss, int *bz_vel, int *bz_vel_recon, int *bz_pres, int *bz_pres_recon);
+/* Run the tuner now for every launch shape of rtm_session_run_range(ss, k0, n) (no
+ * migration), so that the timed run does not include its trial steps. */
 int rtm_session_prepare(rtm_session *ss, int k0, int n);
 /* Shots per launch (batch slots) of the session: options.batch, or as many as device memory
  * holds. */

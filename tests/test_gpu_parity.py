@@ -453,15 +453,18 @@ def test_packed_strips_and_gathers_survive_subnormal_values(rtmlib, prec):
 @pytest.mark.gpu
 def test_tile_heights_do_not_change_the_bits(rtmlib, monkeypatch):
     """Tile heights (and with them the row groups and the interior/general split of the tiles)
-    only reorganise the work: gathers and images are bit-identical for every choice."""
+    only reorganise the work: gathers and images are bit-identical for every choice, the
+    reconstruction pressure's height different from the other pressure kernels' too."""
     G = rtmlib
     c = GENERAL[2]
     v, rho = _random_model(c["nz"], c["nx"], 7)
     shots = list(range(1, c["nshot"] + 1))
     s = cfg_from(G, _survey(c, 0))
     runs = []
-    for vel, recon, pres in ((None, None, None), ("16", "32", "32"), ("8", "8", "8"), ("64", "16", "64")):
-        for k, val in (("RTM_B200_BZ_VEL", vel), ("RTM_B200_BZ_VEL_RECON", recon), ("RTM_B200_BZ_PRES", pres)):
+    for vel, recon, pres, pres_recon in ((None, None, None, None), ("16", "32", "32", "8"), ("8", "8", "8", "32"),
+                                         ("64", "16", "64", "16")):
+        for k, val in (("RTM_B200_BZ_VEL", vel), ("RTM_B200_BZ_VEL_RECON", recon), ("RTM_B200_BZ_PRES", pres),
+                       ("RTM_B200_BZ_PRES_RECON", pres_recon)):
             if val is None:
                 monkeypatch.delenv(k, raising=False)
             else:
@@ -544,7 +547,7 @@ def test_tile_height_tuner(rtmlib, monkeypatch, tmp_path):
     s = cfg_from(G, _survey(c, 0))
     cache = tmp_path / "tune.txt"
     monkeypatch.setenv("RTM_B200_TUNE_CACHE", str(cache))
-    for k in ("RTM_B200_BZ_VEL", "RTM_B200_BZ_VEL_RECON", "RTM_B200_BZ_PRES", "RTM_B200_TUNE"):
+    for k in ("RTM_B200_BZ_VEL", "RTM_B200_BZ_VEL_RECON", "RTM_B200_BZ_PRES", "RTM_B200_BZ_PRES_RECON", "RTM_B200_TUNE"):
         monkeypatch.delenv(k, raising=False)
     with G.Session(s, G.RunOptions(), shots, v, rho) as ss:
         ss.run()
@@ -553,7 +556,8 @@ def test_tile_height_tuner(rtmlib, monkeypatch, tmp_path):
         gathers = [ss.gather(k) for k in range(len(shots))]
     assert set(h.values()) <= {8, 16, 32}
     lines = cache.read_text().split("\n")
-    assert any(ln.split()[1:4] == [str(h["vel"]), str(h["vel_recon"]), str(h["pres"])] for ln in lines if ln), lines
+    want_line = [str(h[k]) for k in ("vel", "vel_recon", "pres", "pres_recon")]
+    assert any(ln.split()[1:5] == want_line for ln in lines if ln), lines
     monkeypatch.setenv("RTM_B200_TUNE", "0")
     want = G.migrate(s, G.RunOptions(), shots, v, rho)
     for k in ("image1", "image2s", "illum"):
