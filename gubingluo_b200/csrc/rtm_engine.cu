@@ -810,9 +810,12 @@ static void shot_tiles(const rtm_session *ss, const ShotState &sh, int j, bool f
     // whole-grid tiles, and the reconstruction's tiles: it writes only the interior and the
     // ten-cell strips around it, x in [npml-10, X-npml+10), z in [npml-10, Z-npml+10).  The
     // reconstruction's tile columns start on a 32-column (128-byte) boundary, so that every
-    // warp's row access covers whole 128-byte lines (the kernels mask the cells outside the
+    // warp's row access covers whole 128-byte lines, unless the 4-column boundary nearest
+    // below the region needs one tile column fewer (the kernels skip the columns outside the
     // region)
-    const int xr0 = (s.npml - RTM_RADIUS) & ~31, xr1 = sh.X - s.npml + RTM_RADIUS;
+    const int xr1 = sh.X - s.npml + RTM_RADIUS, xlo = s.npml - RTM_RADIUS;
+    const int xr0 = (xr1 - (xlo & ~31) + RTM_BX - 1) / RTM_BX <= (xr1 - (xlo & ~3) + RTM_BX - 1) / RTM_BX
+                        ? xlo & ~31 : xlo & ~3;
     const int zr0 = s.npml - RTM_RADIUS, zr1 = sh.Z - s.npml + RTM_RADIUS;
     // velocity tiles: interior when every column lies in [npml, X-npml-1) and every row in
     // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies

@@ -113,9 +113,11 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
             gow[u] = vzp[g0 + u * pitch];
         }
     };
-    if (x < X && z0 + U <= zend) load_group(z0, cir, cov, cow);
+    // the reconstruction leaves every column outside [npml-R, X-npml+R) alone
+    const bool dead = x >= X || (MODE == 3 && (x < npml - R || x >= X - npml + R));
+    if (!dead && z0 + U <= zend) load_group(z0, cir, cov, cow);
     __syncthreads();
-    if (!tile_wait(&s_bar, a.err, use & 1u) || x >= X) return;   // no barrier below
+    if (!tile_wait(&s_bar, a.err, use & 1u) || dead) return;   // no barrier below
 
     const float *col = &sw[tx + 12];   // staged column x: col[r*WW] = p[z0-9+r][x]
     float q[QN];                        // q[k] = p[z-9+k][x] at the current row z
@@ -334,9 +336,11 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
             }
         }
     };
-    if (x < X && z0 + U <= zend) load_group(z0, ckk, cp0, cs1, cs2, cps, cg1, cil);
+    // the reconstruction leaves every column outside [npml-R, X-npml+R) alone
+    const bool dead = x >= X || (MODE == 3 && (x < npml - R || x >= X - npml + R));
+    if (!dead && z0 + U <= zend) load_group(z0, ckk, cp0, cs1, cs2, cps, cg1, cil);
     __syncthreads();
-    if (!tile_wait(&s_bar, a.err, use & 1u) || x >= X) return;
+    if (!tile_wait(&s_bar, a.err, use & 1u) || dead) return;
 
     const float *colx = &svx[tx + 12];   // colx[r*WW] = vx[z0+r][x]
     const float *colz = &svz[tx];        // colz[r*BX] = vz[z0-10+r][x]

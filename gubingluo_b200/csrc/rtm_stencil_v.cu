@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(32 * BZ / U, min_blocks(32 * BZ / U, 80)) k_ve
     const int x = x0 + 4 * g, zr = z0 + U * r;
     float *__restrict__ vxp = W.vx;
     float *__restrict__ vzp = W.vz;
-    const bool live = x < X && zr < Z;
+    // (the reconstruction leaves every column outside [npml-R, X-npml+R) alone)
+    const bool live = x < X && zr < Z && (MODE != 3 || (x + 4 > npml - R && x < X - npml + R));
     // operands of the thread's cells, loaded while the tile is staged (x < X keeps the four
     // columns inside the row pitch, a multiple of 32 >= X)
     float4 ir[U], ov[U], ow[U];
@@ -189,7 +190,8 @@ __global__ void __launch_bounds__(32 * BZ / U, min_blocks(32 * BZ / U, MODE == 2
     const float *__restrict__ psp = S.a.p;
     ACC *__restrict__ g1p = (ACC *)S.g1;
     ACC *__restrict__ ilp = (ACC *)S.illum;
-    const bool live = x < X && zr < Z;
+    // (the reconstruction leaves every column outside [npml-R, X-npml+R) alone)
+    const bool live = x < X && zr < Z && (MODE != 3 || (x + 4 > npml - R && x < X - npml + R));
     const int zend = min(z0 + BZ, Z);
     const bool edge_tile = MODE != 3 && (x0 < R || x0 + BX > X - R || z0 < R || zend > Z - R);
     // columns of the x PML band / of the image interior among the thread's four
