@@ -48,9 +48,18 @@ MODEL_TEXT = {1: "four flat layers and a dipping 3500 m/s wedge",
               5: "gradient + salt body + water layer"}
 
 
+# per-shot image accumulation (rtm_options.accum_fp64) chosen by the flags, and its description
+ACCUM_TEXT = {0: "FP32", 1: "FP64", 2: "compensated FP32 pair (Kahan)",
+              3: "FP64 totals of 16-step FP32 partial sums"}
+
+
+def accum_mode(args) -> int:
+    return 2 if args.accum_kahan else 3 if args.accum_blocked else 1 if args.accum_fp64 else 0
+
+
 def workload_text(args, s, shots, meta):
     """The workload of a --config run (configuration 2's text is WORKLOAD)."""
-    fp32 = args.strips == "fp32" and args.gathers == "fp32" and not args.accum_fp64 and not args.accum_kahan
+    fp32 = args.strips == "fp32" and args.gathers == "fp32" and accum_mode(args) == 0
     if args.config == 2 and s.nt == 4000 and fp32:
         return WORKLOAD
     X, Z = s.nx + 2 * s.npml, s.nz + 2 * s.npml
@@ -62,8 +71,7 @@ def workload_text(args, s, shots, meta):
         spread = "full spread" if s.layout == 2 else f"layout {s.layout}"
     form = "FP32 stencil/strips/gathers/accumulators" if fp32 else (
         f"FP32 stencil, {args.strips} strips, {args.gathers} gathers, "
-        f"{'compensated FP32 pair (Kahan)' if args.accum_kahan else 'FP64' if args.accum_fp64 else 'FP32'} "
-        f"accumulators")
+        f"{ACCUM_TEXT[accum_mode(args)]} accumulators")
     return (f"config {args.config}: {s.nx}x{s.nz} grid (X x Z = {X} x {Z} padded), dx=dz={s.dx:g} m, "
             f"{s.npml}-cell PML, nt={s.nt}, dt={s.dt * 1e3:g} ms, {s.fdom:g} Hz Ricker, {len(shots)} shots "
             f"({spread}), source-illumination-normalised imaging, {form}")
@@ -90,6 +98,8 @@ def parse():
     ap.add_argument("--accum-fp64", action="store_true")
     ap.add_argument("--accum-kahan", action="store_true",
                     help="per-shot accumulation in compensated fp32 pairs, stacked in fp64")
+    ap.add_argument("--accum-blocked", action="store_true",
+                    help="per-shot accumulation in fp64 totals of 16-step fp32 partial sums, stacked in fp64")
     ap.add_argument("--cpu-sample-steps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -105,6 +115,9 @@ def parse():
                     help="plain per-shot arm: every k-th shot of the 256 (default 8: 32 shots)")
     ap.add_argument("--headline-arms", default="batched,plain,graph",
                     help="which arms of the configuration-4 comparison to run (comma-separated)")
+    ap.add_argument("--headline-accum", type=int, default=3, choices=[1, 2, 3],
+                    help="image accumulation of the batched arm (rtm_options.accum_fp64; default 3: fp64 "
+                         "totals of 16-step fp32 partial sums)")
     return ap.parse_args()
 
 
@@ -264,7 +277,7 @@ def run_ours(args, rank, world, local_rank):
     uniq = mine[: min(len(mine), need)]
     step_shots = [uniq[(i * B + j) % len(uniq)] for i in range(K + W) for j in range(B)]
     opts = G.RunOptions(device=local_rank, strip_precision=args.strips, gather_precision=args.gathers,
-                        accum_fp64=2 if args.accum_kahan else int(args.accum_fp64), batch=args.batch or B)
+                        accum_fp64=accum_mode(args), batch=args.batch or B)
     # ---- synthetic data: model this rank's gathers in the true model (untimed setup)
     t0 = time.time()
     s_model = G.SurveyConfig(**{**s.__dict__, "mode": 0})
@@ -288,7 +301,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ss.stream())
     ptrs = ss.image_ptrs()
     npix = s.nx * s.nz
-    typestr = "<f8" if (args.accum_fp64 or args.accum_kahan) else "<f4"
+    typestr = "<f8" if accum_mode(args) else "<f4"
     img_views = [torch.as_tensor(_CudaArray(ptrs[k], npix, typestr), device=f"cuda:{local_rank}")
                  for k in ("image1", "image2s", "illum")] if dist else []
 
@@ -379,7 +392,9 @@ def run_ours(args, rank, world, local_rank):
     ss.close()
 
     # ---- roofline of the dominant kernel
-    accum_bytes = 8 if (args.accum_fp64 or args.accum_kahan) else 4
+    # bytes per accumulator cell that the receiver pressure kernel reads and writes (the blocked
+    # form's kernel updates fp32 partials; its flush is a launch of its own)
+    accum_bytes = 8 if accum_mode(args) in (1, 2) else 4
     sampled = {k: v for k, v in kern.items() if v[0] > 0}
     dom = max(sampled, key=lambda k: sampled[k][0])
     launch_ms = sampled[dom][0]
@@ -479,7 +494,7 @@ def run_headline(args, local_rank):
     arms = set(args.headline_arms.split(","))
     empty = {"shots": 0, "shots_per_s": None, "gcell_updates_per_s": None}
     batched = timed(G.RunOptions(device=local_rank, strip_precision="fp16", gather_precision="fp16",
-                                 accum_fp64=True), shots, 4) if "batched" in arms else empty
+                                 accum_fp64=args.headline_accum), shots, 4) if "batched" in arms else empty
     sample = shots[args.headline_sample // 2::args.headline_sample]
     # plain FP32, one shot per launch: direct launches, and each pass replayed as a CUDA graph
     # (rounded grids, so that shots of nearby windows share a graph; every shot here has its
@@ -494,8 +509,9 @@ def run_headline(args, local_rank):
                          "apertures drawn from %d-%d columns (layout-1 windows cut at the model's edges), "
                          "gradient + random-field model, gathers modelled by this library before timing"
                          % (s.nt, min(ap.values()), max(ap.values()))),
-            "batched_mixed": {**batched, "form": "fp16 strips + fp16 gathers + fp64 images, all 256 shots, "
-                                                   "as many per launch as fit"},
+            "batched_mixed": {**batched, "form": "fp16 strips + fp16 gathers + %s images, all 256 shots, "
+                                                   "in equal launches of as many as fit"
+                                                   % ACCUM_TEXT[args.headline_accum]},
             "plain_fp32_per_shot": {**plain, "form": "fp32, one shot per launch, direct launches",
                                     "sample": f"every {args.headline_sample}th shot ({len(sample)} shots)"},
             "plain_fp32_per_shot_graph": {**plain_graph, "form": "fp32, one shot per launch, each pass replayed as "
@@ -726,7 +742,8 @@ def main():
     headline = None
     if world == 1 and not args.no_headline and args.config == 2 and not args.profile_only:
         headline = run_headline(args, local_rank)
-    acc_txt = "kahan-f32 images" if args.accum_kahan else "f64 images" if args.accum_fp64 else "f32 images"
+    acc_txt = {0: "f32 images", 1: "f64 images", 2: "kahan-f32 images", 3: "f64 images of f32 16-step partials"}[
+        accum_mode(args)]
     dtype = "f32" if acc_txt == "f32 images" and args.strips == "fp32" and args.gathers == "fp32" else \
         f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {acc_txt}"
     ws_gb = r["shots_per_launch"] * 12 * r["X"] * r["Z"] * 4 / 1e9

@@ -100,6 +100,7 @@ struct Slot {
     void *strips = nullptr;
     float *strip_scale = nullptr, *strip_stage = nullptr;
     void *g1 = nullptr, *illum = nullptr;
+    double *g1t = nullptr, *illt = nullptr;               // fp64 totals of the blocked accumulation
     void *gx[4] = {nullptr, nullptr, nullptr, nullptr};   // other imaging conditions (g2, g3, g3t, g4)
     float *ps_pre = nullptr, *p_pre = nullptr;           // pressures before the current backward step
 };
@@ -359,6 +360,13 @@ static int upload_model(rtm_session *ss, const std::vector<float> &vp2, const st
     return RTM_OK;
 }
 
+// Bytes per cell of the per-shot accumulators g1 and illum that the imaging kernels update every
+// step: fp32, fp64, a compensated fp32 pair, or the fp32 partial sums of the blocked form.
+static int acc_bytes(const rtm_options &o)
+{
+    return o.accum_fp64 == RTM_ACC_FP64 || o.accum_fp64 == RTM_ACC_KAHAN ? 8 : 4;
+}
+
 static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, int Z, int strip_len, int nxi, int nzi,
                          bool fused)
 {
@@ -369,7 +377,8 @@ static size_t slot_bytes(const rtm_survey &s, const rtm_options &o, int pitch, i
         b += (size_t)s.nt * 4 * sizeof(float) + 256;
         b += (size_t)kRing * strip_len * sizeof(float) + 256;
     }
-    b += 2 * ((size_t)pitch * Z * (o.accum_fp64 ? 8 : 4) + 256);   // g1, illum on the padded grid
+    b += 2 * ((size_t)pitch * Z * acc_bytes(o) + 256);   // g1, illum on the padded grid
+    if (o.accum_fp64 == RTM_ACC_FP64_BLOCKED) b += 2 * ((size_t)pitch * Z * 8 + 256);   // their fp64 totals
     if (o.extra_images) b += 4 * ((size_t)pitch * Z * (o.accum_fp64 ? 8 : 4) + 256) + 2 * field;
     (void)nxi;
     (void)nzi;
@@ -493,7 +502,7 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             for (bool &v : ss->vec) v = false;
         }
         if (o.extra_images < 0 || o.extra_images > 2) return fail(RTM_ERR_ARG, "extra_images must be 0, 1 or 2");
-        if (o.accum_fp64 < 0 || o.accum_fp64 > 2) return fail(RTM_ERR_ARG, "accum_fp64 must be 0, 1 or 2");
+        if (o.accum_fp64 < 0 || o.accum_fp64 > 3) return fail(RTM_ERR_ARG, "accum_fp64 must be 0, 1, 2 or 3");
         for (int bz : {ss->bz_vel, ss->bz_vel_recon, ss->bz_pres, ss->bz_pres_recon})
             if (bz != 8 && bz != 16 && bz != 32 && bz != 64) return fail(RTM_ERR_ARG, "tile heights must be 8, 16, 32 or 64");
     }
@@ -627,10 +636,15 @@ static int open_session(rtm_session *ss, const float *vp, const float *rho, cons
             sl.strip_scale = (float *)ss->arena.take((size_t)s.nt * 4 * 4);
             sl.strip_stage = (float *)ss->arena.take((size_t)kRing * big.strip_len * 4);
         }
-        size_t ib = (size_t)big.pitch * big.Z * (o.accum_fp64 ? 8 : 4);
-        sl.g1 = ss->arena.take(ib);
-        sl.illum = ss->arena.take(ib);
+        const size_t cells = (size_t)big.pitch * big.Z, ib = cells * (o.accum_fp64 ? 8 : 4);
+        sl.g1 = ss->arena.take(cells * acc_bytes(o));
+        sl.illum = ss->arena.take(cells * acc_bytes(o));
         if (!sl.strips || !sl.g1 || !sl.illum) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
+        if (o.accum_fp64 == RTM_ACC_FP64_BLOCKED) {
+            sl.g1t = (double *)ss->arena.take(cells * 8);
+            sl.illt = (double *)ss->arena.take(cells * 8);
+            if (!sl.g1t || !sl.illt) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
+        }
         if (o.extra_images) {
             for (void *&g : sl.gx)
                 if (!(g = ss->arena.take(ib))) return fail(RTM_ERR_NOMEM, "device arena exhausted (slots)");
@@ -906,6 +920,7 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         d.gather = s.mode == 0 ? sh.gather_raw : sh.gather32;
         d.gather_scale = nullptr;
         d.g1 = sl.g1; d.illum = sl.illum;
+        d.g1t = sl.g1t; d.illt = sl.illt;
         for (int k = 0; k < 4; k++) d.gx[k] = sl.gx[k];
         d.ps_pre = sl.ps_pre; d.p_pre = sl.p_pre;
         d.vp2_b = sh.mb.vp2;
@@ -942,9 +957,13 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
         float *f[16] = {sl.a.p,  sl.a.vx, sl.a.vz,  sl.a.sx,  sl.a.sz, sl.b.p,   sl.b.vx,  sl.b.vz,
                         sl.b.sx, sl.b.sz, sl.a2.p, sl.a2.vx, sl.a2.vz, sl.b2.p, sl.b2.vx, sl.b2.vz};
         for (int i = 0; i < (ss->fused ? 16 : 10); i++) CK(cudaMemsetAsync(f[i], 0, fb, st));
-        size_t ib = (size_t)sh.pitch * sh.Z * (o.accum_fp64 ? 8 : 4);
-        CK(cudaMemsetAsync(sl.g1, 0, ib, st));
-        CK(cudaMemsetAsync(sl.illum, 0, ib, st));
+        const size_t cells = (size_t)sh.pitch * sh.Z, ib = cells * (o.accum_fp64 ? 8 : 4);
+        CK(cudaMemsetAsync(sl.g1, 0, cells * acc_bytes(o), st));
+        CK(cudaMemsetAsync(sl.illum, 0, cells * acc_bytes(o), st));
+        if (sl.g1t) {
+            CK(cudaMemsetAsync(sl.g1t, 0, cells * 8, st));
+            CK(cudaMemsetAsync(sl.illt, 0, cells * 8, st));
+        }
         if (o.extra_images)
             for (void *g : sl.gx) CK(cudaMemsetAsync(g, 0, ib, st));
     }
@@ -1020,7 +1039,8 @@ static int batch_setup(rtm_session *ss, int k0, int n, BatchRun &br)
     a.dtz = s.dt / s.dz;
     a.strip_prec = o.strip_precision;
     a.gather_prec = RTM_PREC_FP32;
-    a.accum_fp64 = o.accum_fp64;
+    // the stencil kernels image into fp32 partial sums in the blocked form
+    a.accum_fp64 = o.accum_fp64 == RTM_ACC_FP64_BLOCKED ? RTM_ACC_FP32 : o.accum_fp64;
     a.err = ss->d_err;
     {
         // L2 prefetch of the tiles' operand rows: on for batches of 4 shots or more (measured:
@@ -1139,7 +1159,7 @@ static int persistent_pass(rtm_session *ss, BatchRun &br, int dir, int nsteps, b
     const rtm_options &o = ss->o;
     if (!ss->persist || ss->nsnap) return RTM_OK;
     if (dir == 0 && save && o.strip_precision != RTM_PREC_FP32) return RTM_OK;
-    if (dir == 1 && o.extra_images) return RTM_OK;
+    if (dir == 1 && (o.extra_images || o.accum_fp64 == RTM_ACC_FP64_BLOCKED)) return RTM_OK;
     cudaStream_t st = ss->stream;
     PassArgs P{};
     P.a = br.a;
@@ -1337,6 +1357,13 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     unsigned *snap_b = ntsnap ? ss->d_absmax + (size_t)ss->nsnap * ss->B : nullptr;
     if (ntsnap) CK(cudaMemsetAsync(snap_b, 0, sizeof(unsigned) * ss->nsnap * ss->B, st));
     nvtxRangePushA("rtm: backward pass");
+    // blocked accumulation: the partial sums go into the fp64 totals every RTM_ACC_BLOCK steps
+    // and after the last step (it = 0)
+    auto flush_images = [&](int it) {
+        if (o.accum_fp64 != RTM_ACC_FP64_BLOCKED || it % RTM_ACC_BLOCK) return;
+        launch_image_flush(table(ss, br), n, br.ex_nxi, br.ex_nzi, st);
+        ss->launches++;
+    };
     auto loop = [&] {
         for (int it = s.nt - 2; it >= 0; it--) {
             a.it = it;
@@ -1365,6 +1392,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
                 timing_end(ss, e);
                 br.pb ^= 1;
                 ss->launches += 4;
+                flush_images(it);
                 if (o.extra_images) {
                     launch_image_extra(table(ss, br), n, br.ex_nxi, br.ex_nzi, o.extra_images == 2, o.accum_fp64, s.dx,
                                        s.dz, s.dt, st);
@@ -1388,6 +1416,7 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
             launch_pres_tiles(ss, br, RTM_WAVE_RECEIVER, 0);
             timing_end(ss, e);
             ss->launches += 3;
+            flush_images(it);
             if (o.extra_images) {
                 launch_image_extra(ss->d_shots, n, br.ex_nxi, br.ex_nzi, o.extra_images == 2, o.accum_fp64, s.dx, s.dz,
                                    s.dt, st);
@@ -1431,9 +1460,11 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
         ShotState &sh = ss->shots[br.k0 + j];
         int nwin = 50;   // rtm_model.cu:70, :464-465
         while (2 * nwin >= sh.nxi) nwin -= 3;
-        fill_finalize_shot(fin.data() + j * finalize_shot_size(), ss->slots[j].g1, ss->slots[j].illum,
-                           o.extra_images ? ss->slots[j].gx : nullptr, sh.g.nx1, sh.nxi, nwin, sh.pitch, s.npml,
-                           o.accum_fp64);
+        const Slot &sl = ss->slots[j];
+        const bool blocked = o.accum_fp64 == RTM_ACC_FP64_BLOCKED;   // the totals hold every step
+        fill_finalize_shot(fin.data() + j * finalize_shot_size(), blocked ? (void *)sl.g1t : sl.g1,
+                           blocked ? (void *)sl.illt : sl.illum, o.extra_images ? sl.gx : nullptr, sh.g.nx1, sh.nxi,
+                           nwin, sh.pitch, s.npml, blocked ? RTM_ACC_FP64 : o.accum_fp64);
     }
     CK(cudaMemcpyAsync(ss->d_fin, fin.data(), fin.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ss->d_nonfinite, 0x7f, sizeof(int), st));   // 0x7f7f7f7f: none

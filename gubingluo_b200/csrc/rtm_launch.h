@@ -41,4 +41,7 @@ void fill_finalize_shot(void *dst, const void *g1, const void *illum, const void
                         int nwin, int pitch, int npml, int acc);
 void launch_image_extra(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, int parity, int fp64,
                         float dx, float dz, float dt, cudaStream_t s);
+// RTM_ACC_FP64_BLOCKED: every shot's fp32 partial sums g1, illum added into its fp64 totals
+// and cleared, on the image interior (max_nxi x max_nzi: the batch's largest interior).
+void launch_image_flush(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, cudaStream_t s);
 void launch_finalize_extra(const void *fs, int nshots, int nx, int nz, int fp64, void *const img[7], cudaStream_t s);

@@ -101,6 +101,7 @@ struct ShotDev {
     void *gather;                       // [nt][nrec] of the gather precision
     float *gather_scale;                // [nt]
     void *g1, *illum;                   // [Z][pitch] float or double accumulators (interior cells used)
+    double *g1t, *illt;                 // RTM_ACC_FP64_BLOCKED: [Z][pitch] fp64 totals (g1, illum: fp32 partials)
     const void *tmaps;                  // RTM_TMAP_COUNT TMA tensor maps (128 B each) of this shot's slot
     // the other imaging conditions (when enabled): accumulators g2 (decomposition), g3
     // (Poynting angle), g3t (true amplitude), g4 (energy norm), [Z][pitch] float or double;
@@ -118,8 +119,12 @@ struct KahanAcc {
     __host__ __device__ KahanAcc() : s(0.f), c(0.f) {}
     __host__ __device__ KahanAcc(int) : s(0.f), c(0.f) {}
 };
-// Per-shot accumulation of g1 and illum (rtm_options.accum_fp64): fp32, fp64, compensated fp32.
-enum RtmAccum { RTM_ACC_FP32 = 0, RTM_ACC_FP64 = 1, RTM_ACC_KAHAN = 2 };
+// Per-shot accumulation of g1 and illum (rtm_options.accum_fp64): fp32, fp64, compensated fp32,
+// or fp64 totals of fp32 partial sums over RTM_ACC_BLOCK steps (the partials are imaged as the
+// fp32 form does and added into the totals, then cleared, every RTM_ACC_BLOCK steps and after
+// the last one).
+enum RtmAccum { RTM_ACC_FP32 = 0, RTM_ACC_FP64 = 1, RTM_ACC_KAHAN = 2, RTM_ACC_FP64_BLOCKED = 3 };
+#define RTM_ACC_BLOCK 16
 
 // TMA tensor maps of one slot: the staged fields of the two wavefields with the box each
 // stencil kernel loads (velocity: p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139;

@@ -7,8 +7,9 @@ against the CPU oracle (FP32 restatement and FP64 build of the same scheme).
   oracle, and within 1e-4 of the FP64 oracle.
 * Configuration 4 at full length (nt = 5000, 0.8 ms) on its narrowest and widest drawn
   apertures (201 and 801 columns; 281 x 881 and 881 x 881 padded): fp16 boundary strips and
-  gathers with fp64 image accumulation within 1e-3 rel-L2 of the FP64 oracle, bf16 strips
-  and gathers too, plain FP32 within 1e-4.  The drift of the source wavefield reconstructed
+  gathers with fp64 image accumulation (every step, and fp64 totals of 16-step fp32 partial
+  sums) within 1e-3 rel-L2 of the FP64 oracle, bf16 strips and gathers too, plain FP32 within
+  1e-4.  The drift of the source wavefield reconstructed
   from fp16 strips against the one reconstructed from fp32 strips, taken at the end of the
   backward pass (t = 0, where the field is the young source wavelet and smallest), is
   reported and held to 1e-2.
@@ -80,6 +81,7 @@ def test_config4_precision_form_full_length(rtmlib, oracle, which):
     cfg = G.SurveyConfig(**s1)
     forms = {"fp32": G.RunOptions(),
              "fp16": G.RunOptions(strip_precision="fp16", gather_precision="fp16", accum_fp64=True),
+             "fp16 blocked": G.RunOptions(strip_precision="fp16", gather_precision="fp16", accum_fp64=3),
              "bf16": G.RunOptions(strip_precision="bf16", gather_precision="bf16", accum_fp64=True)}
     errs = {}
     for name, opts in forms.items():

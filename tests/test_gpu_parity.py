@@ -198,7 +198,8 @@ def test_batching_is_bitwise_invariant(rtmlib):
 
 
 @pytest.mark.parametrize("strips,gathers,fp64", [("fp16", "fp16", True), ("bf16", "bf16", True),
-                                                 ("fp16", "fp32", False), ("fp32", "fp32", True)])
+                                                 ("fp16", "fp32", False), ("fp32", "fp32", True),
+                                                 ("fp16", "fp16", 3)])
 def test_precision_forms_against_fp64_oracle(rtmlib, oracle, strips, gathers, fp64):
     c = GENERAL[0]
     v, rho = _random_model(c["nz"], c["nx"], 11)
@@ -585,6 +586,38 @@ def test_compensated_fp32_accumulation(rtmlib, monkeypatch):
     ds = G.migrate(s, G.RunOptions(accum_fp64=2), shots, v, rho)
     for k in ("image1", "image2s", "illum"):
         assert np.array_equal(ds["f64"][k], dk["f64"][k]), k
+
+
+@pytest.mark.gpu
+def test_blocked_fp64_accumulation(rtmlib, monkeypatch):
+    """accum_fp64 = 3: the steps image into fp32 partial sums, which a flush adds into fp64
+    totals every 16 steps and after the last (nt - 1 backward steps, not a multiple of 16
+    here): within 1e-6 rel-L2 of fp64 accumulation every step; the same bits from both kernel
+    forms, from graph replays, from one shot per launch, and from the whole-step kernel; the
+    other imaging conditions (their accumulators fp64 as before) within 1e-6 too."""
+    G = rtmlib
+    c = GENERAL[0]
+    assert (c["nt"] - 1) % 16
+    v, rho = _random_model(c["nz"], c["nx"], 17)
+    shots = [1, 2]
+    s = cfg_from(G, _survey(c, 0))
+    d64 = G.migrate(s, G.RunOptions(accum_fp64=1, extra_images=1), shots, v, rho)
+    db = G.migrate(s, G.RunOptions(accum_fp64=3, extra_images=1), shots, v, rho)
+    for k in ("image1", "image2s", "illum"):
+        assert np.abs(d64["f64"][k]).max() > 0
+        assert rel_l2(db["f64"][k], d64["f64"][k]) < 1e-6, (k, rel_l2(db["f64"][k], d64["f64"][k]))
+    for k in ("image3s", "image4s", "image5s"):   # normalised by the (blocked) illumination
+        assert rel_l2(db[k], d64[k]) < 1e-6, (k, rel_l2(db[k], d64[k]))
+    variants = [("scalar", {}, {"RTM_B200_KERNELS": "scalar"}), ("vector", {}, {"RTM_B200_KERNELS": "vector"}),
+                ("graph", {"use_graph": 1}, {}), ("per shot", {"batch": 1}, {}),
+                ("whole step", {}, {"RTM_B200_FUSED": "1", "RTM_B200_TZ_STEP": "16"})]
+    for name, opts, env in variants:
+        with monkeypatch.context() as m:
+            for k, val in env.items():
+                m.setenv(k, val)
+            dv = G.migrate(s, G.RunOptions(accum_fp64=3, **opts), shots, v, rho)
+        for k in ("image1", "image2s", "illum"):
+            assert np.array_equal(dv["f64"][k], db["f64"][k]), (name, k)
 
 
 @pytest.mark.gpu
