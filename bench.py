@@ -50,7 +50,7 @@ MODEL_TEXT = {1: "four flat layers and a dipping 3500 m/s wedge",
 
 # per-shot image accumulation (rtm_options.accum_fp64) chosen by the flags, and its description
 ACCUM_TEXT = {0: "FP32", 1: "FP64", 2: "compensated FP32 pair (Kahan)",
-              3: "FP64 totals of 16-step FP32 partial sums"}
+              3: "FP64 totals of 32-step FP32 partial sums"}
 
 
 def accum_mode(args) -> int:
@@ -99,7 +99,7 @@ def parse():
     ap.add_argument("--accum-kahan", action="store_true",
                     help="per-shot accumulation in compensated fp32 pairs, stacked in fp64")
     ap.add_argument("--accum-blocked", action="store_true",
-                    help="per-shot accumulation in fp64 totals of 16-step fp32 partial sums, stacked in fp64")
+                    help="per-shot accumulation in fp64 totals of 32-step fp32 partial sums, stacked in fp64")
     ap.add_argument("--cpu-sample-steps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -117,7 +117,7 @@ def parse():
                     help="which arms of the configuration-4 comparison to run (comma-separated)")
     ap.add_argument("--headline-accum", type=int, default=3, choices=[1, 2, 3],
                     help="image accumulation of the batched arm (rtm_options.accum_fp64; default 3: fp64 "
-                         "totals of 16-step fp32 partial sums)")
+                         "totals of 32-step fp32 partial sums)")
     return ap.parse_args()
 
 
@@ -201,6 +201,9 @@ def ncu_traffic_per_unit(kernel: str, X: int, Z: int):
 # kernel families timed by the session (split kernels; whole-step kernel)
 KERNEL_FAMILIES = ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv", "step_fwd", "step_recon",
                    "step_recv", "pass_fwd", "pass_bwd")
+# the other kernels of a step, timed the same way and reported beside the stencil families
+# (strip_pack runs once per 32 source-pass steps, image_flush once per 16 backward steps)
+AUX_FAMILIES = ("strip_save", "strip_pack", "image_flush")
 
 
 def kernel_bytes(kind: str, X: int, Z: int, nxi: int, nzi: int, nrec: int, accum_bytes: int, nt: int = 1) -> float:
@@ -343,6 +346,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
     kern = {k: ss.kernel_ms(k) for k in KERNEL_FAMILIES}
+    aux = {k: round(v[0], 4) for k, v in ((k, ss.kernel_ms(k)) for k in AUX_FAMILIES) if v[0] > 0}
     tiles = ss.tile_heights()
     if args.profile_only:
         ss.close()
@@ -416,7 +420,8 @@ def run_ours(args, rank, world, local_rank):
                 # every family's algorithmic bytes per launch / its mean event time, of the same peak
                 "kernel_frac": {k: round(sum(kernel_bytes(k, geos[sh].nxpad, geos[sh].nzpad, geos[sh].nxlength, s.nz,
                                                           geos[sh].nrec, accum_bytes, s.nt) for sh in first)
-                                         / (v[0] * 1e-3) / 1e9 / peak, 4) for k, v in sampled.items()}}
+                                         / (v[0] * 1e-3) / 1e9 / peak, 4) for k, v in sampled.items()},
+                "aux_kernel_ms": aux}
     return dict(value=value, gcell=gcell, ms_total=ms_total, launches=launches, e2e=e2e, roofline=roofline, tiles=tiles,
                 clocks=clock_info, shots_done=shots_done, t_data=t_data, X=X, Z=Z, nxi=nxi, nzi=nzi, nrec=nrec,
                 w_shot=w_timed / (K * B), s=s, shots_per_launch=nshots_launch, meta=meta, all_shots=all_shots)
@@ -481,7 +486,8 @@ def run_headline(args, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        kern = {k: round(v[0], 4) for k, v in ((k, ss.kernel_ms(k)) for k in KERNEL_FAMILIES) if v[0] > 0}
+        kern = {k: round(v[0], 4) for k, v in ((k, ss.kernel_ms(k)) for k in KERNEL_FAMILIES + AUX_FAMILIES)
+                if v[0] > 0}
         tiles = ss.tile_heights()
         ss.close()
         w = sum(w_of(sh) for sh in arm_shots)
@@ -742,7 +748,7 @@ def main():
     headline = None
     if world == 1 and not args.no_headline and args.config == 2 and not args.profile_only:
         headline = run_headline(args, local_rank)
-    acc_txt = {0: "f32 images", 1: "f64 images", 2: "kahan-f32 images", 3: "f64 images of f32 16-step partials"}[
+    acc_txt = {0: "f32 images", 1: "f64 images", 2: "kahan-f32 images", 3: "f64 images of f32 32-step partials"}[
         accum_mode(args)]
     dtype = "f32" if acc_txt == "f32 images" and args.strips == "fp32" and args.gathers == "fp32" else \
         f"f32 stencil, {args.strips} strips, {args.gathers} gathers, {acc_txt}"

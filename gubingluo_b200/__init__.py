@@ -214,7 +214,7 @@ class RunOptions:
     strip_precision: str = "fp32"
     gather_precision: str = "fp32"
     accum_fp64: int = 0     # 0 fp32, 1 (or True) fp64, 2 compensated fp32 pairs, 3 fp64 totals of
-                            # 16-step fp32 partial sums; 1-3 stack in fp64
+                            # 32-step fp32 partial sums; 1-3 stack in fp64
     batch: int = 0
     use_graph: int = 0      # 1: each pass as a CUDA graph per launch shape; 2: with rounded fixed grids
     verbose: bool = False

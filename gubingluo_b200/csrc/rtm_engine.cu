@@ -1245,11 +1245,16 @@ static int batch_forward(rtm_session *ss, BatchRun &br, int nsteps, bool save, b
                 ss->launches += 1;
             }
             if (save) {
+                timing_begin(ss, "strip_save", it, &e);
                 launch_strip_save(table(ss, br), br.n, br.strip_grid, it, a.ring, o.strip_precision, st);
+                timing_end(ss, e);
                 ss->launches++;
             }
             if (save && o.strip_precision != RTM_PREC_FP32 && (a.ring == kRing - 1 || it == nsteps - 1)) {
+                // timed on every 8th ring (the sampling step of timing_begin)
+                timing_begin(ss, "strip_pack", (it / kRing) % 8 == 1 ? 7 : 0, &e);
                 launch_strip_pack(table(ss, br), br.n, it - a.ring, 0, a.ring + 1, o.strip_precision, st);
+                timing_end(ss, e);
                 ss->launches++;
             }
         }
@@ -1361,7 +1366,10 @@ static int batch_backward(rtm_session *ss, BatchRun &br)
     // and after the last step (it = 0)
     auto flush_images = [&](int it) {
         if (o.accum_fp64 != RTM_ACC_FP64_BLOCKED || it % RTM_ACC_BLOCK) return;
+        cudaEvent_t e;
+        timing_begin(ss, "image_flush", (it / RTM_ACC_BLOCK) % 4 == 1 ? 7 : 0, &e);   // every 4th flush
         launch_image_flush(table(ss, br), n, br.ex_nxi, br.ex_nzi, st);
+        timing_end(ss, e);
         ss->launches++;
     };
     auto loop = [&] {

@@ -125,12 +125,29 @@ __global__ void k_mute(float *g, const float *vrow, int X, int nsx, int nsz, int
 // batch, copy the ten cells inside each PML edge of vx, vz and p into the step's strip
 // record, laid out [vx lr 2][nzi][10] [vz tb 2][10][nxi] [p lr 2][nzi][10] [p tb 2][10][nxi].
 // fp32 strips go straight to strips[it]; fp16/bf16 strips go to the fp32 staging ring slot
-// `ring` and are packed later.  Grid (ceil(strip_len / 256), nshots).
-__global__ void k_strip_save(const ShotDev *shots, int it, int ring, int prec)
+// `ring` and are packed later.  Each thread copies CPT cells blockDim apart, its loads issued
+// before its stores: 8 when the batch's strips fill the GPU several times over, so that a
+// thread has several loads in flight (one cell per thread waited out the load latency in ~17
+// rounds of resident threads at 64 shots); 1 for small batches, where more threads with one
+// cell each finish sooner.  Grid (ceil(strip_len / (256 * CPT)), nshots).
+template <int CPT>
+__global__ void __launch_bounds__(256) k_strip_save(const ShotDev *shots, int it, int ring, int prec)
 {
     const ShotDev &S = shots[blockIdx.y];
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx < S.strip_len) strip_save_cell(S, idx, it, ring, prec);
+    const int i0 = blockIdx.x * blockDim.x * CPT + threadIdx.x;
+    float v[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        const int idx = i0 + c * blockDim.x;
+        v[c] = idx < S.strip_len ? strip_cell_value(S, idx) : 0.0f;
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        const int idx = i0 + c * blockDim.x;
+        if (idx >= S.strip_len) break;
+        if (prec == RTM_FP32) ((float *)S.strips)[(size_t)it * S.strip_len + idx] = v[c];
+        else S.strip_stage[(size_t)ring * S.strip_len + idx] = v[c];
+    }
 }
 
 // =====================================================================================
@@ -453,8 +470,13 @@ void launch_mute(float *g, const float *vrow, int X, int nsx, int nsz, int nt, i
 void launch_strip_save(const ShotDev *shots, int nshots, int max_strip_len, int it, int ring, int prec,
                        cudaStream_t s)
 {
-    dim3 grid((max_strip_len + 255) / 256, nshots);
-    k_strip_save<<<grid, 256, 0, s>>>(shots, it, ring, prec);
+    if ((long)nshots * max_strip_len >= 8L * 148 * 2048) {
+        dim3 grid((max_strip_len + 256 * 8 - 1) / (256 * 8), nshots);
+        k_strip_save<8><<<grid, 256, 0, s>>>(shots, it, ring, prec);
+    } else {
+        dim3 grid((max_strip_len + 255) / 256, nshots);
+        k_strip_save<1><<<grid, 256, 0, s>>>(shots, it, ring, prec);
+    }
 }
 void launch_strip_pack(const ShotDev *shots, int nshots, int it0, int ring0, int nsteps, int prec, cudaStream_t s)
 {

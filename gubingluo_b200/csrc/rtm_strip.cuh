@@ -5,9 +5,8 @@
 #pragma once
 #include "rtm_types.h"
 
-// Cell idx (< S.strip_len) of step it: fp32 strips straight to strips[it]; fp16/bf16 strips
-// to the fp32 staging ring slot `ring` (packed later).
-__device__ __forceinline__ void strip_save_cell(const ShotDev &S, int idx, int it, int ring, int prec)
+// Value of strip cell idx (< S.strip_len) in the source wavefield's current fields.
+__device__ __forceinline__ float strip_cell_value(const ShotDev &S, int idx)
 {
     constexpr int R = RTM_RADIUS;
     const int X = S.X, Z = S.Z, npml = S.npml, nxi = S.nxi, nzi = S.nzi, pitch = S.pitch;
@@ -33,7 +32,14 @@ __device__ __forceinline__ void strip_save_cell(const ShotDev &S, int idx, int i
         z = side == 0 ? npml - R + r : (pstrip ? Z - npml : Z - npml - 1) + r;
         f = pstrip ? S.a.p : S.a.vz;
     }
-    const float v = f[(size_t)z * pitch + x];
+    return f[(size_t)z * pitch + x];
+}
+
+// Cell idx (< S.strip_len) of step it: fp32 strips straight to strips[it]; fp16/bf16 strips
+// to the fp32 staging ring slot `ring` (packed later).
+__device__ __forceinline__ void strip_save_cell(const ShotDev &S, int idx, int it, int ring, int prec)
+{
+    const float v = strip_cell_value(S, idx);
     if (prec == RTM_FP32) ((float *)S.strips)[(size_t)it * S.strip_len + idx] = v;
     else S.strip_stage[(size_t)ring * S.strip_len + idx] = v;
 }

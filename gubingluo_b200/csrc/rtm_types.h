@@ -124,7 +124,7 @@ struct KahanAcc {
 // fp32 form does and added into the totals, then cleared, every RTM_ACC_BLOCK steps and after
 // the last one).
 enum RtmAccum { RTM_ACC_FP32 = 0, RTM_ACC_FP64 = 1, RTM_ACC_KAHAN = 2, RTM_ACC_FP64_BLOCKED = 3 };
-#define RTM_ACC_BLOCK 16
+#define RTM_ACC_BLOCK 32
 
 // TMA tensor maps of one slot: the staged fields of the two wavefields with the box each
 // stencil kernel loads (velocity: p rows z0-9 .. z0+BZ+12, columns x0-12 .. x0+139;

@@ -77,8 +77,8 @@ typedef struct rtm_options {
     int gather_precision;    /* RTM_PREC_*: storage of the receiver gathers */
     int accum_fp64;          /* per-shot image/illumination accumulation: 0 fp32; 1 fp64; 2
                                 compensated fp32 pairs (Kahan, 8 bytes like fp64); 3 fp64
-                                totals of fp32 partial sums over 16 steps (the steps image into
-                                fp32 partials, which a flush adds into the fp64 totals every 16
+                                totals of fp32 partial sums over 32 steps (the steps image into
+                                fp32 partials, which a flush adds into the fp64 totals every 32
                                 steps and after the last); with 1, 2 or 3 the stacked images and
                                 the division are fp64 */
     int batch;               /* shots per launch; 0 = as many as fit in device memory */

@@ -7,7 +7,7 @@ against the CPU oracle (FP32 restatement and FP64 build of the same scheme).
   oracle, and within 1e-4 of the FP64 oracle.
 * Configuration 4 at full length (nt = 5000, 0.8 ms) on its narrowest and widest drawn
   apertures (201 and 801 columns; 281 x 881 and 881 x 881 padded): fp16 boundary strips and
-  gathers with fp64 image accumulation (every step, and fp64 totals of 16-step fp32 partial
+  gathers with fp64 image accumulation (every step, and fp64 totals of 32-step fp32 partial
   sums) within 1e-3 rel-L2 of the FP64 oracle, bf16 strips and gathers too, plain FP32 within
   1e-4.  The drift of the source wavefield reconstructed
   from fp16 strips against the one reconstructed from fp32 strips, taken at the end of the

@@ -591,13 +591,13 @@ def test_compensated_fp32_accumulation(rtmlib, monkeypatch):
 @pytest.mark.gpu
 def test_blocked_fp64_accumulation(rtmlib, monkeypatch):
     """accum_fp64 = 3: the steps image into fp32 partial sums, which a flush adds into fp64
-    totals every 16 steps and after the last (nt - 1 backward steps, not a multiple of 16
+    totals every 32 steps and after the last (nt - 1 backward steps, not a multiple of 32
     here): within 1e-6 rel-L2 of fp64 accumulation every step; the same bits from both kernel
     forms, from graph replays, from one shot per launch, and from the whole-step kernel; the
     other imaging conditions (their accumulators fp64 as before) within 1e-6 too."""
     G = rtmlib
     c = GENERAL[0]
-    assert (c["nt"] - 1) % 16
+    assert (c["nt"] - 1) % 32
     v, rho = _random_model(c["nz"], c["nx"], 17)
     shots = [1, 2]
     s = cfg_from(G, _survey(c, 0))
