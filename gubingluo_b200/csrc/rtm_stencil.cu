@@ -39,8 +39,10 @@
 // Velocity update.  MODE 0: forward, full grid; 2: receiver (backward model), full grid;
 // 3: reconstruction of the source wavefield (interior only, vx/vz strips of step it+1
 // restored).
-// Register budget (measured): 6 blocks per SM (80 registers, no spills) in every mode but the
-// 8-row reconstruction tiles (5, which would spill at 6); with its interior-tile body the
+// Register budget (measured): 6 blocks per SM (80 registers, no spills) for the reconstruction
+// and for the 32-row forward and receiver tiles (whose 33 KB of staged rows allow no more),
+// 8 (64 registers, no spills) for the 8- and 16-row forward and receiver tiles, 5 for the
+// 8-row reconstruction tiles (which would spill at 6); with its interior-tile body the
 // reconstruction runs 4% faster at 6 than at 5.
 // The work of one block on tile t (the kernels below, and the persistent pass kernel);
 // `sw` is the block's dynamic shared memory; `use`: how many tiles the block has staged with
@@ -229,7 +231,8 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
 // g1 += ps*p, illum += ps*ps; 3: reconstruction (interior, p strips of step it restored,
 // source subtracted).
 // Register budgets (measured, no spills): 7 blocks per SM (72 registers) for the forward and
-// receiver passes in their 2-row groups, 6 (80 registers) for the reconstruction in 4-row
+// receiver passes in their 2-row groups (8 at 64 registers for the forward pass's 8-row
+// tiles; the receiver pass spills there), 6 (80 registers) for the reconstruction in 4-row
 // groups, 4 for the receiver pass with fp64 accumulators (123 registers).  With 4-row groups
 // the receiver pass needed 96 registers (5 blocks) and spilled when capped at 6.
 //
@@ -481,7 +484,8 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
 // The kernels: one block per tile of the launch's list (reconstruction: tiles of the
 // interior and its strips only).
 template <int BZ, int MODE>
-__global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_BLOCKS) : 6) k_vel(const StepArgs a)
+__global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_BLOCKS) : BZ <= 16 ? 8 : 6)
+    k_vel(const StepArgs a)
 {
     extern __shared__ __align__(128) float sw[];
     if (tile_beyond(a)) return;   // fixed-grid launch: past this batch's tiles
@@ -490,7 +494,7 @@ __global__ void __launch_bounds__(BX, MODE == 3 ? (BZ == 8 ? 5 : RTM_VEL_RECON_B
 template <int BZ, int MODE, typename ACC>
 __global__ void __launch_bounds__(BX, MODE == 2   ? (sizeof(ACC) == 8 ? 4 : RTM_PRES_RECV_BLOCKS)
                                      : MODE == 3 ? RTM_PRES_RECON_BLOCKS
-                                                 : RTM_PRES_FWD_BLOCKS)
+                                                 : BZ == 8 ? 8 : RTM_PRES_FWD_BLOCKS)
     k_pres(const StepArgs a, int record)
 {
     extern __shared__ __align__(128) float sm[];
