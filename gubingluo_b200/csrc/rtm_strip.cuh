@@ -16,17 +16,23 @@ __device__ __forceinline__ float strip_cell_value(const ShotDev &S, int idx)
     if (k < 2 * lr || (k >= 2 * lr + 2 * tb && k < 4 * lr + 2 * tb)) {   // left/right strips
         const bool pstrip = k >= 2 * lr;
         if (pstrip) k -= 2 * lr + 2 * tb;
-        const int side = k / lr, rem = k - side * lr;
-        z = npml + rem / R;
-        const int c = rem % R;
+        const int side = k >= lr ? 1 : 0, rem = k - side * lr;   // k < 2 * lr here
+        const int q = rem / R;                                   // R: a constant divisor
+        z = npml + q;
+        const int c = rem - q * R;
         // vx right strip starts at X-npml-1 (vx has X-1 columns), p right strip at X-npml
         x = side == 0 ? npml - R + c : (pstrip ? X - npml : X - npml - 1) + c;
         f = pstrip ? S.a.p : S.a.vx;
     } else {                                                             // top/bottom strips
         const bool pstrip = k >= 4 * lr + 2 * tb;
         k -= pstrip ? 4 * lr + 2 * tb : 2 * lr;
-        const int side = k / tb, rem = k - side * tb;
-        const int r = rem / nxi;
+        const int side = k >= tb ? 1 : 0, rem = k - side * tb;   // k < 2 * tb here
+        // r = rem / nxi (< R): a float estimate (rem < 2^24, exact in fp32; the product's
+        // rounding moves the estimate by at most one) corrected both ways, without the
+        // integer division's instruction sequence
+        int r = __float2int_rz(__int2float_rn(rem) * __frcp_rn(__int2float_rn(nxi)));
+        r -= (r * nxi > rem) ? 1 : 0;
+        r += ((r + 1) * nxi <= rem) ? 1 : 0;
         x = npml + (rem - r * nxi);
         // vz bottom strip starts at Z-npml-1 (vz has Z-1 rows), p bottom strip at Z-npml
         z = side == 0 ? npml - R + r : (pstrip ? Z - npml : Z - npml - 1) + r;
