@@ -202,7 +202,7 @@ def ncu_traffic_per_unit(kernel: str, X: int, Z: int):
 KERNEL_FAMILIES = ("vel_fwd", "pres_fwd", "vel_recon", "pres_recon", "vel_recv", "pres_recv", "step_fwd", "step_recon",
                    "step_recv", "pass_fwd", "pass_bwd")
 # the other kernels of a step, timed the same way and reported beside the stencil families
-# (strip_pack runs once per 32 source-pass steps, image_flush once per 16 backward steps)
+# (strip_pack runs once per 32 source-pass steps, image_flush once per 32 backward steps)
 AUX_FAMILIES = ("strip_save", "strip_pack", "image_flush")
 
 
