@@ -128,9 +128,12 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
 
     // interior tiles (TileRef.interior: every column in [npml, X-npml-1), every row in
     // [npml, Z-npml-1), where the velocity damping is 1 and no strip lies): the update
-    // alone, in the arithmetic of the general body
+    // alone, in the arithmetic of the general body.  The 32-row forward and receiver tiles
+    // unroll four row groups, so that the z window's shift becomes register renaming within
+    // them (measured 1.5-2.5% faster; the pressure kernels and the smaller tiles were not
+    // faster that way, or spilled)
     if (t.interior) {
-#pragma unroll 1
+#pragma unroll (MODE == 3 || BZ < 32 ? 1 : 4)
         for (int z = z0; z < z0 + BZ; z += U) {
             float nir[U], nov[U], now[U];
             const bool more = z + 2 * U <= z0 + BZ;
