@@ -502,18 +502,20 @@ void launch_finalize(const void *fs, int nshots, int nx, int nz, int fp64, void 
 __global__ void k_image_flush(const ShotDev *shots)
 {
     const ShotDev &S = shots[blockIdx.z];
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x, iz = blockIdx.y;
-    if (ix >= S.X - 2 * S.npml || iz >= S.Z - 2 * S.npml) return;
-    const size_t id = (size_t)(iz + S.npml) * S.pitch + (ix + S.npml);
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x, nzi = S.Z - 2 * S.npml;
+    if (ix >= S.X - 2 * S.npml) return;
     float *g1 = (float *)S.g1, *il = (float *)S.illum;
-    S.g1t[id] += (double)g1[id];
-    S.illt[id] += (double)il[id];
-    g1[id] = 0.f;
-    il[id] = 0.f;
+    for (int iz = blockIdx.y; iz < nzi; iz += gridDim.y) {
+        const size_t id = (size_t)(iz + S.npml) * S.pitch + (ix + S.npml);
+        S.g1t[id] += (double)g1[id];
+        S.illt[id] += (double)il[id];
+        g1[id] = 0.f;
+        il[id] = 0.f;
+    }
 }
 void launch_image_flush(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, cudaStream_t s)
 {
-    dim3 grid((max_nxi + 255) / 256, max_nzi, nshots);
+    dim3 grid((max_nxi + 255) / 256, std::min(max_nzi, 65535), nshots);
     k_image_flush<<<grid, 256, 0, s>>>(shots);
 }
 void launch_image_extra(const ShotDev *shots, int nshots, int max_nxi, int max_nzi, int parity, int fp64,
