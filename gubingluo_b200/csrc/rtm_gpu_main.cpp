@@ -28,7 +28,8 @@ static void selfdoc()
         "  table is scanned once into ./shotprofileId.dat (reused when present).\n"
         "Writes ./output/{idevice}{Illum,Image1,Image2s,...,Image5m}.su.\n"
         "Environment: RTM_B200_STRIPS / RTM_B200_GATHERS = fp32|fp16|bf16,\n"
-        "  RTM_B200_ACCUM_FP64=1, RTM_B200_BATCH=<shots per launch>, RTM_B200_RECEIVER_DEPTH=<cells>,\n"
+        "  RTM_B200_ACCUM_FP64=1|2|3 (fp64 / compensated fp32 / fp64 totals of 32-step fp32 sums),\n"
+        "  RTM_B200_BATCH=<shots per launch>, RTM_B200_RECEIVER_DEPTH=<cells>,\n"
         "  RTM_B200_EXTRA_IMAGES=0|1|2, RTM_B200_FK_MIRROR=0|1, RTM_B200_LOG=<JSON-lines file>.\n"
         "Options: --checkpoint <file> saves the stacked images after every batch;\n"
         "  --resume continues from that file when it matches the run (same parameters and models).\n");
