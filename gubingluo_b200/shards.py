@@ -50,3 +50,62 @@ def allreduce_images(tensors, dist) -> None:
         return
     for t in tensors:
         dist.all_reduce(t)
+
+
+def migrate_sharded(survey: SurveyConfig, options, shots, vp, rho, gathers=None, vp_mig=None, rho_mig=None,
+                    dist=None, migrate_fn=None) -> dict:
+    """Migrate `shots` over the ranks of the default torch.distributed process group, one
+    process per GPU (`options.device` = the rank's GPU): every rank computes the same
+    longest-processing-time partition, migrates its own shots, and one all-reduce per image
+    sums the stacked images, which every rank then returns.  `gathers` (mode 1) lists every
+    shot's gather in the order of `shots`, on every rank (each rank uploads only its own).
+    With `dist` None, or a world of one, it is `migrate` on all the shots.
+
+    The images travel through the rank's GPU for an NCCL group and stay on the host for gloo;
+    in mode 0 each rank returns the gathers of its own shots (`shots_of_rank`, in that order).
+    The sums over ranks add the ranks' stacked images in rank order, not shot by shot, so the
+    result equals a single-process run's to within the images' rounding, not bit for bit.
+    `migrate_fn(survey, options, shots, vp, rho, gathers, vp_mig, rho_mig)` replaces the
+    library's `migrate` (the CPU tests pass the oracle there).  Every rank must call this with
+    the same arguments; a rank that fails before the reduction makes the others' reduction
+    fail with an error (or time out with the process group's timeout) rather than wait."""
+    import numpy as np
+
+    if migrate_fn is None:
+        from . import migrate as migrate_fn
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    parts = lpt_shards(shot_costs(survey, shots), world)
+    idx = parts[rank]
+    mine = [shots[i] for i in idx]
+    if mine:
+        out = dict(migrate_fn(survey, options, mine, vp, rho, None if gathers is None else [gathers[i] for i in idx],
+                              vp_mig, rho_mig))
+    else:   # more ranks than shots: this rank adds zeros
+        z = np.zeros((survey.nz, survey.nx), np.float32)
+        out = {k: z.copy() for k in ("image1", "image2s", "image2m", "illum")}
+        if getattr(options, "accum_fp64", 0):
+            out["f64"] = {k: np.zeros((survey.nz, survey.nx)) for k in ("image1", "image2s", "illum")}
+        if getattr(options, "extra_images", 0):
+            for k in ("image3s", "image4s", "image5s", "image3m", "image4m", "image5m", "imagetrue"):
+                out[k] = z.copy()
+        if survey.mode == 0:
+            out["gathers"] = []
+    out["shots_of_rank"] = mine
+    if world == 1:
+        return out
+    import torch
+
+    dev = f"cuda:{options.device}" if dist.get_backend() == "nccl" else "cpu"
+
+    def reduced(a):   # on a copy: the caller's arrays (which may alias each other) stay as they were
+        t = torch.tensor(np.asarray(a), device=dev)
+        dist.all_reduce(t)
+        return t.cpu().numpy()
+
+    # the same keys in the same order on every rank: every image is a sum over shots
+    for k in sorted(k for k, v in out.items() if k.startswith(("image", "illum")) and isinstance(v, np.ndarray)):
+        out[k] = reduced(out[k])
+    if "f64" in out:
+        out["f64"] = {k: reduced(out["f64"][k]) for k in sorted(out["f64"])}
+    return out

@@ -1,9 +1,10 @@
 """One rank of the two-rank CPU check of the shot-sharded migration (run by test_shards.py).
 
-Each rank migrates its longest-processing-time shard of the shots with the oracle (FP64 CPU
-restatement; the GPU library is not needed here), then the ranks sum their stacked images
-over gloo, exactly as the multi-GPU run sums its device images over NCCL.  Rank 0 writes
-the reduced images to the output file.
+Each rank calls the library's `shards.migrate_sharded` over gloo, with the oracle (FP64 CPU
+restatement; the GPU library is not needed here) in place of the GPU migration: the
+function partitions the shots, the rank migrates its longest-processing-time share, and the
+ranks sum their stacked images, as a multi-GPU run sums them over NCCL.  Rank 0 writes the
+reduced images to the output file.
 
     python tests/_gloo_rank.py <rank> <world> <port> <out.npz> [fail]
 
@@ -36,9 +37,8 @@ def survey():
 def main():
     rank, world, port, out = int(sys.argv[1]), int(sys.argv[2]), sys.argv[3], sys.argv[4]
     fail = len(sys.argv) > 5 and sys.argv[5] == "fail"
-    import torch
     import torch.distributed as dist
-    from gubingluo_b200 import SurveyConfig, shards
+    from gubingluo_b200 import RunOptions, SurveyConfig, shards
     from oracle import oracle as O
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -46,24 +46,23 @@ def main():
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=20 if fail else 60))
     s, shots, vp, rho = survey()
     cfg = SurveyConfig(**{k: s[k] for k in SurveyConfig.__dataclass_fields__})
-    parts = shards.lpt_shards(shards.shot_costs(cfg, shots), world)
-    mine = [shots[i] for i in parts[rank]]
-    if mine:
-        r = O.rtm_model(s, mine, vp, rho, precision="f64")
-        imgs = [r["image1"], r["image2s"], r["illum"]]
-    else:
-        imgs = [np.zeros((s["nz"], s["nx"])) for _ in range(3)]
-    ts = [torch.from_numpy(np.ascontiguousarray(a, np.float64)) for a in imgs]
-    if fail and rank == world - 1:
-        os._exit(3)   # ends without leaving the process group, like a crashed rank
+
+    def oracle_migrate(survey_, options, mine, vp_, rho_, gathers, vp_mig, rho_mig):
+        r = O.rtm_model(s, mine, vp_, rho_, precision="f64")
+        if fail and rank == world - 1:
+            os._exit(3)   # after its shots, before the reduction; leaves without a word, like a crash
+        return {"image1": r["image1"], "image2s": r["image2s"], "image2m": r["image1"], "illum": r["illum"]}
+
     try:
-        shards.allreduce_images(ts, dist)
+        red = shards.migrate_sharded(cfg, RunOptions(), shots, vp, rho, dist=dist, migrate_fn=oracle_migrate)
     except Exception as e:   # the peer is gone: report and stop
         with open(out + ".failed", "w") as f:
             f.write(f"rank {rank}: {type(e).__name__}: {e}")
         os._exit(4)
+    parts = shards.lpt_shards(shards.shot_costs(cfg, shots), world)
+    assert red["shots_of_rank"] == [shots[i] for i in parts[rank]]
     if rank == 0:
-        np.savez(out, image1=ts[0].numpy(), image2s=ts[1].numpy(), illum=ts[2].numpy(),
+        np.savez(out, image1=red["image1"], image2s=red["image2s"], illum=red["illum"],
                  parts=np.array([len(p) for p in parts]))
     dist.barrier()
     dist.destroy_process_group()

@@ -95,3 +95,59 @@ def test_a_rank_that_dies_before_the_reduction_ends_the_others(tmp_path):
     assert os.path.exists(out + ".failed") and not os.path.exists(out)
     assert "rank 0" in open(out + ".failed").read()
     assert time.time() - t0 < 200
+
+
+class _RecordingDist:
+    """Stands in for torch.distributed in one process: records the all-reduce calls (shape,
+    dtype) without reducing, so that ranks with and without shots can be compared."""
+
+    def __init__(self, world, rank):
+        self.world, self.rank, self.calls = world, rank, []
+
+    def get_world_size(self):
+        return self.world
+
+    def get_rank(self):
+        return self.rank
+
+    def get_backend(self):
+        return "gloo"
+
+    def all_reduce(self, t):
+        self.calls.append((tuple(t.shape), str(t.dtype)))
+
+
+def test_sharded_migration_ranks_take_the_same_collective_steps(rtmlib):
+    """Every rank of migrate_sharded makes the same all-reduce calls in the same order, also a
+    rank left without shots (more ranks than shots, which adds zeros), with fp64 and the other
+    imaging conditions on; world 1 runs the migration on all the shots."""
+    from gubingluo_b200 import RunOptions, SurveyConfig
+    from gubingluo_b200.shards import migrate_sharded
+    s = SurveyConfig(nx=40, nz=20, nt=50, dx=10.0, dz=10.0, dt=1e-3, npml=10, layout=2, spx0=100.0, spz0=10.0,
+                     dspx=100.0, mode=1)
+    opts = RunOptions(accum_fp64=3, extra_images=1)
+    seen = []
+
+    def fake(survey, options, shots, vp, rho, gathers, vp_mig, rho_mig):
+        seen.append((list(shots), None if gathers is None else len(gathers)))
+        one = np.ones((survey.nz, survey.nx), np.float32)
+        out = {k: one * len(shots) for k in ("image1", "image2s", "image2m", "illum")}
+        out["f64"] = {k: np.ones((survey.nz, survey.nx)) for k in ("image1", "image2s", "illum")}
+        for k in ("image3s", "image4s", "image5s", "image3m", "image4m", "image5m", "imagetrue"):
+            out[k] = one.copy()
+        out["stats"] = object()
+        return out
+
+    shots = [1, 2]
+    gathers = [np.zeros((50, 40), np.float32) for _ in shots]
+    calls = []
+    for rank in range(3):
+        d = _RecordingDist(3, rank)
+        out = migrate_sharded(s, opts, shots, None, None, gathers=gathers, dist=d, migrate_fn=fake)
+        calls.append(d.calls)
+        assert out["shots_of_rank"] == ([1], [2], [])[rank]
+        assert out["image1"].shape == (20, 40)
+    assert calls[0] == calls[1] == calls[2] and len(calls[0]) == 11 + 3
+    assert seen == [([1], 1), ([2], 1)]   # rank 2 migrated nothing
+    out = migrate_sharded(s, opts, shots, None, None, gathers=gathers, migrate_fn=fake)
+    assert out["shots_of_rank"] == shots and float(out["image1"][0, 0]) == 2.0
