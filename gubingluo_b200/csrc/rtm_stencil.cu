@@ -98,11 +98,14 @@ __device__ __forceinline__ void vel_tile(const StepArgs &a, const TileRef t, flo
     // vx order of this column (cuda_norderx): full unless within ten cells of the edge
     const int ox = min(min(x + 1, X - 1 - x), R);
     const int zend = min(z0 + BZ, Z);
-    // Tiles that reach the outer ten cells of the grid take the table-coefficient form of the
-    // unrolled groups: vx order per column (cuda_norderx), vz order per row (cuda_norderz).
-    // The reconstruction writes only cells at least npml >= R from the edge, where every
-    // order is full.
-    const bool edge_tile = MODE != 3 && (x0 < R || x0 + BX > X - R || z0 < R || zend > Z - R);
+    // Warps whose columns, or whose tile's rows, reach the outer ten cells of the grid take the
+    // table-coefficient form of the unrolled groups: vx order per column (cuda_norderx), vz
+    // order per row (cuda_norderz).  The others have the full order everywhere, whose table
+    // row equals the constant coefficients, so either form gives the same bits; the choice is
+    // per warp, so warps do not diverge.  The reconstruction writes only cells at least
+    // npml >= R from the edge, where every order is full.
+    const int xw0 = x0 + (tx & ~31);
+    const bool edge_tile = MODE != 3 && (xw0 < R || xw0 + 32 > X - R || z0 < R || zend > Z - R);
     const float *cxe = &s_tab[(max(ox, 1) - 1) * R];
     // operands of the first unrolled group, loaded while the tile is staged
     float cir[U], cov[U], cow[U];
@@ -312,8 +315,11 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
     // local order of this column (cuda_norder): full unless within ten cells of the edge
     const int rpx = min(min(x, X - 1 - x), R);
     const int zend = min(z0 + BZ, Z);
-    // tiles that reach the outer ten cells take the table-coefficient form of the groups
-    const bool edge_tile = MODE != 3 && (x0 < R || x0 + BX > X - R || z0 < R || zend > Z - R);
+    // warps whose columns, or whose tile's rows, reach the outer ten cells take the
+    // table-coefficient form of the groups (per warp, as in the velocity kernel; per tile in
+    // the receiver pass, whose larger body ran 2-4% slower with the choice per warp)
+    const int xw0 = MODE == 2 ? x0 : x0 + (tx & ~31), xw1 = MODE == 2 ? x0 + BX : xw0 + 32;
+    const bool edge_tile = MODE != 3 && (xw0 < R || xw1 > X - R || z0 < R || zend > Z - R);
     // operands of an unrolled group of rows
     float ckk[U], cp0[U], cs1[U], cs2[U], cps[U];
     ACC cg1[U], cil[U];

@@ -609,7 +609,8 @@ def test_blocked_fp64_accumulation(rtmlib, monkeypatch):
     for k in ("image3s", "image4s", "image5s"):   # normalised by the (blocked) illumination
         assert rel_l2(db[k], d64[k]) < 1e-6, (k, rel_l2(db[k], d64[k]))
     variants = [("scalar", {}, {"RTM_B200_KERNELS": "scalar"}), ("vector", {}, {"RTM_B200_KERNELS": "vector"}),
-                ("graph", {"use_graph": 1}, {}), ("per shot", {"batch": 1}, {}),
+                ("graph", {"use_graph": 1}, {}), ("rounded graph", {"use_graph": 2, "batch": 1}, {}),
+                ("per shot", {"batch": 1}, {}),
                 ("whole step", {}, {"RTM_B200_FUSED": "1", "RTM_B200_TZ_STEP": "16"})]
     for name, opts, env in variants:
         with monkeypatch.context() as m:
