@@ -14,8 +14,8 @@
 //   * the full-order coefficients come from the kernel-parameter constant bank.  Tiles that
 //     reach the outer ten cells of the grid, where the local order is reduced (reference
 //     cuda_norder*, kernel.cu:271-317), run the same groups with coefficients from rows of the
-//     zero-padded table (the choice is per tile, so warps do not diverge); rows left over
-//     after the last whole group take a compact one-row path;
+//     zero-padded table (the choice is per warp or per tile, so warps do not diverge); rows
+//     left over after the last whole group take a compact one-row path;
 //   * PML damping, split pressure, source, receivers, strip restore and imaging are per-row
 //     or per-column predicates of the same kernel (strips are saved by k_strip_save after
 //     each forward step).
