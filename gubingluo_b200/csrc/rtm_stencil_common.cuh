@@ -259,6 +259,30 @@ __device__ __forceinline__ float tap_sum(C c, F f, G g)
     return s0;
 }
 
+// x-derivatives of the U rows of one column group (U even) with rows u and u+1 as the two
+// lanes of packed fp32 pairs (sm_100: one instruction for both lanes): each lane takes the
+// difference, then a fused multiply-add, in tap order, as tap_sum's sum is compiled, so the
+// results are tap_sum's bits with half the arithmetic instructions.  Row u's staged row
+// starts at rw + u * WW; f(i) = row[i + FO], g(i) = row[GO - i].
+template <int U, int FO, int GO, typename C>
+__device__ __forceinline__ void dx_pairs(const float *rw, float (&dx)[U], C c)
+{
+    static_assert(U % 2 == 0, "rows are paired");
+#pragma unroll
+    for (int u = 0; u < U; u += 2) {
+        const float *r0 = rw + u * WW, *r1 = r0 + WW;
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 1; i <= R; i++) {
+            const float ci = c(i - 1);
+            const float2 d = __fadd2_rn(make_float2(r0[i + FO], r1[i + FO]), make_float2(-r0[GO - i], -r1[GO - i]));
+            s = __ffma2_rn(make_float2(ci, ci), d, s);
+        }
+        dx[u] = s.x;
+        dx[u + 1] = s.y;
+    }
+}
+
 // Per-column constants of the velocity update.
 struct VelCol {
     bool hvx;            // column x carries a vx cell (x < X-1)
