@@ -393,20 +393,37 @@ __device__ __forceinline__ void pres_tile(const StepArgs &a, int record, const T
             // and reconstruction passes were not faster that way (4% slower at 32-row tiles)
             float dxs[U];
             if (MODE == 0) dx_pairs<U, -1, 0>(&colx[(z - z0) * WW], dxs, [&](int j) { return a.c10[j]; });
+            if constexpr (MODE == 0 && U == 2) {
+                // the update of both rows in packed pairs as well: per lane the products and the
+                // separately rounded sum and difference of p_interior, so the same bits
+                float dz2[2];
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const float *rw = &colx[(z + u - z0) * WW];
-                const float dx = MODE == 0 ? dxs[u]
-                                           : tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return rw[i - 1]; },
-                                                     [&](int i) { return rw[-i]; });
-                const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
-                                         [&](int i) { return q[u + 10 - i]; });
-                const float ddx = dx * a.dtx, ddz = dz * a.dtz;
-                const float pn = MODE == 3 ? p_recon(cp0[u], ddx * ckk[u], ddz * ckk[u])
-                                           : p_interior(cp0[u], ddx * ckk[u], ddz * ckk[u]);
-                const unsigned id = id0 + u * pitch;
-                pp[id] = pn;
-                if (MODE == 2) image_cell<ACC>(g1p, ilp, id, cg1[u], cil[u], cps[u], pn);
+                for (int u = 0; u < 2; u++)
+                    dz2[u] = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                                     [&](int i) { return q[u + 10 - i]; });
+                const float2 kk = make_float2(ckk[0], ckk[1]);
+                const float2 dxs2 = __fmul2_rn(__fmul2_rn(make_float2(dxs[0], dxs[1]), make_float2(a.dtx, a.dtx)), kk);
+                const float2 dzs2 = __fmul2_rn(__fmul2_rn(make_float2(dz2[0], dz2[1]), make_float2(a.dtz, a.dtz)), kk);
+                const float2 sum = __fadd2_rn(dxs2, dzs2);
+                const float2 pn = __fadd2_rn(make_float2(cp0[0], cp0[1]), make_float2(-sum.x, -sum.y));
+                pp[id0] = pn.x;
+                pp[id0 + pitch] = pn.y;
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const float *rw = &colx[(z + u - z0) * WW];
+                    const float dx = MODE == 0 ? dxs[u]
+                                               : tap_sum([&](int j) { return a.c10[j]; },
+                                                         [&](int i) { return rw[i - 1]; }, [&](int i) { return rw[-i]; });
+                    const float dz = tap_sum([&](int j) { return a.c10[j]; }, [&](int i) { return q[u + 9 + i]; },
+                                             [&](int i) { return q[u + 10 - i]; });
+                    const float ddx = dx * a.dtx, ddz = dz * a.dtz;
+                    const float pn = MODE == 3 ? p_recon(cp0[u], ddx * ckk[u], ddz * ckk[u])
+                                               : p_interior(cp0[u], ddx * ckk[u], ddz * ckk[u]);
+                    const unsigned id = id0 + u * pitch;
+                    pp[id] = pn;
+                    if (MODE == 2) image_cell<ACC>(g1p, ilp, id, cg1[u], cil[u], cps[u], pn);
+                }
             }
             advance<U, BX>(q, colz, z + U - z0, z + U < z0 + BZ);
             if (more) {
